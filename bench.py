@@ -1,0 +1,457 @@
+"""Benchmark: placement jobs/s of the B200 ElectroPlace path.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload electro_200k_1024]
+
+A step is one complete placement job of the workload (seeded synthetic
+netlist with the benchmark configuration's shapes): initial placement, the
+Nesterov loop run to overflow <= 0.10 (or max_iters), legalisation of every
+checkpoint and the final binding.
+
+  value  jobs/s with the netlist resident in HBM (context created before the
+         timed region), timed with CUDA events around the K jobs.
+  e2e    jobs/s through the C ABI's one-shot eplace_place with host buffers:
+         upload, run and result download inside the timed region.
+
+Multi-GPU: one placement job does not shard (every iteration needs the whole
+bin map and global dot products), so N ranks run N independent replicas
+(seed + rank), no data-path collective; value = jobs of all ranks / max rank
+time ("weak" scaling).
+
+`--impl reference` times the reference algorithm's CPU form (the FP64 C
+restatement in oracle/, single thread, like the reference loop) on a bounded
+sample of the same workload and prints the same metric.
+"""
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "placement jobs/s (run to overflow <= 0.10)"
+UNIT = "jobs/s"
+L2_BYTES = 126 * 1024 * 1024
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="electro_200k_1024")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-reps", type=int, default=30)
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing (replicas only)
+# ---------------------------------------------------------------------------
+class Dist:
+    def __init__(self, args):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as dist
+
+            backend = "nccl" if torch.cuda.is_available() else "gloo"
+            if backend == "nccl":
+                torch.cuda.set_device(self.local)
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, v):
+        if not self.pg:
+            return v
+        import torch
+
+        dev = "cuda" if torch.cuda.is_available() else "cpu"
+        t = torch.tensor([float(v)], dtype=torch.float64, device=dev)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum(self, v):
+        if not self.pg:
+            return v
+        import torch
+
+        dev = "cuda" if torch.cuda.is_available() else "cpu"
+        t = torch.tensor([float(v)], dtype=torch.float64, device=dev)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.SUM)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+class Clocks:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q, "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# roofline bookkeeping
+# ---------------------------------------------------------------------------
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d["hbm_gbs"], d["bf16_tflops"], "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+def algorithmic(nl, chip):
+    """Algorithmic bytes / flops per launch of each iteration kernel.
+    B_wl = 4(Nn+1) + 4P + 8P + 8N, B_sc = 8N + 8 n_macro + 4WH,
+    B_fin = 8WH (read map) + 4WH (write charge), GEMM = 2 M N K flops,
+    B_step = 68N + 8WH."""
+    N, Nn, P = nl.num_cells, nl.num_nets, nl.num_pins
+    W = chip.bins_x or chip.width
+    H = chip.bins_y or chip.height
+    nmac = 0 if nl.cell_w is None else int((nl.cell_w.astype(np.int32) * nl.cell_h > 1).sum())
+    return {
+        "wa_grad": ("hbm", 4 * (Nn + 1) + 12 * P + 8 * N),
+        "density_scatter": ("hbm", 8 * N + 8 * nmac + 4 * W * H),
+        "density_final": ("hbm", 12 * W * H),
+        "dct_gemm1": ("flops", 2 * H * W * W),
+        "dct_gemm2_spectral": ("flops", 2 * H * W * H),
+        "dct_gemm3": ("flops", 2 * 2 * H * W * W),
+        "dct_gemm4": ("flops", 2 * 2 * H * W * H),
+        "gather_step": ("hbm", 68 * N + 8 * W * H),
+    }
+
+
+def ncu_traffic(kernel, workload):
+    """dram bytes per launch from a committed ncu summary, if one exists."""
+    p = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        for ln in f:
+            if ln.startswith("#") or "=" not in ln:
+                continue
+            kv = dict(t.split("=", 1) for t in ln.split())
+            if kv.get("stage") == kernel and kv.get("workload") == workload:
+                return float(kv["dram_bytes_per_launch"])
+    return None
+
+
+# ---------------------------------------------------------------------------
+# CPU form (oracle restatement, single thread) on a bounded sample
+# ---------------------------------------------------------------------------
+def cpu_sample(nl, chip, cfg, iters_per_job, checkpoints_per_job, budget_s=25.0):
+    """Times the FP64 CPU loop on this workload: k Nesterov iterations (no
+    intermediate legalisation) and one legalisation, and extrapolates to one
+    job of `iters_per_job` iterations with `checkpoints_per_job`
+    legalisations."""
+    from oracle.oracle import Oracle
+
+    import copy
+
+    orc = Oracle(nl, chip)
+    c = copy.copy(cfg)
+    # 2 iterations: fixed costs (set-up, legalisation at iterations 0 and 1, final)
+    c.legalize_interval = 10 ** 9
+    c.max_iters = 2
+    t0 = time.perf_counter()
+    orc.place(c)
+    t2 = time.perf_counter() - t0
+    k = 4
+    c.max_iters = 2 + k
+    t0 = time.perf_counter()
+    orc.place(c)
+    tk = time.perf_counter() - t0
+    t_iter = max((tk - t2) / k, 1e-9)
+    # one legalisation of a spread-out state
+    st, sx, sy = orc.initial_placement(cfg.seed)
+    rng = np.random.default_rng(0)
+    x = np.clip(sx + rng.normal(0, 1.5, sx.size), 0, chip.width - 1)
+    y = np.clip(sy + rng.normal(0, 1.5, sy.size), 0, chip.height - 1)
+    t0 = time.perf_counter()
+    orc.legalize(x, y, 1)
+    t_leg = time.perf_counter() - t0
+    job = iters_per_job * t_iter + checkpoints_per_job * t_leg
+    sample = ("FP64 oracle loop, 1 thread: %d+%d iterations timed (%.3f s/iter), one ring-search legalisation "
+              "(%.3f s), extrapolated to %d iterations + %d legalisations per job" %
+              (2, k, t_iter, t_leg, iters_per_job, checkpoints_per_job))
+    return 1.0 / job, sample, t_iter, t_leg
+
+
+def reference_arm(args, dist):
+    if dist.rank != 0:
+        return
+    import eisenjoch_b200 as E
+
+    nl, chip, cfg = E.workload(args.workload)
+    summary = load_job_summary(args.workload)
+    iters = summary["iters"]
+    cps = iters // cfg.legalize_interval + 2
+    vals = []
+    sample = ""
+    t_start = time.perf_counter()
+    for i in range(args.warmup + args.steps):
+        v, sample, _, _ = cpu_sample(nl, chip, cfg, iters, cps)
+        if i >= args.warmup:
+            vals.append(v)
+    value = statistics.mean(vals)
+    line = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": value,
+        "unit": UNIT,
+        "n_gpus": args.gpus,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": 1000.0 / value,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded generator, benchmark shapes)",
+        "config": {"workload": args.workload, "cells": nl.num_cells, "nets": nl.num_nets, "pins": nl.num_pins,
+                   "bins": [chip.bins_x, chip.bins_y], "sites": [chip.width, chip.height],
+                   "iters_per_job": iters, "iters_source": summary["source"]},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "wall_s": time.perf_counter() - t_start,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def load_job_summary(workload):
+    """Iterations to overflow <= 0.10 of this workload's job: the committed
+    FP64 oracle summary when present (tests/golden), else the benchmark
+    configuration's iteration cap."""
+    p = os.path.join(ROOT, "tests", "golden", "job_summaries.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        if workload in d:
+            return {"iters": int(d[workload]["iters"]), "source": "FP64 oracle full run (tests/golden/job_summaries.json)"}
+    import eisenjoch_b200 as E
+
+    return {"iters": int(E.WORKLOADS[workload]["cfg"].get("max_iters", 500)), "source": "max_iters"}
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def ours(args, dist):
+    import torch
+
+    import eisenjoch_b200 as E
+
+    dev = dist.local
+    torch.cuda.set_device(dev)
+    w = E.WORKLOADS[args.workload]
+    spec = E.SynthSpec(**{**w["spec"].__dict__, "seed": w["spec"].seed + 7919 * dist.rank})
+    nl, chip = E.synth_netlist(spec)
+    cfg = E.ElectroPlaceCfg(**w["cfg"])
+    hbm, bf16, peak_src = peaks()
+
+    ctx = E.PlacementContext(nl, chip, device=dev)
+    # --- per-kernel device times (CUDA events on the library's stream) ---
+    stage_ms = ctx.profile_stages(cfg, reps=args.profile_reps)
+    for _ in range(args.warmup):
+        ctx.run(cfg)
+
+    clocks = Clocks(dev)
+    clocks.start()
+    dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    lat, results = [], []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        r = ctx.run(cfg)
+        lat.append(time.perf_counter() - t0)
+        results.append(r)
+    e1.record()
+    torch.cuda.synchronize()
+    dist.barrier()
+    total_s = e0.elapsed_time(e1) / 1000.0
+    ck = clocks.stop()
+    max_s = dist.max(total_s)
+    jobs = dist.sum(args.steps)
+    value = jobs / max_s
+
+    # --- end to end through the C ABI with host buffers ---
+    for _ in range(1):
+        E.place_electro(nl, chip, cfg, device=dev)
+    dist.barrier()
+    torch.cuda.synchronize()
+    e0.record()
+    e2e_res = []
+    for _ in range(args.steps):
+        e2e_res.append(E.place_electro(nl, chip, cfg, device=dev))
+    e1.record()
+    torch.cuda.synchronize()
+    dist.barrier()
+    e2e_s = dist.max(e0.elapsed_time(e1) / 1000.0)
+    e2e_value = jobs / e2e_s
+    ctx.close()
+
+    if dist.rank != 0:
+        return
+
+    r0 = results[-1]
+    # --- roofline of the dominant kernel ---
+    algo = algorithmic(nl, chip)
+    per_iter = {k: stage_ms[k] for k in stage_ms}
+    dom = max(per_iter, key=lambda k: per_iter[k])
+    kind, amount = algo[dom]
+    dur_s = stage_ms[dom] / 1000.0
+    if kind == "hbm":
+        achieved = amount / dur_s / 1e9
+        roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm}
+    else:
+        achieved = amount / dur_s / 1e12
+        roof = {"bound": "tensor", "achieved": achieved, "peak": bf16, "unit": "TFLOP/s", "frac": achieved / bf16}
+    roof["traffic"] = ncu_traffic(dom, args.workload)
+    roof["kernel"] = dom
+    roof["peak_source"] = peak_src + " (MEASURED_PEAKS.json)" if peak_src == "measured" else "fallback"
+    roof["algorithmic_per_launch"] = amount
+    stages = {}
+    for k, ms in stage_ms.items():
+        kd, am = algo[k]
+        if kd == "hbm":
+            stages[k] = {"ms": ms, "GB/s": am / (ms / 1e3) / 1e9}
+        else:
+            stages[k] = {"ms": ms, "TFLOP/s": am / (ms / 1e3) / 1e12}
+
+    cpu = None
+    if not args.no_cpu_baseline and dist.world == 1:
+        cps = r0.iters // cfg.legalize_interval + 2
+        v, sample, t_iter, t_leg = cpu_sample(nl, chip, cfg, r0.iters, cps)
+        cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "port", "sample": sample}
+
+    launches = sum(r.gpu_launches for r in results)
+    line = {
+        "metric": METRIC,
+        "value": value,
+        "unit": UNIT,
+        "n_gpus": dist.world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": max_s * 1000.0 / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32 (FP64 global reductions)",
+        "data": "synthetic (seeded generator, benchmark shapes); replica r uses seed + 7919 r",
+        "config": {
+            "workload": args.workload,
+            "cells": nl.num_cells, "nets": nl.num_nets, "pins": nl.num_pins, "pads": nl.num_fixed,
+            "sites": [chip.width, chip.height], "bins": [chip.bins_x, chip.bins_y],
+            "max_iters": cfg.max_iters, "legalize_interval": cfg.legalize_interval,
+            "parallelism": "replicas x%d" % dist.world,
+            "l2": "per-iteration working set is L2-resident at this size; no flush between jobs "
+                  "(each job runs hundreds of iterations)",
+            "dct": "fp32 simt gemm",
+        },
+        "job": {
+            "iters": r0.iters, "converged": r0.converged, "overlap": r0.overlap, "hpwl": r0.hpwl,
+            "best_iter": r0.best_iter, "time_to_overflow_s": statistics.median(lat),
+            "gpu_loop_s": r0.gpu_seconds, "p50_latency_s": float(np.percentile(lat, 50)),
+            "p99_latency_s": float(np.percentile(lat, 99)),
+            "iter_us": 1e6 * r0.gpu_seconds / max(1, r0.iters),
+        },
+        "e2e": {
+            "value": e2e_value, "unit": UNIT,
+            "h2d_bytes_per_step": int(np.mean([r.h2d_bytes for r in e2e_res])),
+            "d2h_bytes_per_step": int(np.mean([r.d2h_bytes for r in e2e_res])),
+        },
+        "roofline": roof,
+        "stages": stages,
+        "cpu_baseline": cpu,
+        "gpu_launches": int(launches),
+        "clocks": ck,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    dist = Dist(args)
+    try:
+        if args.impl == "reference":
+            reference_arm(args, dist)
+        else:
+            ours(args, dist)
+    finally:
+        dist.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,1244 @@
+// api.cu -- C ABI of libeplace.so: context set-up, the device-resident
+// ElectroPlace loop (electro_place/mod.rs:65-204) and the stage entry points.
+//
+// Loop structure.  Every iteration runs on the device without host round
+// trips: WA gradient -> density scatter -> density finalise -> 4 DCT GEMM
+// launches -> fused gather/penalty/BB/FISTA step.  All loop scalars (penalty,
+// step sizes, iteration counter) live on the device, so one legalisation
+// interval (legalize_interval iterations) is captured once as a CUDA graph
+// and replayed.  After each interval the solver positions are copied to
+// pinned host memory; host threads legalise those snapshots (the greedy
+// legaliser never feeds back into the positions, only into the choice of the
+// best snapshot), while the device runs ahead.  The convergence test reads
+// the overlap of the interval's last iteration.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <condition_variable>
+#include <cstdio>
+#include <cstring>
+#include <deque>
+#include <functional>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "eplace_internal.h"
+#include "kernels.cuh"
+
+namespace eplace {
+namespace {
+
+thread_local std::string g_thread_error;
+// Host<->device bytes copied by the current call (reported in eplace_result).
+thread_local uint64_t g_h2d = 0, g_d2h = 0;
+
+struct CudaError {
+  cudaError_t e;
+  std::string where;
+};
+
+#define CK(call)                                                           \
+  do {                                                                     \
+    cudaError_t e_ = (call);                                               \
+    if (e_ != cudaSuccess) throw CudaError{e_, std::string(#call)};        \
+  } while (0)
+
+template <typename T>
+struct DBuf {
+  T *p = nullptr;
+  size_t n = 0;
+  DBuf() = default;
+  DBuf(const DBuf &) = delete;
+  DBuf &operator=(const DBuf &) = delete;
+  ~DBuf() { if (p) cudaFree(p); }
+  void alloc(size_t count) {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = count;
+    if (count) CK(cudaMalloc(&p, sizeof(T) * count));
+  }
+  void upload(const T *h, size_t count, cudaStream_t s) {
+    if (count) CK(cudaMemcpyAsync(p, h, sizeof(T) * count, cudaMemcpyHostToDevice, s));
+    g_h2d += sizeof(T) * count;
+  }
+  void zero(cudaStream_t s) {
+    if (n) CK(cudaMemsetAsync(p, 0, sizeof(T) * n, s));
+  }
+};
+
+template <typename T>
+struct PinBuf {
+  T *p = nullptr;
+  size_t n = 0;
+  PinBuf() = default;
+  PinBuf(const PinBuf &) = delete;
+  PinBuf &operator=(const PinBuf &) = delete;
+  ~PinBuf() { if (p) cudaFreeHost(p); }
+  void alloc(size_t count) {
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    n = count;
+    if (count) CK(cudaMallocHost(&p, sizeof(T) * count));
+  }
+};
+
+// Simple FIFO worker pool for the host legaliser.
+class Pool {
+ public:
+  explicit Pool(int n) {
+    for (int i = 0; i < n; ++i) th_.emplace_back([this, i] { loop(i); });
+  }
+  ~Pool() {
+    {
+      std::lock_guard<std::mutex> g(m_);
+      stop_ = true;
+    }
+    cv_.notify_all();
+    for (auto &t : th_) t.join();
+  }
+  void submit(std::function<void(int)> f) {
+    {
+      std::lock_guard<std::mutex> g(m_);
+      q_.push_back(std::move(f));
+    }
+    cv_.notify_one();
+  }
+ private:
+  void loop(int id) {
+    for (;;) {
+      std::function<void(int)> f;
+      {
+        std::unique_lock<std::mutex> g(m_);
+        cv_.wait(g, [this] { return stop_ || !q_.empty(); });
+        if (stop_ && q_.empty()) return;
+        f = std::move(q_.front());
+        q_.pop_front();
+      }
+      f(id);
+    }
+  }
+  std::vector<std::thread> th_;
+  std::deque<std::function<void(int)>> q_;
+  std::mutex m_;
+  std::condition_variable cv_;
+  bool stop_ = false;
+};
+
+}  // namespace
+}  // namespace eplace
+
+using namespace eplace;
+
+struct eplace_ctx {
+  HostProblem hp;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  int num_sms = 0;
+  int step_grid = 0;
+  std::vector<double> pw_host;
+  double total_area = 0.0;
+
+  // problem on device
+  DBuf<uint32_t> net_off, pin_cell;
+  DBuf<uint8_t> has_driver;
+  DBuf<WaTask> wa_tasks;
+  DBuf<float2> half;
+  DBuf<float> area, pw;
+  // state
+  DBuf<float2> look;  // [N + F]
+  DBuf<float2> x, xp, g, gprev, tmp_wl, tmp_den;
+  DBuf<unsigned long long> acc, dens;
+  DBuf<float> rho, T, Exh, Eyh, U, V, Ex, Ey, phi;
+  DBuf<float> mB1, mL2, mB3, mL4, mB5, mL6;  // DCT matrices (row-major operands)
+  DBuf<float> wx, gx2, wy, gy2;
+  DBuf<GemmOp> ops;                         // 0: GEMM1, 1: GEMM2, 2-3: GEMM3, 4-5: GEMM4
+  DBuf<double> mom, part;
+  DBuf<DevScalars> sc;
+  DBuf<IterLog> log;
+  DBuf<unsigned> bar;  // [0..1] grid barrier, [2] finalise ticket, [3] step ticket
+  DBuf<int2> loc;
+  DBuf<unsigned long long> hp_total;
+  size_t log_cap = 0;
+
+  ~eplace_ctx() {
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+namespace {
+
+void set_err(eplace_ctx *c, const std::string &m) {
+  if (c) c->err = m;
+  g_thread_error = m;
+}
+
+eplace_status cuda_fail(eplace_ctx *c, const CudaError &e) {
+  set_err(c, e.where + ": " + cudaGetErrorString(e.e));
+  if (e.e == cudaErrorMemoryAllocation) return EPLACE_ERR_OOM;
+  if (e.e == cudaErrorNoDevice || e.e == cudaErrorInsufficientDriver) return EPLACE_ERR_NO_DEVICE;
+  return EPLACE_ERR_CUDA;
+}
+
+// Packs whole nets into warp tasks of at most 32 pins (and 32 nets); a net
+// with more than 32 pins gets a task of its own.
+std::vector<WaTask> build_wa_tasks(const HostProblem &hp) {
+  std::vector<WaTask> t;
+  uint32_t n = 0;
+  while (n < hp.NN) {
+    const uint32_t b = hp.net_off[n];
+    const uint32_t d = hp.net_off[n + 1] - b;
+    if (d > 32) {
+      t.push_back(make_int4((int)b, (int)(b + d), (int)n, 1));
+      ++n;
+      continue;
+    }
+    uint32_t m = n, e = b;
+    while (m < hp.NN && m - n < 32) {
+      const uint32_t dd = hp.net_off[m + 1] - hp.net_off[m];
+      if (dd > 32 || (hp.net_off[m + 1] - b) > 32) break;
+      e = hp.net_off[m + 1];
+      ++m;
+    }
+    if (e > b) t.push_back(make_int4((int)b, (int)e, (int)n, (int)(m - n)));
+    n = m;
+  }
+  return t;
+}
+
+// DCT matrices as GEMM operands (rustdct conventions, density.rs:211-275).
+void build_matrices(eplace_ctx *c) {
+  const int W = c->hp.BX, H = c->hp.BY;
+  const double pi = 3.14159265358979323846;
+  std::vector<float> B1((size_t)W * W), B3((size_t)W * W), B5((size_t)W * W);
+  std::vector<float> L2((size_t)H * H), L4((size_t)H * H), L6((size_t)H * H);
+  // GEMM1  T = rho * B1,     B1[x][kx] = cos(pi kx (x + 1/2) / W)        (row DCT-II)
+  // GEMM3a U = Ex^ * B3,     B3[kx][x] = sin(pi (kx+1)(x + 1/2) / W), kx = W-1 halved (row DST-III)
+  // GEMM3b V = Ey^ * B5,     B5[kx][x] = cos(pi kx (x + 1/2) / W),    kx = 0 halved   (row DCT-III)
+  for (int a = 0; a < W; ++a)
+    for (int b = 0; b < W; ++b) {
+      B1[(size_t)a * W + b] = (float)std::cos(pi * b * (a + 0.5) / W);
+      B3[(size_t)a * W + b] = (float)(std::sin(pi * (a + 1) * (b + 0.5) / W) * (a == W - 1 ? 0.5 : 1.0));
+      B5[(size_t)a * W + b] = (float)(std::cos(pi * a * (b + 0.5) / W) * (a == 0 ? 0.5 : 1.0));
+    }
+  // GEMM2  A  = L2 * T,      L2[ky][y] = cos(pi ky (y + 1/2) / H)        (column DCT-II)
+  // GEMM4a Ex = L4 * U,      L4[y][ky] = cos(pi ky (y + 1/2) / H), ky = 0 halved   (column DCT-III)
+  // GEMM4b Ey = L6 * V,      L6[y][ky] = sin(pi (ky+1)(y + 1/2) / H), ky = H-1 halved (column DST-III)
+  for (int a = 0; a < H; ++a)
+    for (int b = 0; b < H; ++b) {
+      L2[(size_t)a * H + b] = (float)std::cos(pi * a * (b + 0.5) / H);
+      L4[(size_t)a * H + b] = (float)(std::cos(pi * b * (a + 0.5) / H) * (b == 0 ? 0.5 : 1.0));
+      L6[(size_t)a * H + b] = (float)(std::sin(pi * (b + 1) * (a + 0.5) / H) * (b == H - 1 ? 0.5 : 1.0));
+    }
+  std::vector<float> wx(W), gx2(W), wy(H), gy2(H);
+  for (int k = 0; k < W; ++k) {
+    double w = pi * k / W;
+    wx[k] = (float)w;
+    gx2[k] = (float)(2.0 * (1.0 - std::cos(w)));
+  }
+  for (int k = 0; k < H; ++k) {
+    double w = pi * k / H;
+    wy[k] = (float)w;
+    gy2[k] = (float)(2.0 * (1.0 - std::cos(w)));
+  }
+  cudaStream_t s = c->stream;
+  c->mB1.alloc(B1.size()); c->mB1.upload(B1.data(), B1.size(), s);
+  c->mB3.alloc(B3.size()); c->mB3.upload(B3.data(), B3.size(), s);
+  c->mB5.alloc(B5.size()); c->mB5.upload(B5.data(), B5.size(), s);
+  c->mL2.alloc(L2.size()); c->mL2.upload(L2.data(), L2.size(), s);
+  c->mL4.alloc(L4.size()); c->mL4.upload(L4.data(), L4.size(), s);
+  c->mL6.alloc(L6.size()); c->mL6.upload(L6.data(), L6.size(), s);
+  c->wx.alloc(W); c->wx.upload(wx.data(), W, s);
+  c->gx2.alloc(W); c->gx2.upload(gx2.data(), W, s);
+  c->wy.alloc(H); c->wy.upload(wy.data(), H, s);
+  c->gy2.alloc(H); c->gy2.upload(gy2.data(), H, s);
+  GemmOp ops[6] = {
+      {c->rho.p, c->mB1.p, c->T.p, nullptr},
+      {c->mL2.p, c->T.p, c->Exh.p, c->Eyh.p},
+      {c->Exh.p, c->mB3.p, c->U.p, nullptr},
+      {c->Eyh.p, c->mB5.p, c->V.p, nullptr},
+      {c->mL4.p, c->U.p, c->Ex.p, nullptr},
+      {c->mL6.p, c->V.p, c->Ey.p, nullptr},
+  };
+  c->ops.alloc(6);
+  c->ops.upload(ops, 6, s);
+  CK(cudaStreamSynchronize(s));
+}
+
+void ensure_log(eplace_ctx *c, size_t iters) {
+  if (c->log_cap >= iters + 2) return;
+  c->log_cap = std::max<size_t>(iters + 2, 64);
+  c->log.alloc(c->log_cap);
+  c->log.zero(c->stream);
+}
+
+int grid_for(int n, int block, int cap) {
+  long long g = ((long long)n + block - 1) / block;
+  if (g < 1) g = 1;
+  if (g > cap) g = cap;
+  return (int)g;
+}
+
+// --- kernel sequence of one iteration ------------------------------------
+void launch_wa_stage(eplace_ctx *c, float gamma) {
+  WaArgs a{c->wa_tasks.p, (int)c->wa_tasks.n, c->net_off.p, c->pin_cell.p, c->look.p, c->acc.p, c->hp.N, gamma};
+  CK(launch_wa(a, grid_for((int)c->wa_tasks.n * 32, kWaBlock, c->num_sms * 16), c->stream));
+}
+
+void launch_scatter_stage(eplace_ctx *c) {
+  const HostProblem &hp = c->hp;
+  ScatterArgs a{c->look.p, hp.any_macro ? c->half.p : nullptr, hp.N, hp.BX, hp.BY,
+                (float)hp.sx, (float)hp.sy, 1.0f / (float)hp.sx, 1.0f / (float)hp.sy, c->dens.p};
+  CK(launch_scatter(a, grid_for((int)hp.N, kScatterBlock, c->num_sms * 16), c->stream));
+}
+
+void launch_final_stage(eplace_ctx *c, double *dens_out) {
+  const HostProblem &hp = c->hp;
+  const int nb = hp.BX * hp.BY;
+  const double c0 = c->total_area / (double)nb;
+  FinalArgs a{c->dens.p, nb, (double)hp.sx * hp.sy, c0, c->rho.p, dens_out, c->part.p,
+              c->bar.p + 2, c->sc.p, c->log.p};
+  CK(launch_density_final(a, grid_for(nb, kFinalBlock, c->num_sms * 2), c->stream));
+}
+
+void launch_field_stage(eplace_ctx *c, float *phi) {
+  const int W = c->hp.BX, H = c->hp.BY;
+  SpectralArgs sp{c->wx.p, c->gx2.p, c->wy.p, c->gy2.p, (float)(4.0 / ((double)W * H)), phi};
+  CK(launch_sgemm(c->ops.p + 0, 1, H, W, W, c->stream));
+  CK(launch_sgemm_spectral(c->ops.p + 1, H, W, H, sp, c->stream));
+  CK(launch_sgemm(c->ops.p + 2, 2, H, W, W, c->stream));
+  CK(launch_sgemm(c->ops.p + 4, 2, H, W, H, c->stream));
+}
+
+StepArgs step_args(eplace_ctx *c) {
+  const HostProblem &hp = c->hp;
+  StepArgs a{};
+  a.N = hp.N;
+  a.BX = hp.BX;
+  a.BY = hp.BY;
+  a.sx = (float)hp.sx;
+  a.sy = (float)hp.sy;
+  a.inv_sx = 1.0f / (float)hp.sx;
+  a.inv_sy = 1.0f / (float)hp.sy;
+  a.maxx = (float)(hp.W - 1);
+  a.maxy = (float)(hp.H - 1);
+  a.look = c->look.p;
+  a.half = hp.any_macro ? c->half.p : nullptr;
+  a.area = hp.any_macro ? c->area.p : nullptr;
+  a.pw = c->pw.p;
+  a.acc = c->acc.p;
+  a.Ex = c->Ex.p;
+  a.Ey = c->Ey.p;
+  a.x = c->x.p;
+  a.xp = c->xp.p;
+  a.g = c->g.p;
+  a.gprev = c->gprev.p;
+  a.tmp_wl = c->tmp_wl.p;
+  a.tmp_den = c->tmp_den.p;
+  a.mom = c->mom.p;
+  a.sc = c->sc.p;
+  a.log = c->log.p;
+  a.part = c->part.p;
+  a.bar = c->bar.p;
+  a.ticket = c->bar.p + 3;
+  a.mode = 0;
+  return a;
+}
+
+void launch_step_stage(eplace_ctx *c) {
+  StepArgs a = step_args(c);
+  CK(launch_step(a, c->step_grid, c->stream));
+}
+
+void launch_iteration(eplace_ctx *c, float gamma) {
+  launch_wa_stage(c, gamma);
+  launch_scatter_stage(c);
+  launch_final_stage(c, nullptr);
+  launch_field_stage(c, nullptr);
+  launch_step_stage(c);
+}
+
+constexpr int kLaunchesPerIter = 8;
+
+void upload_momentum(eplace_ctx *c, uint64_t iters) {
+  // FISTA sequence a_0 = 1, a_{k+1} = (1 + sqrt(1 + 4 a_k^2)) / 2; the
+  // look-ahead and the step of iteration k both use m_k = (a_k - 1) / a_{k+1}
+  // (nesterov.rs:41-64, :75-82; m_0 = 0).
+  std::vector<double> m(iters + 2);
+  double a = 1.0;
+  for (size_t k = 0; k < m.size(); ++k) {
+    double an = (1.0 + std::sqrt(1.0 + 4.0 * a * a)) / 2.0;
+    m[k] = (a - 1.0) / an;
+    a = an;
+  }
+  if (c->mom.n < m.size()) c->mom.alloc(m.size());
+  c->mom.upload(m.data(), m.size(), c->stream);
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+int32_t eplace_abi_version(void) { return EPLACE_ABI_VERSION; }
+
+void eplace_cfg_default(eplace_cfg *c) {
+  if (!c) return;
+  c->seed = 1;
+  c->wl_coeff = 0.5;
+  c->target_util = 0.7;
+  c->timing_driven = 0;
+  c->target_density = 1.0;
+  c->timing_weight = 0.0;
+  c->nesterov_step_size = 0.1;
+  c->max_iters = 500;
+  c->legalize_interval = 5;
+}
+
+void eplace_opts_default(eplace_opts *o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof(*o));
+  o->dct_mode = EPLACE_DCT_FP32_SIMT;
+  o->legal_threads = 0;
+  o->use_graphs = 1;
+  o->verbose = 0;
+  o->max_inflight = 3;
+}
+
+size_t eplace_last_error(const eplace_ctx *ctx, char *buf, size_t len) {
+  const std::string &m = ctx ? ctx->err : g_thread_error;
+  if (buf && len) {
+    size_t k = std::min(len - 1, m.size());
+    std::memcpy(buf, m.data(), k);
+    buf[k] = 0;
+  }
+  return m.size();
+}
+
+eplace_status eplace_ctx_create(const eplace_netlist *nl, const eplace_chip *chip, int32_t device,
+                                eplace_ctx **out) {
+  if (!out) return EPLACE_ERR_INVALID;
+  *out = nullptr;
+  std::unique_ptr<eplace_ctx> c(new eplace_ctx());
+  std::string msg;
+  eplace_status st = load_problem(nl, chip, c->hp, msg);
+  if (st != EPLACE_OK) {
+    set_err(nullptr, msg);
+    return st;
+  }
+  try {
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+      set_err(nullptr, "no CUDA device");
+      return EPLACE_ERR_NO_DEVICE;
+    }
+    if (device < 0 || device >= ndev) {
+      set_err(nullptr, "device index out of range");
+      return EPLACE_ERR_INVALID;
+    }
+    c->device = device;
+    CK(cudaSetDevice(device));
+    int major = 0;
+    CK(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device));
+    if (major != 10) {
+      set_err(nullptr, "this library is built for sm_100a (B200) only");
+      return EPLACE_ERR_NO_DEVICE;
+    }
+    CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    CK(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device));
+    const HostProblem &hp = c->hp;
+    cudaStream_t s = c->stream;
+    c->net_off.alloc(hp.net_off.size());
+    c->net_off.upload(hp.net_off.data(), hp.net_off.size(), s);
+    c->pin_cell.alloc(hp.P);
+    c->pin_cell.upload(hp.pin_cell.data(), hp.P, s);
+    c->has_driver.alloc(hp.NN);
+    c->has_driver.upload(hp.has_driver.data(), hp.NN, s);
+    std::vector<WaTask> tasks = build_wa_tasks(hp);
+    c->wa_tasks.alloc(tasks.size());
+    c->wa_tasks.upload(tasks.data(), tasks.size(), s);
+    std::vector<float2> half(hp.N);
+    std::vector<float> area(hp.N);
+    double tot = 0.0;
+    for (uint32_t i = 0; i < hp.N; ++i) {
+      half[i] = make_float2(0.5f * hp.cw[i], 0.5f * hp.ch[i]);
+      area[i] = (float)(hp.cw[i] * hp.ch[i]);
+      tot += area[i];
+    }
+    c->total_area = tot;
+    c->half.alloc(hp.N);
+    c->half.upload(half.data(), hp.N, s);
+    c->area.alloc(hp.N);
+    c->area.upload(area.data(), hp.N, s);
+    pin_weights(hp, c->pw_host);
+    std::vector<float> pwf(c->pw_host.begin(), c->pw_host.end());
+    c->pw.alloc(hp.N);
+    c->pw.upload(pwf.data(), hp.N, s);
+    c->look.alloc((size_t)hp.N + hp.F);
+    std::vector<float2> fixed(hp.F);
+    for (uint32_t f = 0; f < hp.F; ++f) fixed[f] = make_float2((float)hp.fx[f], (float)hp.fy[f]);
+    if (hp.F) CK(cudaMemcpyAsync(c->look.p + hp.N, fixed.data(), sizeof(float2) * hp.F, cudaMemcpyHostToDevice, s));
+    g_h2d += sizeof(float2) * hp.F;
+    for (auto *b : {&c->x, &c->xp, &c->g, &c->gprev, &c->tmp_wl, &c->tmp_den}) b->alloc(hp.N);
+    c->acc.alloc(2 * (size_t)hp.N);
+    c->acc.zero(s);
+    const size_t nb = (size_t)hp.BX * hp.BY;
+    c->dens.alloc(nb);
+    c->dens.zero(s);
+    for (auto *b : {&c->rho, &c->T, &c->Exh, &c->Eyh, &c->U, &c->V, &c->Ex, &c->Ey}) b->alloc(nb);
+    build_matrices(c.get());
+    c->step_grid = std::max(1, std::min(step_max_grid(device), grid_for((int)hp.N, kStepBlock, 1 << 30)));
+    c->part.alloc(4 * (size_t)std::max(c->step_grid, c->num_sms * 2) + 8);
+    c->sc.alloc(1);
+    c->bar.alloc(4);
+    c->bar.zero(s);
+    c->loc.alloc((size_t)hp.N + hp.F);
+    std::vector<int2> floc(hp.F);
+    for (uint32_t f = 0; f < hp.F; ++f) floc[f] = make_int2(hp.fx[f], hp.fy[f]);
+    if (hp.F) CK(cudaMemcpyAsync(c->loc.p + hp.N, floc.data(), sizeof(int2) * hp.F, cudaMemcpyHostToDevice, s));
+    g_h2d += sizeof(int2) * hp.F;
+    c->hp_total.alloc(1);
+    ensure_log(c.get(), 8);
+    CK(cudaStreamSynchronize(s));
+  } catch (const CudaError &e) {
+    return cuda_fail(nullptr, e);
+  }
+  *out = c.release();
+  return EPLACE_OK;
+}
+
+void eplace_ctx_destroy(eplace_ctx *ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  delete ctx;
+}
+
+// Resets the loop state on the device for a new run from positions (sx, sy).
+static void reset_state(eplace_ctx *c, const std::vector<int32_t> &sx, const std::vector<int32_t> &sy,
+                        const eplace_cfg *cfg) {
+  const HostProblem &hp = c->hp;
+  cudaStream_t s = c->stream;
+  std::vector<float2> p(hp.N);
+  for (uint32_t i = 0; i < hp.N; ++i) p[i] = make_float2((float)sx[i], (float)sy[i]);
+  c->x.upload(p.data(), hp.N, s);
+  c->xp.upload(p.data(), hp.N, s);
+  CK(cudaMemcpyAsync(c->look.p, p.data(), sizeof(float2) * hp.N, cudaMemcpyHostToDevice, s));
+  g_h2d += sizeof(float2) * hp.N;
+  c->gprev.zero(s);
+  c->g.zero(s);
+  c->acc.zero(s);
+  c->dens.zero(s);
+  DevScalars sc{};
+  sc.lam = 0.0;
+  sc.step[0] = sc.step[1] = cfg->nesterov_step_size;
+  sc.overlap = 0.0;
+  sc.lam_init = 0;
+  sc.iter = 0;
+  sc.err = 0;
+  c->sc.upload(&sc, 1, s);
+  c->bar.zero(s);
+  CK(cudaStreamSynchronize(s));
+}
+
+namespace {
+struct Checkpoint {
+  int32_t iter = -1;
+  std::vector<float> xs, ys;
+  std::vector<int32_t> sx, sy;
+  double disp = 0.0;
+  int64_t hpwl = 0;
+  eplace_status st = EPLACE_OK;
+  std::atomic<bool> done{false};
+};
+}  // namespace
+
+eplace_status eplace_run(eplace_ctx *c, const eplace_cfg *cfg, const eplace_opts *opts_in,
+                         eplace_result *res) {
+  if (!c || !cfg || !res) return EPLACE_ERR_INVALID;
+  const auto t_start = std::chrono::steady_clock::now();
+  const uint64_t h2d0 = g_h2d, d2h0 = g_d2h;
+  eplace_opts opts;
+  eplace_opts_default(&opts);
+  if (opts_in) opts = *opts_in;
+  const HostProblem &hp = c->hp;
+  res->traj_len = 0;
+  res->iters = 0;
+  res->best_iter = -1;
+  res->converged = 0;
+  res->hpwl = 0;
+  res->overlap = 0.0;
+  res->gpu_seconds = 0.0;
+  res->gpu_launches = 0;
+  if (cfg->legalize_interval == 0) {
+    set_err(c, "legalize_interval must be positive");
+    return EPLACE_ERR_INVALID;
+  }
+  if (!(cfg->wl_coeff > 0) || !std::isfinite(cfg->wl_coeff) || !std::isfinite(cfg->nesterov_step_size)) {
+    set_err(c, "wl_coeff / nesterov_step_size must be finite (wl_coeff > 0)");
+    return EPLACE_ERR_INVALID;
+  }
+  if (opts.dct_mode != EPLACE_DCT_FP32_SIMT) {
+    set_err(c, "dct_mode not available in this build");
+    return EPLACE_ERR_INVALID;
+  }
+  if (!res->bel_tile && hp.N) return EPLACE_ERR_INVALID;
+  std::string msg;
+  std::vector<int32_t> isx, isy;
+  eplace_status st = initial_placement(hp, cfg->seed, isx, isy, msg);
+  if (st != EPLACE_OK) {
+    set_err(c, msg);
+    return st;
+  }
+  if (hp.N == 0) {  // mod.rs:80-82
+    res->total_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+    return EPLACE_OK;
+  }
+  const uint64_t max_iters = cfg->max_iters;
+  const uint64_t interval = cfg->legalize_interval;
+  int nthreads = opts.legal_threads > 0 ? opts.legal_threads : (int)std::max(1u, std::thread::hardware_concurrency());
+  nthreads = std::min(nthreads, 64);
+  std::vector<std::unique_ptr<Checkpoint>> cps;
+  std::vector<std::unique_ptr<Legalizer>> legal;
+  std::unique_ptr<Pool> pool;
+  cudaGraphExec_t gexec = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::vector<cudaEvent_t> evs;
+  eplace_status final_st = EPLACE_OK;
+  try {
+    CK(cudaSetDevice(c->device));
+    cudaStream_t s = c->stream;
+    ensure_log(c, max_iters);
+    upload_momentum(c, max_iters);
+    reset_state(c, isx, isy, cfg);
+    for (int i = 0; i < nthreads; ++i) legal.emplace_back(new Legalizer(hp));
+    pool.reset(new Pool(nthreads));
+    const float gamma = (float)cfg->wl_coeff;
+    CK(cudaEventCreate(&ev0));
+    CK(cudaEventCreate(&ev1));
+
+    // Interval boundaries: iterations k with k % interval == 0, plus the last.
+    struct Chunk {
+      uint64_t first, last;
+    };
+    std::vector<Chunk> chunks;
+    {
+      uint64_t k = 0;
+      while (k < max_iters) {
+        uint64_t last = (k == 0) ? 0 : std::min(max_iters - 1, ((k + interval - 1) / interval) * interval);
+        if (last < k) last = max_iters - 1;
+        chunks.push_back({k, last});
+        k = last + 1;
+      }
+    }
+    // Pinned snapshot ring.
+    const int inflight = std::max(1, std::min(opts.max_inflight, 8));
+    std::vector<std::unique_ptr<PinBuf<float2>>> snaps(inflight);
+    std::vector<std::unique_ptr<PinBuf<IterLog>>> logs(inflight);
+    std::vector<std::unique_ptr<PinBuf<DevScalars>>> scs(inflight);
+    for (int i = 0; i < inflight; ++i) {
+      snaps[i].reset(new PinBuf<float2>());
+      snaps[i]->alloc(hp.N);
+      logs[i].reset(new PinBuf<IterLog>());
+      logs[i]->alloc(interval + 1);
+      scs[i].reset(new PinBuf<DevScalars>());
+      scs[i]->alloc(1);
+      cudaEvent_t e;
+      CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      evs.push_back(e);
+    }
+    bool use_graph = opts.use_graphs != 0 && interval > 1;
+    uint64_t launched_iters = 0;
+    auto launch_chunk = [&](const Chunk &ch) {
+      uint64_t n = ch.last - ch.first + 1;
+      launched_iters += n;
+      if (use_graph && n == interval) {
+        if (!gexec) {
+          CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+          bool ok = true;
+          try {
+            for (uint64_t k = 0; k < n; ++k) launch_iteration(c, gamma);
+          } catch (const CudaError &) {
+            ok = false;
+          }
+          cudaError_t ce = cudaStreamEndCapture(s, &graph);
+          if (!ok || ce != cudaSuccess || cudaGraphInstantiate(&gexec, graph, 0) != cudaSuccess) {
+            // Capture not available (e.g. cooperative nodes): plain launches.
+            cudaGetLastError();
+            if (graph) cudaGraphDestroy(graph);
+            graph = nullptr;
+            gexec = nullptr;
+            use_graph = false;
+            for (uint64_t k = 0; k < n; ++k) launch_iteration(c, gamma);
+            return;
+          }
+        }
+        CK(cudaGraphLaunch(gexec, s));
+      } else {
+        for (uint64_t k = 0; k < n; ++k) launch_iteration(c, gamma);
+      }
+    };
+
+    std::deque<std::pair<size_t, int>> pending;  // (chunk index, slot)
+    size_t next_chunk = 0;
+    bool stop = false;
+    size_t converged_chunk = chunks.size();
+    uint64_t iters_done = 0;
+    double last_overlap = 0.0;
+    std::vector<IterLog> iterlog;
+    // Fold legalised checkpoints in iteration order (record_metric,
+    // common.rs:485-495: strict '<' keeps the first best); the positions
+    // and bindings of every checkpoint but the current best are released.
+    Checkpoint *best = nullptr;
+    double best_metric = INFINITY;
+    size_t fold_next = 0;
+    auto fold = [&]() {
+      while (fold_next < cps.size() && final_st == EPLACE_OK) {
+        Checkpoint *cp = cps[fold_next].get();
+        if (!cp->done.load(std::memory_order_acquire)) break;
+        ++fold_next;
+        if (cp->st != EPLACE_OK) {
+          final_st = cp->st;
+          set_err(c, "logic");
+          break;
+        }
+        const IterLog &L = iterlog[cp->iter];
+        if (res->traj && res->traj_len < res->traj_capacity) {
+          eplace_traj_entry &t = res->traj[res->traj_len++];
+          t.iter = cp->iter;
+          t.hpwl = (double)cp->hpwl;
+          t.displacement = cp->disp;
+          t.step_x = L.step_norm[0];
+          t.step_y = L.step_norm[1];
+          t.density_penalty = L.lam;
+          t.overlap = L.overlap;
+        }
+        if (opts.verbose) {
+          std::fprintf(stderr,
+                       "ElectroPlace iter %d: HPWL=%.0f, disp=%.1f, step=(%.4f,%.4f), density_p=%.3f, overlap=%.4f\n",
+                       cp->iter, (double)cp->hpwl, cp->disp, L.step_norm[0], L.step_norm[1], L.lam, L.overlap);
+        }
+        Checkpoint *drop = cp;
+        if ((double)cp->hpwl < best_metric) {
+          best_metric = (double)cp->hpwl;
+          drop = best;
+          best = cp;
+        }
+        if (drop) {
+          std::vector<float>().swap(drop->xs);
+          std::vector<float>().swap(drop->ys);
+          std::vector<int32_t>().swap(drop->sx);
+          std::vector<int32_t>().swap(drop->sy);
+        }
+      }
+    };
+    CK(cudaEventRecord(ev0, s));
+    int slot_rr = 0;
+    while ((!stop && next_chunk < chunks.size()) || !pending.empty()) {
+      while (!stop && next_chunk < chunks.size() && (int)pending.size() < inflight) {
+        const Chunk &ch = chunks[next_chunk];
+        launch_chunk(ch);
+        const int slot = slot_rr;
+        slot_rr = (slot_rr + 1) % inflight;
+        CK(cudaMemcpyAsync(snaps[slot]->p, c->x.p, sizeof(float2) * hp.N, cudaMemcpyDeviceToHost, s));
+        const uint64_t n = ch.last - ch.first + 1;
+        CK(cudaMemcpyAsync(logs[slot]->p, c->log.p + ch.first, sizeof(IterLog) * n, cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(scs[slot]->p, c->sc.p, sizeof(DevScalars), cudaMemcpyDeviceToHost, s));
+        g_d2h += sizeof(float2) * hp.N + sizeof(IterLog) * n + sizeof(DevScalars);
+        CK(cudaEventRecord(evs[slot], s));
+        pending.push_back({next_chunk, slot});
+        ++next_chunk;
+      }
+      if (pending.empty()) break;
+      auto [ci, slot] = pending.front();
+      pending.pop_front();
+      CK(cudaEventSynchronize(evs[slot]));
+      if (stop) continue;  // ran ahead of convergence: discard
+      const Chunk &ch = chunks[ci];
+      if (scs[slot]->p->err) {
+        set_err(c, "a bounded device wait timed out");
+        final_st = EPLACE_ERR_TIMEOUT;
+        stop = true;
+        continue;
+      }
+      const uint64_t n = ch.last - ch.first + 1;
+      for (uint64_t k = 0; k < n; ++k) iterlog.push_back(logs[slot]->p[k]);
+      iters_done = ch.last + 1;
+      const IterLog &L = logs[slot]->p[n - 1];
+      last_overlap = L.overlap;
+      // Legalise this checkpoint on the host pool (mod.rs:176-183).
+      auto cp = std::make_unique<Checkpoint>();
+      cp->iter = (int32_t)ch.last;
+      cp->xs.resize(hp.N);
+      cp->ys.resize(hp.N);
+      for (uint32_t i = 0; i < hp.N; ++i) {
+        cp->xs[i] = snaps[slot]->p[i].x;
+        cp->ys[i] = snaps[slot]->p[i].y;
+      }
+      Checkpoint *raw = cp.get();
+      cps.push_back(std::move(cp));
+      pool->submit([raw, &legal, &hp](int tid) {
+        raw->sx.resize(hp.N);
+        raw->sy.resize(hp.N);
+        raw->st = legal[tid]->run(raw->xs.data(), raw->ys.data(), raw->sx.data(), raw->sy.data(), &raw->disp);
+        if (raw->st == EPLACE_OK) raw->hpwl = hpwl_host(hp, raw->sx.data(), raw->sy.data());
+        raw->done.store(true, std::memory_order_release);
+      });
+      // Convergence (mod.rs:190-195).
+      if (ch.last >= 20 && L.overlap < 0.1) {
+        stop = true;
+        converged_chunk = ci;
+      }
+      fold();
+      if (final_st != EPLACE_OK) stop = true;
+    }
+    CK(cudaEventRecord(ev1, s));
+    CK(cudaStreamSynchronize(s));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, ev0, ev1));
+    res->gpu_seconds = ms * 1e-3;
+    res->gpu_launches = (uint64_t)kLaunchesPerIter * launched_iters;
+    res->iters = (uint32_t)iters_done;
+    res->converged = converged_chunk < chunks.size() ? 1 : 0;
+    res->overlap = last_overlap;
+    // Wait for the legaliser, then fold the remaining checkpoints.
+    pool.reset();
+    fold();
+    if (final_st == EPLACE_OK) {
+      if (opts.verbose && res->converged)
+        std::fprintf(stderr, "ElectroPlace converged at iteration %d (overlap %.4f < 0.1)\n",
+                     (int)(iters_done - 1), last_overlap);
+      // Final legalisation of the best snapshot (mod.rs:199).  Its result is
+      // the checkpoint's own binding: legalisation is a pure function of the
+      // positions and the fixed cells.
+      std::vector<int32_t> fsx(hp.N), fsy(hp.N);
+      std::vector<float> bx(hp.N), by(hp.N);
+      if (best) {
+        fsx = best->sx;
+        fsy = best->sy;
+        bx = best->xs;
+        by = best->ys;
+        res->best_iter = best->iter;
+      } else {
+        for (uint32_t i = 0; i < hp.N; ++i) {
+          bx[i] = (float)isx[i];
+          by[i] = (float)isy[i];
+        }
+        double d = 0.0;
+        eplace_status ls = legal[0]->run(bx.data(), by.data(), fsx.data(), fsy.data(), &d);
+        if (ls != EPLACE_OK) {
+          final_st = ls;
+          set_err(c, "logic");
+        }
+      }
+      if (final_st == EPLACE_OK) {
+        for (uint32_t i = 0; i < hp.N; ++i) {
+          res->bel_tile[i] = fsy[i] * hp.W + fsx[i];
+          if (res->bel_index) res->bel_index[i] = 0;
+          if (res->x) res->x[i] = bx[i];
+          if (res->y) res->y[i] = by[i];
+        }
+        res->hpwl = hpwl_host(hp, fsx.data(), fsy.data());
+      }
+    }
+  } catch (const CudaError &e) {
+    final_st = cuda_fail(c, e);
+  }
+  pool.reset();
+  if (gexec) cudaGraphExecDestroy(gexec);
+  if (graph) cudaGraphDestroy(graph);
+  if (ev0) cudaEventDestroy(ev0);
+  if (ev1) cudaEventDestroy(ev1);
+  for (auto e : evs) cudaEventDestroy(e);
+  res->total_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+  res->h2d_bytes = g_h2d - h2d0;
+  res->d2h_bytes = g_d2h - d2h0;
+  return final_st;
+}
+
+eplace_status eplace_place(const eplace_netlist *nl, const eplace_chip *chip, const eplace_cfg *cfg,
+                           const eplace_opts *opts, int32_t device, eplace_result *res) {
+  const uint64_t h2d0 = g_h2d, d2h0 = g_d2h;
+  const auto t0 = std::chrono::steady_clock::now();
+  eplace_ctx *c = nullptr;
+  eplace_status st = eplace_ctx_create(nl, chip, device, &c);
+  if (st != EPLACE_OK) return st;
+  st = eplace_run(c, cfg, opts, res);
+  if (st != EPLACE_OK) g_thread_error = c->err;
+  eplace_ctx_destroy(c);
+  if (res) {
+    res->h2d_bytes = g_h2d - h2d0;
+    res->d2h_bytes = g_d2h - d2h0;
+    res->total_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  }
+  return st;
+}
+
+eplace_status eplace_profile_stages(eplace_ctx *c, const eplace_cfg *cfg, int32_t dct_mode, uint32_t reps,
+                                    double *stage_ms) {
+  if (!c || !cfg || !stage_ms || reps == 0) return EPLACE_ERR_INVALID;
+  if (dct_mode != EPLACE_DCT_FP32_SIMT) {
+    set_err(c, "dct_mode not available in this build");
+    return EPLACE_ERR_INVALID;
+  }
+  const HostProblem &hp = c->hp;
+  if (hp.N == 0) return EPLACE_ERR_INVALID;
+  std::vector<cudaEvent_t> ev(9, nullptr);
+  eplace_status st = EPLACE_OK;
+  try {
+    CK(cudaSetDevice(c->device));
+    std::string msg;
+    std::vector<int32_t> isx, isy;
+    st = initial_placement(hp, cfg->seed, isx, isy, msg);
+    if (st != EPLACE_OK) {
+      set_err(c, msg);
+      return st;
+    }
+    ensure_log(c, reps);
+    upload_momentum(c, reps);
+    reset_state(c, isx, isy, cfg);
+    for (auto &e : ev) CK(cudaEventCreate(&e));
+    const float gamma = (float)cfg->wl_coeff;
+    const int W = hp.BX, H = hp.BY;
+    SpectralArgs sp{c->wx.p, c->gx2.p, c->wy.p, c->gy2.p, (float)(4.0 / ((double)W * H)), nullptr};
+    double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    cudaStream_t s = c->stream;
+    for (uint32_t r = 0; r < reps; ++r) {
+      CK(cudaEventRecord(ev[0], s));
+      launch_wa_stage(c, gamma);
+      CK(cudaEventRecord(ev[1], s));
+      launch_scatter_stage(c);
+      CK(cudaEventRecord(ev[2], s));
+      launch_final_stage(c, nullptr);
+      CK(cudaEventRecord(ev[3], s));
+      CK(launch_sgemm(c->ops.p + 0, 1, H, W, W, s));
+      CK(cudaEventRecord(ev[4], s));
+      CK(launch_sgemm_spectral(c->ops.p + 1, H, W, H, sp, s));
+      CK(cudaEventRecord(ev[5], s));
+      CK(launch_sgemm(c->ops.p + 2, 2, H, W, W, s));
+      CK(cudaEventRecord(ev[6], s));
+      CK(launch_sgemm(c->ops.p + 4, 2, H, W, H, s));
+      CK(cudaEventRecord(ev[7], s));
+      launch_step_stage(c);
+      CK(cudaEventRecord(ev[8], s));
+      CK(cudaEventSynchronize(ev[8]));
+      for (int k = 0; k < 8; ++k) {
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, ev[k], ev[k + 1]));
+        acc[k] += ms;
+      }
+    }
+    for (int k = 0; k < 8; ++k) stage_ms[k] = acc[k] / reps;
+  } catch (const CudaError &e) {
+    st = cuda_fail(c, e);
+  }
+  for (auto e : ev)
+    if (e) cudaEventDestroy(e);
+  return st;
+}
+
+// ---------------------------------------------------------------------------
+// Stage entry points (host buffers in/out, one kernel family each).
+// ---------------------------------------------------------------------------
+static void upload_look(eplace_ctx *c, const float *x, const float *y) {
+  std::vector<float2> p(c->hp.N);
+  for (uint32_t i = 0; i < c->hp.N; ++i) p[i] = make_float2(x[i], y[i]);
+  if (c->hp.N) CK(cudaMemcpyAsync(c->look.p, p.data(), sizeof(float2) * c->hp.N, cudaMemcpyHostToDevice, c->stream));
+}
+
+eplace_status eplace_stage_wa_grad(eplace_ctx *c, double wl_coeff, const float *x, const float *y, float *gx,
+                                   float *gy) {
+  if (!c || (c->hp.N && (!x || !y || !gx || !gy))) return EPLACE_ERR_INVALID;
+  try {
+    CK(cudaSetDevice(c->device));
+    upload_look(c, x, y);
+    c->acc.zero(c->stream);
+    launch_wa_stage(c, (float)wl_coeff);
+    std::vector<long long> acc(2 * (size_t)c->hp.N);
+    if (c->hp.N)
+      CK(cudaMemcpyAsync(acc.data(), c->acc.p, sizeof(long long) * acc.size(), cudaMemcpyDeviceToHost, c->stream));
+    c->acc.zero(c->stream);
+    CK(cudaStreamSynchronize(c->stream));
+    for (uint32_t i = 0; i < c->hp.N; ++i) {
+      gx[i] = (float)((double)acc[2 * i] * kFixInv);
+      gy[i] = (float)((double)acc[2 * i + 1] * kFixInv);
+    }
+  } catch (const CudaError &e) {
+    return cuda_fail(c, e);
+  }
+  return EPLACE_OK;
+}
+
+eplace_status eplace_stage_density(eplace_ctx *c, const float *x, const float *y, double *density,
+                                   double *overlap) {
+  if (!c || !density || (c->hp.N && (!x || !y))) return EPLACE_ERR_INVALID;
+  try {
+    CK(cudaSetDevice(c->device));
+    const size_t nb = (size_t)c->hp.BX * c->hp.BY;
+    DBuf<double> dout;
+    dout.alloc(nb);
+    DevScalars sc{};
+    c->sc.upload(&sc, 1, c->stream);
+    upload_look(c, x, y);
+    c->dens.zero(c->stream);
+    launch_scatter_stage(c);
+    launch_final_stage(c, dout.p);
+    CK(cudaMemcpyAsync(density, dout.p, sizeof(double) * nb, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(&sc, c->sc.p, sizeof(sc), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (overlap) *overlap = sc.overlap;
+  } catch (const CudaError &e) {
+    return cuda_fail(c, e);
+  }
+  return EPLACE_OK;
+}
+
+eplace_status eplace_stage_field(eplace_ctx *c, const double *density, int32_t dct_mode, float *ex, float *ey,
+                                 float *phi_hat) {
+  if (!c || !density || !ex || !ey) return EPLACE_ERR_INVALID;
+  if (dct_mode != EPLACE_DCT_FP32_SIMT) {
+    set_err(c, "dct_mode not available in this build");
+    return EPLACE_ERR_INVALID;
+  }
+  try {
+    CK(cudaSetDevice(c->device));
+    const size_t nb = (size_t)c->hp.BX * c->hp.BY;
+    const double c0 = c->total_area / (double)nb;
+    std::vector<float> rho(nb);
+    for (size_t i = 0; i < nb; ++i) rho[i] = (float)(density[i] - c0);
+    c->rho.upload(rho.data(), nb, c->stream);
+    DBuf<float> phi;
+    if (phi_hat) phi.alloc(nb);
+    launch_field_stage(c, phi_hat ? phi.p : nullptr);
+    CK(cudaMemcpyAsync(ex, c->Ex.p, sizeof(float) * nb, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(ey, c->Ey.p, sizeof(float) * nb, cudaMemcpyDeviceToHost, c->stream));
+    if (phi_hat) CK(cudaMemcpyAsync(phi_hat, phi.p, sizeof(float) * nb, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  } catch (const CudaError &e) {
+    return cuda_fail(c, e);
+  }
+  return EPLACE_OK;
+}
+
+eplace_status eplace_stage_gather(eplace_ctx *c, const float *x, const float *y, const float *ex, const float *ey,
+                                  float *gx, float *gy) {
+  // The gather is fused into the step kernel; mode 1 of that kernel stops
+  // after the gather and leaves the density gradient in its scratch buffer.
+  if (!c || !ex || !ey || (c->hp.N && (!x || !y || !gx || !gy))) return EPLACE_ERR_INVALID;
+  try {
+    CK(cudaSetDevice(c->device));
+    const HostProblem &hp = c->hp;
+    const size_t nb = (size_t)hp.BX * hp.BY;
+    upload_look(c, x, y);
+    c->Ex.upload(ex, nb, c->stream);
+    c->Ey.upload(ey, nb, c->stream);
+    StepArgs a = step_args(c);
+    a.mode = 1;
+    CK(launch_step(a, c->step_grid, c->stream));
+    std::vector<float2> t(hp.N);
+    if (hp.N) CK(cudaMemcpyAsync(t.data(), c->tmp_den.p, sizeof(float2) * hp.N, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    for (uint32_t i = 0; i < hp.N; ++i) {
+      gx[i] = t[i].x;
+      gy[i] = t[i].y;
+    }
+  } catch (const CudaError &e) {
+    return cuda_fail(c, e);
+  }
+  return EPLACE_OK;
+}
+
+static std::vector<float2> pack2(const float *a, const float *b, size_t n) {
+  std::vector<float2> v(n);
+  for (size_t i = 0; i < n; ++i) v[i] = make_float2(a[i], b[i]);
+  return v;
+}
+
+static void unpack2(const std::vector<float2> &v, float *a, float *b) {
+  for (size_t i = 0; i < v.size(); ++i) {
+    a[i] = v[i].x;
+    b[i] = v[i].y;
+  }
+}
+
+eplace_status eplace_stage_step(eplace_ctx *c, uint64_t iter, const float *look_x, const float *look_y,
+                                const float *gwl_x, const float *gwl_y, const float *ex, const float *ey,
+                                float *x, float *y, float *x_prev, float *y_prev, float *gprev_x,
+                                float *gprev_y, double *scal, double *out, float *next_look_x,
+                                float *next_look_y) {
+  const uint32_t N = c ? c->hp.N : 0;
+  if (!c || !ex || !ey || !scal || !out) return EPLACE_ERR_INVALID;
+  if (N && (!look_x || !look_y || !gwl_x || !gwl_y || !x || !y || !x_prev || !y_prev || !gprev_x || !gprev_y ||
+            !next_look_x || !next_look_y))
+    return EPLACE_ERR_INVALID;
+  try {
+    CK(cudaSetDevice(c->device));
+    const HostProblem &hp = c->hp;
+    const size_t nb = (size_t)hp.BX * hp.BY;
+    cudaStream_t s = c->stream;
+    ensure_log(c, iter + 2);
+    upload_momentum(c, iter + 2);
+    upload_look(c, look_x, look_y);
+    c->Ex.upload(ex, nb, s);
+    c->Ey.upload(ey, nb, s);
+    std::vector<long long> acc(2 * (size_t)N);
+    for (uint32_t i = 0; i < N; ++i) {
+      acc[2 * i] = llrint((double)gwl_x[i] * kFixScale);
+      acc[2 * i + 1] = llrint((double)gwl_y[i] * kFixScale);
+    }
+    if (N) CK(cudaMemcpyAsync(c->acc.p, acc.data(), sizeof(long long) * acc.size(), cudaMemcpyHostToDevice, s));
+    std::vector<float2> vx = pack2(x, y, N), vxp = pack2(x_prev, y_prev, N), vg = pack2(gprev_x, gprev_y, N);
+    c->x.upload(vx.data(), N, s);
+    c->xp.upload(vxp.data(), N, s);
+    c->gprev.upload(vg.data(), N, s);
+    DevScalars sc{};
+    sc.lam = scal[0];
+    sc.lam_init = scal[1] != 0.0;
+    sc.step[0] = scal[2];
+    sc.step[1] = scal[3];
+    sc.iter = (int32_t)iter;
+    c->sc.upload(&sc, 1, s);
+    c->bar.zero(s);
+    launch_step_stage(c);
+    std::vector<float2> lk(N);
+    if (N) {
+      CK(cudaMemcpyAsync(vx.data(), c->x.p, sizeof(float2) * N, cudaMemcpyDeviceToHost, s));
+      CK(cudaMemcpyAsync(vxp.data(), c->xp.p, sizeof(float2) * N, cudaMemcpyDeviceToHost, s));
+      CK(cudaMemcpyAsync(vg.data(), c->gprev.p, sizeof(float2) * N, cudaMemcpyDeviceToHost, s));
+      CK(cudaMemcpyAsync(lk.data(), c->look.p, sizeof(float2) * N, cudaMemcpyDeviceToHost, s));
+    }
+    IterLog L{};
+    CK(cudaMemcpyAsync(&L, c->log.p + iter, sizeof(L), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(&sc, c->sc.p, sizeof(sc), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (sc.err) {
+      set_err(c, "a bounded device wait timed out");
+      return EPLACE_ERR_TIMEOUT;
+    }
+    unpack2(vx, x, y);
+    unpack2(vxp, x_prev, y_prev);
+    unpack2(vg, gprev_x, gprev_y);
+    unpack2(lk, next_look_x, next_look_y);
+    scal[0] = sc.lam;
+    scal[1] = sc.lam_init;
+    scal[2] = sc.step[0];
+    scal[3] = sc.step[1];
+    out[0] = L.step_norm[0];
+    out[1] = L.step_norm[1];
+    out[2] = L.alpha[0];
+    out[3] = L.alpha[1];
+  } catch (const CudaError &e) {
+    return cuda_fail(c, e);
+  }
+  return EPLACE_OK;
+}
+
+eplace_status eplace_stage_hpwl(eplace_ctx *c, const int32_t *sx, const int32_t *sy, int64_t *hpwl) {
+  if (!c || !hpwl || (c->hp.N && (!sx || !sy))) return EPLACE_ERR_INVALID;
+  try {
+    CK(cudaSetDevice(c->device));
+    const HostProblem &hp = c->hp;
+    std::vector<int2> l(hp.N);
+    for (uint32_t i = 0; i < hp.N; ++i) {
+      if (sx[i] < 0 || sx[i] >= hp.W || sy[i] < 0 || sy[i] >= hp.H) {
+        set_err(c, "site out of range");
+        return EPLACE_ERR_INVALID;
+      }
+      l[i] = make_int2(sx[i] + (hp.cw[i] - 1) / 2, sy[i] + (hp.ch[i] - 1) / 2);
+    }
+    if (hp.N) CK(cudaMemcpyAsync(c->loc.p, l.data(), sizeof(int2) * hp.N, cudaMemcpyHostToDevice, c->stream));
+    c->hp_total.zero(c->stream);
+    HpwlArgs a{c->net_off.p, c->pin_cell.p, c->has_driver.p, c->loc.p, hp.NN, c->hp_total.p};
+    if (hp.NN) CK(launch_hpwl(a, grid_for((int)hp.NN, kHpwlBlock, c->num_sms * 8), c->stream));
+    unsigned long long t = 0;
+    CK(cudaMemcpyAsync(&t, c->hp_total.p, sizeof(t), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    *hpwl = (int64_t)t;
+  } catch (const CudaError &e) {
+    return cuda_fail(c, e);
+  }
+  return EPLACE_OK;
+}
+
+eplace_status eplace_legalize(eplace_ctx *c, const float *x, const float *y, int32_t *sx, int32_t *sy,
+                              double *disp) {
+  if (!c || (c->hp.N && (!x || !y || !sx || !sy))) return EPLACE_ERR_INVALID;
+  Legalizer L(c->hp);
+  eplace_status st = L.run(x, y, sx, sy, disp);
+  if (st != EPLACE_OK) set_err(c, "logic");
+  return st;
+}
+
+eplace_status eplace_legalize_host(const eplace_netlist *nl, const eplace_chip *chip, const float *x, const float *y,
+                                   int32_t *sx, int32_t *sy, double *disp) {
+  HostProblem hp;
+  std::string msg;
+  eplace_status st = load_problem(nl, chip, hp, msg);
+  if (st != EPLACE_OK) {
+    set_err(nullptr, msg);
+    return st;
+  }
+  if (hp.N && (!x || !y || !sx || !sy)) return EPLACE_ERR_INVALID;
+  Legalizer L(hp);
+  st = L.run(x, y, sx, sy, disp);
+  if (st != EPLACE_OK) set_err(nullptr, "logic");
+  return st;
+}
+
+eplace_status eplace_hpwl_host(const eplace_netlist *nl, const eplace_chip *chip, const int32_t *sx,
+                               const int32_t *sy, int64_t *hpwl) {
+  HostProblem hp;
+  std::string msg;
+  eplace_status st = load_problem(nl, chip, hp, msg);
+  if (st != EPLACE_OK) {
+    set_err(nullptr, msg);
+    return st;
+  }
+  if (!hpwl || (hp.N && (!sx || !sy))) return EPLACE_ERR_INVALID;
+  *hpwl = hpwl_host(hp, sx, sy);
+  return EPLACE_OK;
+}
+
+eplace_status eplace_initial_placement_host(const eplace_netlist *nl, const eplace_chip *chip, uint64_t seed,
+                                            int32_t *sx, int32_t *sy) {
+  HostProblem hp;
+  std::string msg;
+  eplace_status st = load_problem(nl, chip, hp, msg);
+  if (st != EPLACE_OK) {
+    set_err(nullptr, msg);
+    return st;
+  }
+  std::vector<int32_t> vx, vy;
+  st = initial_placement(hp, seed, vx, vy, msg);
+  if (st != EPLACE_OK) {
+    set_err(nullptr, msg);
+    return st;
+  }
+  if (hp.N && (!sx || !sy)) return EPLACE_ERR_INVALID;
+  std::copy(vx.begin(), vx.end(), sx);
+  std::copy(vy.begin(), vy.end(), sy);
+  return EPLACE_OK;
+}
+
+eplace_status eplace_synth_size(const eplace_synth_spec *spec, eplace_synth_info *info) {
+  if (!spec || !info) return EPLACE_ERR_INVALID;
+  return synth(*spec, info, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr);
+}
+
+eplace_status eplace_synth_fill(const eplace_synth_spec *spec, uint8_t *cw, uint8_t *ch, int32_t *fx, int32_t *fy,
+                                uint32_t *net_off, uint32_t *pin_cell) {
+  if (!spec || !net_off || (spec->num_pads && (!fx || !fy))) return EPLACE_ERR_INVALID;
+  eplace_synth_info info{};
+  return synth(*spec, &info, cw, ch, fx, fy, net_off, pin_cell);
+}
+
+}  // extern "C"

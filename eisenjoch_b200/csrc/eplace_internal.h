@@ -1,0 +1,69 @@
+// eplace_internal.h -- declarations shared by the host C++ and CUDA sources
+// of libeplace.so.  Nothing here crosses the C ABI.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/eplace.h"
+
+namespace eplace {
+
+// Fixed-point scale of the deterministic accumulators (WA gradient, density
+// map): value = int64 / 2^32.  Integer addition is associative, so the sum
+// is independent of the order in which atomics land.
+constexpr double kFixScale = 4294967296.0;
+constexpr double kFixInv = 1.0 / 4294967296.0;
+
+// Host copy of a validated problem.
+struct HostProblem {
+  int32_t W = 0, H = 0, BX = 0, BY = 0;
+  int32_t sx = 1, sy = 1;  // sites per bin along x / y
+  uint32_t N = 0, F = 0, NN = 0, P = 0;
+  std::vector<uint8_t> cw, ch;          // footprint (sites)
+  std::vector<int32_t> init_x, init_y;  // -1 = unbound
+  std::vector<int32_t> fx, fy;
+  std::vector<uint8_t> f_logic;
+  std::vector<uint32_t> net_off, pin_cell;
+  std::vector<uint8_t> has_driver;
+  bool any_macro = false;
+  uint32_t max_degree = 0;
+};
+
+// Validates the C structs and copies them.  Returns EPLACE_OK or
+// EPLACE_ERR_INVALID with msg set.
+eplace_status load_problem(const eplace_netlist *nl, const eplace_chip *chip, HostProblem &hp,
+                           std::string &msg);
+
+// initial_placement (placer/common.rs:27-117) with the reference RNG.
+eplace_status initial_placement(const HostProblem &hp, uint64_t seed, std::vector<int32_t> &sx,
+                                std::vector<int32_t> &sy, std::string &msg);
+
+// compute_pin_weights (placer/common.rs:381-407).
+void pin_weights(const HostProblem &hp, std::vector<double> &w);
+
+// Greedy legaliser (electro_place/mod.rs:206-255), exact ring search.
+struct Legalizer {
+  explicit Legalizer(const HostProblem &hp);
+  // Returns EPLACE_OK or EPLACE_ERR_NO_BELS.
+  eplace_status run(const float *x, const float *y, int32_t *site_x, int32_t *site_y,
+                    double *displacement);
+
+ private:
+  const HostProblem &hp_;
+  std::vector<uint64_t> base_free_;  // per-row bitmaps of free logic sites
+  std::vector<uint64_t> free_;
+  std::vector<uint32_t> order_;      // macros first, then unit cells (solver order)
+  int32_t words_per_row_ = 0;
+};
+
+// total_hpwl (metrics/wirelength.rs:10-51) on the host.
+int64_t hpwl_host(const HostProblem &hp, const int32_t *site_x, const int32_t *site_y);
+
+// Synthetic generator (no reference counterpart).
+eplace_status synth(const eplace_synth_spec &spec, eplace_synth_info *info, uint8_t *cw,
+                    uint8_t *ch, int32_t *fx, int32_t *fy, uint32_t *net_off,
+                    uint32_t *pin_cell);
+
+}  // namespace eplace

@@ -1,0 +1,471 @@
+// host.cpp -- host-side parts of the ElectroPlace path: problem validation,
+// the reference's initial placement and pin weights, the exact greedy
+// legaliser, integer HPWL and the synthetic netlist generator.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "eplace_internal.h"
+
+namespace eplace {
+
+// ---------------------------------------------------------------------------
+// Validation.  The reference Design cannot hold malformed nets; the flat
+// arrays can, so they are checked here instead of trusting the caller.
+// ---------------------------------------------------------------------------
+eplace_status load_problem(const eplace_netlist *nl, const eplace_chip *chip, HostProblem &hp,
+                           std::string &msg) {
+  if (!nl || !chip) { msg = "null netlist or chip"; return EPLACE_ERR_INVALID; }
+  if (chip->width <= 0 || chip->height <= 0) { msg = "chip width/height must be positive"; return EPLACE_ERR_INVALID; }
+  hp.W = chip->width;
+  hp.H = chip->height;
+  hp.BX = chip->bins_x > 0 ? chip->bins_x : chip->width;
+  hp.BY = chip->bins_y > 0 ? chip->bins_y : chip->height;
+  if (hp.W % hp.BX || hp.H % hp.BY) { msg = "width/height must be multiples of bins_x/bins_y"; return EPLACE_ERR_INVALID; }
+  hp.sx = hp.W / hp.BX;
+  hp.sy = hp.H / hp.BY;
+  if ((int64_t)hp.BX * hp.BY > (1 << 26)) { msg = "bin grid too large"; return EPLACE_ERR_INVALID; }
+  hp.N = nl->num_cells;
+  hp.F = nl->num_fixed;
+  hp.NN = nl->num_nets;
+  if (hp.N > (1u << 30) || hp.F > (1u << 30)) { msg = "too many cells"; return EPLACE_ERR_INVALID; }
+  if (hp.NN > 0 && (!nl->net_offsets || !nl->pin_cell)) { msg = "missing net arrays"; return EPLACE_ERR_INVALID; }
+  if (hp.F > 0 && (!nl->fixed_x || !nl->fixed_y)) { msg = "missing fixed-cell locations"; return EPLACE_ERR_INVALID; }
+  hp.P = hp.NN ? nl->net_offsets[hp.NN] : 0;
+  if (hp.NN && nl->net_offsets[0] != 0) { msg = "net_offsets[0] must be 0"; return EPLACE_ERR_INVALID; }
+  hp.net_off.assign(nl->net_offsets, nl->net_offsets + (hp.NN ? hp.NN + 1 : 0));
+  if (hp.NN == 0) hp.net_off.assign(1, 0);
+  for (uint32_t n = 0; n < hp.NN; ++n) {
+    if (hp.net_off[n + 1] < hp.net_off[n]) { msg = "net_offsets not monotone"; return EPLACE_ERR_INVALID; }
+    hp.max_degree = std::max(hp.max_degree, hp.net_off[n + 1] - hp.net_off[n]);
+  }
+  hp.pin_cell.assign(nl->pin_cell, nl->pin_cell + hp.P);
+  for (uint32_t p = 0; p < hp.P; ++p)
+    if (hp.pin_cell[p] >= hp.N + hp.F) { msg = "pin_cell out of range"; return EPLACE_ERR_INVALID; }
+  hp.cw.assign(hp.N, 1);
+  hp.ch.assign(hp.N, 1);
+  if (nl->cell_w) std::copy(nl->cell_w, nl->cell_w + hp.N, hp.cw.begin());
+  if (nl->cell_h) std::copy(nl->cell_h, nl->cell_h + hp.N, hp.ch.begin());
+  for (uint32_t i = 0; i < hp.N; ++i) {
+    if (hp.cw[i] == 0 || hp.ch[i] == 0 || hp.cw[i] > hp.W || hp.ch[i] > hp.H) {
+      msg = "cell footprint out of range";
+      return EPLACE_ERR_INVALID;
+    }
+    if (hp.cw[i] * hp.ch[i] > 1) hp.any_macro = true;
+  }
+  hp.init_x.assign(hp.N, -1);
+  hp.init_y.assign(hp.N, -1);
+  if (nl->cell_init_x && nl->cell_init_y) {
+    for (uint32_t i = 0; i < hp.N; ++i) {
+      int32_t x = nl->cell_init_x[i], y = nl->cell_init_y[i];
+      if (x < 0) continue;
+      if (x >= hp.W || y < 0 || y >= hp.H) { msg = "cell_init out of range"; return EPLACE_ERR_INVALID; }
+      hp.init_x[i] = x;
+      hp.init_y[i] = y;
+    }
+  }
+  hp.fx.assign(nl->fixed_x, nl->fixed_x + hp.F);
+  hp.fy.assign(nl->fixed_y, nl->fixed_y + hp.F);
+  hp.f_logic.assign(hp.F, 0);
+  if (nl->fixed_on_logic) std::copy(nl->fixed_on_logic, nl->fixed_on_logic + hp.F, hp.f_logic.begin());
+  for (uint32_t f = 0; f < hp.F; ++f) {
+    if (hp.f_logic[f] && (hp.fx[f] < 0 || hp.fx[f] >= hp.W || hp.fy[f] < 0 || hp.fy[f] >= hp.H)) {
+      msg = "fixed cell on a logic BEL outside the chip";
+      return EPLACE_ERR_INVALID;
+    }
+  }
+  hp.has_driver.assign(hp.NN, 1);
+  if (nl->net_has_driver) std::copy(nl->net_has_driver, nl->net_has_driver + hp.NN, hp.has_driver.begin());
+  return EPLACE_OK;
+}
+
+// ---------------------------------------------------------------------------
+// xorshift64 (context/rng.rs:19-31) and Fisher-Yates (rng.rs:52-61).
+// ---------------------------------------------------------------------------
+static inline uint64_t xorshift64(uint64_t &s) {
+  s ^= s << 13;
+  s ^= s >> 7;
+  s ^= s << 17;
+  return s;
+}
+
+// initial_placement (placer/common.rs:27-117).  All movable cells share one
+// bucket (tile-major logic BELs, context/buckets.rs:37-43); bound cells keep
+// their BEL; the available BELs are shuffled once and handed out in order.
+eplace_status initial_placement(const HostProblem &hp, uint64_t seed, std::vector<int32_t> &sx,
+                                std::vector<int32_t> &sy, std::string &msg) {
+  sx.assign(hp.N, 0);
+  sy.assign(hp.N, 0);
+  if (hp.N == 0) return EPLACE_OK;
+  const int64_t nsites = (int64_t)hp.W * hp.H;
+  std::vector<uint8_t> occ((size_t)nsites, 0);
+  for (uint32_t f = 0; f < hp.F; ++f)
+    if (hp.f_logic[f]) occ[(size_t)hp.fy[f] * hp.W + hp.fx[f]] = 1;
+  uint32_t unbound = 0;
+  for (uint32_t i = 0; i < hp.N; ++i) {
+    if (hp.init_x[i] >= 0) {
+      size_t t = (size_t)hp.init_y[i] * hp.W + hp.init_x[i];
+      if (occ[t]) {
+        msg = "cell " + std::to_string(i);
+        return EPLACE_ERR_INITIAL_PLACEMENT;
+      }
+      occ[t] = 1;
+      sx[i] = hp.init_x[i];
+      sy[i] = hp.init_y[i];
+    } else {
+      ++unbound;
+    }
+  }
+  if (unbound == 0) return EPLACE_OK;
+  std::vector<int32_t> avail;
+  avail.reserve((size_t)nsites);
+  for (int64_t t = 0; t < nsites; ++t)
+    if (!occ[(size_t)t]) avail.push_back((int32_t)t);
+  uint64_t rng = seed ? seed : 1;
+  for (size_t i = avail.size(); i-- > 1;) {
+    size_t j = (uint32_t)xorshift64(rng) % (uint32_t)(i + 1);
+    std::swap(avail[i], avail[j]);
+  }
+  if (unbound > avail.size()) {
+    msg = "logic (need " + std::to_string(unbound) + " BELs but only " + std::to_string(avail.size()) +
+          " available)";
+    return EPLACE_ERR_NO_BELS;
+  }
+  size_t k = 0;
+  for (uint32_t i = 0; i < hp.N; ++i) {
+    if (hp.init_x[i] >= 0) continue;
+    int32_t t = avail[k++];
+    sx[i] = t % hp.W;
+    sy[i] = t / hp.W;
+  }
+  return EPLACE_OK;
+}
+
+// compute_pin_weights (placer/common.rs:381-407).
+void pin_weights(const HostProblem &hp, std::vector<double> &w) {
+  w.assign(hp.N, 0.0);
+  for (uint32_t n = 0; n < hp.NN; ++n) {
+    uint32_t b = hp.net_off[n], e = hp.net_off[n + 1];
+    if (e - b < 2) continue;
+    double wt = 1.0 / (double)(e - b);
+    for (uint32_t q = b; q < e; ++q)
+      if (hp.pin_cell[q] < hp.N) w[hp.pin_cell[q]] += wt;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Greedy legaliser (electro_place/mod.rs:206-255).
+// The reference scans every bucket BEL in chipdb order and keeps the first
+// strict minimum of (bx - x)^2 + (by - y)^2.  The same minimum and tie-break
+// (lowest tile index) are found here by visiting rows outward from the
+// target: in one row the best free site is the nearest free bit left of or
+// right of floor(x) (per-row 64-bit free maps), and a row whose dy^2 already
+// exceeds the best cost cannot win or tie.  Macros (w*h > 1, an extension)
+// go first onto fully free blocks, cost measured at the block centre.
+// ---------------------------------------------------------------------------
+Legalizer::Legalizer(const HostProblem &hp) : hp_(hp) {
+  words_per_row_ = (hp.W + 63) / 64;
+  base_free_.assign((size_t)words_per_row_ * hp.H, 0);
+  for (int32_t y = 0; y < hp.H; ++y)
+    for (int32_t x = 0; x < hp.W; ++x) base_free_[(size_t)y * words_per_row_ + (x >> 6)] |= 1ull << (x & 63);
+  for (uint32_t f = 0; f < hp.F; ++f)
+    if (hp.f_logic[f])
+      base_free_[(size_t)hp.fy[f] * words_per_row_ + (hp.fx[f] >> 6)] &= ~(1ull << (hp.fx[f] & 63));
+  order_.reserve(hp.N);
+  for (uint32_t i = 0; i < hp.N; ++i)
+    if (hp.cw[i] * hp.ch[i] > 1) order_.push_back(i);
+  for (uint32_t i = 0; i < hp.N; ++i)
+    if (hp.cw[i] * hp.ch[i] == 1) order_.push_back(i);
+}
+
+namespace {
+// highest free x <= pos in the row, or -1
+inline int32_t free_at_or_left(const uint64_t *row, int32_t pos) {
+  if (pos < 0) return -1;
+  int32_t w = pos >> 6;
+  uint64_t m = row[w] & (((pos & 63) == 63) ? ~0ull : ((2ull << (pos & 63)) - 1));
+  while (true) {
+    if (m) return (w << 6) + 63 - __builtin_clzll(m);
+    if (--w < 0) return -1;
+    m = row[w];
+  }
+}
+// lowest free x >= pos in the row, or -1
+inline int32_t free_at_or_right(const uint64_t *row, int32_t pos, int32_t W, int32_t words) {
+  if (pos >= W) return -1;
+  if (pos < 0) pos = 0;
+  int32_t w = pos >> 6;
+  uint64_t m = row[w] & (~0ull << (pos & 63));
+  while (true) {
+    if (m) {
+      int32_t x = (w << 6) + __builtin_ctzll(m);
+      return x < W ? x : -1;
+    }
+    if (++w >= words) return -1;
+    m = row[w];
+  }
+}
+}  // namespace
+
+eplace_status Legalizer::run(const float *x, const float *y, int32_t *site_x, int32_t *site_y,
+                             double *displacement) {
+  const int32_t W = hp_.W, H = hp_.H, WR = words_per_row_;
+  free_ = base_free_;
+  uint64_t *fm = free_.data();
+  double total = 0.0;
+  for (uint32_t i : order_) {
+    const double tx = (double)x[i], ty = (double)y[i];
+    const int w = hp_.cw[i], h = hp_.ch[i];
+    double best = INFINITY;
+    int64_t best_t = -1;
+    if (w == 1 && h == 1) {
+      int32_t cy = (int32_t)std::floor(ty + 0.5);
+      cy = std::min(std::max(cy, 0), H - 1);
+      const int32_t fx0 = (int32_t)std::floor(tx);
+      auto scan_row = [&](int32_t row) {
+        const uint64_t *r = fm + (size_t)row * WR;
+        const double dy = (double)row - ty;
+        const double dy2 = dy * dy;
+        int32_t l = free_at_or_left(r, std::min(fx0, W - 1));
+        int32_t rr = free_at_or_right(r, fx0 + 1, W, WR);
+        for (int32_t c : {l, rr}) {
+          if (c < 0) continue;
+          double dx = (double)c - tx;
+          double cost = dx * dx + dy2;
+          int64_t t = (int64_t)row * W + c;
+          if (cost < best || (cost == best && t < best_t)) {
+            best = cost;
+            best_t = t;
+          }
+        }
+      };
+      scan_row(cy);
+      bool up = true, down = true;
+      for (int32_t d = 1; up || down; ++d) {
+        if (down) {
+          int32_t row = cy - d;
+          if (row < 0) {
+            down = false;
+          } else {
+            double dy = (double)row - ty;
+            if (best_t >= 0 && dy * dy > best) down = false;
+            else scan_row(row);
+          }
+        }
+        if (up) {
+          int32_t row = cy + d;
+          if (row >= H) {
+            up = false;
+          } else {
+            double dy = (double)row - ty;
+            if (best_t >= 0 && dy * dy > best) up = false;
+            else scan_row(row);
+          }
+        }
+      }
+    } else {
+      // Macro: ring search over anchors around the target anchor.
+      const double ox = 0.5 * (w - 1), oy = 0.5 * (h - 1);
+      const int32_t AW = W - w + 1, AH = H - h + 1;
+      if (AW > 0 && AH > 0) {
+        int32_t cx = std::min(std::max((int32_t)std::floor(tx - ox + 0.5), 0), AW - 1);
+        int32_t cy = std::min(std::max((int32_t)std::floor(ty - oy + 0.5), 0), AH - 1);
+        auto block_free = [&](int32_t ax, int32_t ay) {
+          for (int dy = 0; dy < h; ++dy) {
+            const uint64_t *r = fm + (size_t)(ay + dy) * WR;
+            for (int dx = 0; dx < w; ++dx) {
+              int32_t xx = ax + dx;
+              if (!((r[xx >> 6] >> (xx & 63)) & 1)) return false;
+            }
+          }
+          return true;
+        };
+        const int32_t rmax = std::max(AW, AH);
+        for (int32_t r = 0; r <= rmax; ++r) {
+          if (best_t >= 0 && r >= 1 && (double)(r - 1) * (double)(r - 1) > best) break;
+          int32_t y0 = cy - r, y1 = cy + r, x0 = cx - r, x1 = cx + r;
+          for (int32_t ay = std::max(y0, 0); ay <= std::min(y1, AH - 1); ++ay) {
+            bool full = (ay == y0 || ay == y1);
+            int32_t stepx = full ? 1 : std::max(x1 - x0, 1);
+            for (int32_t ax = x0; ax <= x1; ax += stepx) {
+              if (ax < 0 || ax >= AW) continue;
+              if (!block_free(ax, ay)) continue;
+              double dx = ((double)ax + ox) - tx, dy = ((double)ay + oy) - ty;
+              double cost = dx * dx + dy * dy;
+              int64_t t = (int64_t)ay * W + ax;
+              if (cost < best || (cost == best && t < best_t)) {
+                best = cost;
+                best_t = t;
+              }
+            }
+          }
+        }
+      }
+    }
+    if (best_t < 0) return EPLACE_ERR_NO_BELS;
+    const int32_t bx = (int32_t)(best_t % W), by = (int32_t)(best_t / W);
+    for (int dy = 0; dy < h; ++dy)
+      for (int dx = 0; dx < w; ++dx) {
+        int32_t xx = bx + dx;
+        fm[(size_t)(by + dy) * WR + (xx >> 6)] &= ~(1ull << (xx & 63));
+      }
+    site_x[i] = bx;
+    site_y[i] = by;
+    total += best;
+  }
+  if (displacement) *displacement = total;
+  return EPLACE_OK;
+}
+
+// total_hpwl (metrics/wirelength.rs:10-51): integer bbox of driver + users;
+// nets without a driver or without users contribute 0.  A macro's pins sit
+// at anchor + (w-1)/2 (integer), which is the BEL itself for a unit cell.
+int64_t hpwl_host(const HostProblem &hp, const int32_t *sx, const int32_t *sy) {
+  int64_t total = 0;
+  for (uint32_t n = 0; n < hp.NN; ++n) {
+    uint32_t b = hp.net_off[n], e = hp.net_off[n + 1];
+    if (!hp.has_driver[n] || e - b < 2) continue;
+    int32_t x0 = INT32_MAX, x1 = INT32_MIN, y0 = INT32_MAX, y1 = INT32_MIN;
+    for (uint32_t q = b; q < e; ++q) {
+      uint32_t c = hp.pin_cell[q];
+      int32_t lx, ly;
+      if (c < hp.N) {
+        lx = sx[c] + (hp.cw[c] - 1) / 2;
+        ly = sy[c] + (hp.ch[c] - 1) / 2;
+      } else {
+        lx = hp.fx[c - hp.N];
+        ly = hp.fy[c - hp.N];
+      }
+      x0 = std::min(x0, lx);
+      x1 = std::max(x1, lx);
+      y0 = std::min(y0, ly);
+      y1 = std::max(y1, ly);
+    }
+    total += (int64_t)(x1 - x0) + (int64_t)(y1 - y0);
+  }
+  return total;
+}
+
+// ---------------------------------------------------------------------------
+// Synthetic netlist generator.  Independent splitmix64 streams for macro
+// sizes, degrees, pins and pad nets, so the pin count is known from the
+// degree stream alone.
+//   degree: 2 (p .60), U[3,5] (.25), U[6,20] (.12), U[21,200] (.03), <= cells
+//   pins: a uniformly chosen home cluster of `cluster_size` consecutive
+//         cells supplies each pin with probability `locality`, otherwise
+//         any cell; no cell twice in one net; pin 0 is the driver
+//   pads: evenly spaced along the perimeter walk, each joins one uniformly
+//         chosen net as a user (appended after the net's cell pins)
+// ---------------------------------------------------------------------------
+namespace {
+struct SplitMix {
+  uint64_t s;
+  explicit SplitMix(uint64_t seed) : s(seed) {}
+  uint64_t next() {
+    uint64_t z = (s += 0x9e3779b97f4a7c15ull);
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    return z ^ (z >> 31);
+  }
+  double uniform() { return (double)(next() >> 11) * (1.0 / 9007199254740992.0); }
+  uint32_t below(uint32_t n) { return (uint32_t)(next() % n); }
+};
+
+uint32_t draw_degree(SplitMix &r, uint32_t ncells) {
+  double u = r.uniform();
+  uint32_t d;
+  if (u < 0.60) d = 2;
+  else if (u < 0.85) d = 3 + r.below(3);
+  else if (u < 0.97) d = 6 + r.below(15);
+  else d = 21 + r.below(180);
+  return std::min(d, ncells);
+}
+}  // namespace
+
+eplace_status synth(const eplace_synth_spec &sp, eplace_synth_info *info, uint8_t *cw, uint8_t *ch,
+                    int32_t *fx, int32_t *fy, uint32_t *net_off, uint32_t *pin_cell) {
+  if (sp.width <= 0 || sp.height <= 0 || sp.cluster_size == 0) return EPLACE_ERR_INVALID;
+  if (sp.num_pads > 0 && sp.width < 2) return EPLACE_ERR_INVALID;
+  if (sp.num_nets > 0 && sp.num_cells < 2 && sp.num_pads == 0) return EPLACE_ERR_INVALID;
+  const uint32_t N = sp.num_cells, NN = sp.num_nets, F = sp.num_pads;
+  SplitMix rdeg(sp.seed ^ 0x1d8e4e27c47d124full);
+  SplitMix rpin(sp.seed ^ 0x6a09e667f3bcc909ull);
+  SplitMix rmac(sp.seed ^ 0xbb67ae8584caa73bull);
+  SplitMix rpad(sp.seed ^ 0x3c6ef372fe94f82bull);
+  std::vector<uint32_t> deg(NN), pads_per_net(NN, 0), pad_net(F);
+  uint64_t total = 0;
+  uint32_t maxdeg = 0;
+  for (uint32_t n = 0; n < NN; ++n) {
+    deg[n] = N >= 2 ? draw_degree(rdeg, N) : 0;
+  }
+  for (uint32_t f = 0; f < F; ++f) {
+    pad_net[f] = NN ? rpad.below(NN) : 0;
+    if (NN) pads_per_net[pad_net[f]]++;
+  }
+  for (uint32_t n = 0; n < NN; ++n) {
+    total += deg[n] + pads_per_net[n];
+    maxdeg = std::max(maxdeg, deg[n] + pads_per_net[n]);
+  }
+  if (total > 0xffffffffull) return EPLACE_ERR_INVALID;
+  if (info) {
+    info->num_pins = (uint32_t)total;
+    info->max_degree = maxdeg;
+  }
+  if (!net_off) return EPLACE_OK;  // size query
+  // footprints
+  for (uint32_t i = 0; i < N; ++i) {
+    uint8_t s = 1;
+    if (sp.macro_fraction > 0 && rmac.uniform() < sp.macro_fraction) {
+      uint32_t lo = std::max(1u, sp.macro_min), hi = std::max(lo, sp.macro_max);
+      s = (uint8_t)(lo + rmac.below(hi - lo + 1));
+    }
+    if (cw) cw[i] = s;
+    if (ch) ch[i] = s;
+  }
+  // pads along the perimeter walk
+  const int64_t W = sp.width, H = sp.height;
+  const int64_t L = (H >= 2) ? 2 * W + 2 * H - 4 : W;
+  for (uint32_t f = 0; f < F; ++f) {
+    int64_t p = (int64_t)((uint64_t)f * (uint64_t)L / (uint64_t)F);
+    int64_t x, y;
+    if (p < W) { x = p; y = 0; }
+    else if (p < W + H - 1) { x = W - 1; y = p - W + 1; }
+    else if (p < 2 * W + H - 2) { x = W - 2 - (p - (W + H - 1)); y = H - 1; }
+    else { x = 0; y = H - 2 - (p - (2 * W + H - 2)); }
+    fx[f] = (int32_t)x;
+    fy[f] = (int32_t)y;
+  }
+  // nets
+  const uint32_t cs = sp.cluster_size;
+  const uint32_t nclusters = N ? (N + cs - 1) / cs : 0;
+  std::vector<uint32_t> pad_cursor(NN, 0);
+  net_off[0] = 0;
+  for (uint32_t n = 0; n < NN; ++n) net_off[n + 1] = net_off[n] + deg[n] + pads_per_net[n];
+  for (uint32_t n = 0; n < NN; ++n) {
+    uint32_t *out = pin_cell + net_off[n];
+    uint32_t d = deg[n];
+    if (d > 0) {
+      uint32_t home = rpin.below(nclusters);
+      uint32_t lo = home * cs, sz = std::min(cs, N - lo);
+      for (uint32_t k = 0; k < d; ++k) {
+        uint32_t c = 0;
+        for (int attempt = 0;; ++attempt) {
+          bool local = attempt < 64 && rpin.uniform() < sp.locality;
+          c = local ? lo + rpin.below(sz) : rpin.below(N);
+          bool dup = false;
+          for (uint32_t j = 0; j < k; ++j)
+            if (out[j] == c) { dup = true; break; }
+          if (!dup) break;
+        }
+        out[k] = c;
+      }
+    }
+  }
+  for (uint32_t f = 0; f < F; ++f) {
+    uint32_t n = pad_net[f];
+    pin_cell[net_off[n] + deg[n] + pad_cursor[n]++] = N + f;
+  }
+  return EPLACE_OK;
+}
+
+}  // namespace eplace

@@ -1,0 +1,665 @@
+// kernels.cu -- sm_100a kernels of the ElectroPlace iteration.
+//
+//   k_wa            WA wirelength gradient (placer/common.rs:205-291,
+//                   solver/wa.rs:51-101): net-segmented warp reductions over
+//                   the CSR pin array, deterministic fixed-point scatter.
+//   k_scatter       cell -> bin overlap areas (electro_place/density.rs:54-76),
+//                   fixed-point atomics (order independent, bit-reproducible).
+//   k_density_final FP64 sum / overflow (density.rs:79-86), FP32 charge map
+//                   for the transform, resets the accumulator.
+//   k_sgemm         FP32 DCT-matrix GEMMs (density.rs:96-166), spectral
+//                   Poisson scaling fused into the second GEMM's epilogue.
+//   k_step          field gather + penalty + preconditioner + Barzilai-
+//                   Borwein + FISTA + clamp + next look-ahead in one
+//                   cooperative kernel (density.rs:171-206,
+//                   electro_place/mod.rs:131-173, solver/nesterov.rs:41-101,
+//                   :199-218).
+//   k_hpwl          integer HPWL (metrics/wirelength.rs:10-51).
+#include <cooperative_groups.h>
+
+#include "kernels.cuh"
+
+namespace eplace {
+
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr float kLog2e = 1.4426950408889634f;
+// Bound on any spin wait: ~2 s at the B200's clock (clock64 counts SM cycles).
+constexpr long long kSpinCycles = 4000000000ll;
+
+__device__ __forceinline__ unsigned long long to_fix(float v) {
+  return (unsigned long long)__float2ll_rn(v * 4294967296.0f);
+}
+__device__ __forceinline__ double from_fix(unsigned long long v) {
+  return (double)(long long)v * (1.0 / 4294967296.0);
+}
+
+struct OpMax {
+  __device__ float operator()(float a, float b) const { return fmaxf(a, b); }
+};
+struct OpMin {
+  __device__ float operator()(float a, float b) const { return fminf(a, b); }
+};
+struct OpAdd {
+  __device__ float operator()(float a, float b) const { return a + b; }
+};
+
+// Reduction over the lanes [head, end) of a warp segment, result broadcast
+// to every lane of the segment.  Lane l accumulates [l, min(l + 2o, end))
+// at step o, so the head ends with the segment total.
+template <typename Op>
+__device__ __forceinline__ float seg_allreduce(float v, int lane, int end, int head, Op op) {
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    float u = __shfl_down_sync(kFull, v, o);
+    if (lane + o < end) v = op(v, u);
+  }
+  return __shfl_sync(kFull, v, head);
+}
+
+template <typename Op>
+__device__ __forceinline__ float warp_allreduce(float v, Op op) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = op(v, __shfl_xor_sync(kFull, v, o));
+  return v;
+}
+
+__device__ __forceinline__ double warp_sum_d(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+  return v;
+}
+
+// Deterministic block sum of K doubles (fixed tree for a fixed block size).
+template <int K>
+__device__ __forceinline__ void block_sum(double (&v)[K], double *smem /* [32*K] */) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int k = 0; k < K; ++k) v[k] = warp_sum_d(v[k]);
+  __syncthreads();
+  if (lane == 0)
+#pragma unroll
+    for (int k = 0; k < K; ++k) smem[wid * K + k] = v[k];
+  __syncthreads();
+  if (wid == 0) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      double t = lane < nw ? smem[lane * K + k] : 0.0;
+      v[k] = warp_sum_d(t);
+    }
+  }
+  __syncthreads();
+}
+
+// Per-axis WA terms with max/min shifts.  The reference shifts by the pin
+// mean (wa.rs:58); shifting the positive exponentials by the maximum and the
+// negative ones by the minimum leaves value and gradient unchanged and keeps
+// every exponential in (0, 1], so FP32 cannot overflow.
+//   d_max_i = e+_i/S+ (1 + g (u_i - A+/S+)),  u = x - max
+//   d_min_i = e-_i/S- (1 - g (v_i - A-/S-)),  v = x - min
+__device__ __forceinline__ float wa_pin_grad(float u, float v, float ep, float em, float Sp,
+                                             float Ap, float Sm, float Am, float gamma) {
+  float dmax = (ep / Sp) * (1.0f + gamma * (u - Ap / Sp));
+  float dmin = (em / Sm) * (1.0f - gamma * (v - Am / Sm));
+  return dmax - dmin;
+}
+
+__device__ void wa_big_net(const WaArgs &a, int pb, int pe, int lane) {
+  const float kg = a.gamma * kLog2e;
+  float mx = -INFINITY, mn = INFINITY, my = -INFINITY, ny = INFINITY;
+  for (int q = pb + lane; q < pe; q += 32) {
+    float2 p = a.pos[a.pin_cell[q]];
+    mx = fmaxf(mx, p.x);
+    mn = fminf(mn, p.x);
+    my = fmaxf(my, p.y);
+    ny = fminf(ny, p.y);
+  }
+  mx = warp_allreduce(mx, OpMax());
+  mn = warp_allreduce(mn, OpMin());
+  my = warp_allreduce(my, OpMax());
+  ny = warp_allreduce(ny, OpMin());
+  float s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  for (int q = pb + lane; q < pe; q += 32) {
+    float2 p = a.pos[a.pin_cell[q]];
+    float ux = p.x - mx, vx = p.x - mn, uy = p.y - my, vy = p.y - ny;
+    float epx = exp2f(kg * ux), emx = exp2f(-kg * vx);
+    float epy = exp2f(kg * uy), emy = exp2f(-kg * vy);
+    s[0] += epx; s[1] += ux * epx; s[2] += emx; s[3] += vx * emx;
+    s[4] += epy; s[5] += uy * epy; s[6] += emy; s[7] += vy * emy;
+  }
+#pragma unroll
+  for (int k = 0; k < 8; ++k) s[k] = warp_allreduce(s[k], OpAdd());
+  for (int q = pb + lane; q < pe; q += 32) {
+    uint32_t c = a.pin_cell[q];
+    if (c >= a.N) continue;
+    float2 p = a.pos[c];
+    float ux = p.x - mx, vx = p.x - mn, uy = p.y - my, vy = p.y - ny;
+    float gx = wa_pin_grad(ux, vx, exp2f(kg * ux), exp2f(-kg * vx), s[0], s[1], s[2], s[3], a.gamma);
+    float gy = wa_pin_grad(uy, vy, exp2f(kg * uy), exp2f(-kg * vy), s[4], s[5], s[6], s[7], a.gamma);
+    atomicAdd(&a.acc[2 * c], to_fix(gx));
+    atomicAdd(&a.acc[2 * c + 1], to_fix(gy));
+  }
+}
+
+__global__ void __launch_bounds__(kWaBlock) k_wa(const WaArgs a) {
+  const int lane = threadIdx.x & 31;
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  const float kg = a.gamma * kLog2e;
+  for (int t = gw; t < a.ntasks; t += nw) {
+    const WaTask tk = a.tasks[t];
+    const int pb = tk.x, npin = tk.y - tk.x;
+    if (npin > 32) {
+      wa_big_net(a, pb, tk.y, lane);
+      continue;
+    }
+    // Segment heads: bit j set where a net starts at lane j.
+    uint32_t bits = 0;
+    if (lane < tk.w) {
+      uint32_t off = a.net_off[tk.z + lane] - (uint32_t)pb;
+      if (off < (uint32_t)npin) bits = 1u << off;
+    }
+    bits = __reduce_or_sync(kFull, bits);
+    const uint32_t le = kFull >> (31 - lane);
+    const int head = 31 - __clz(bits & le);
+    const uint32_t above = bits & ~le;
+    const int end = above ? (__ffs(above) - 1) : npin;
+    const bool valid = lane < npin;
+    uint32_t c = 0xffffffffu;
+    float2 p = make_float2(0.f, 0.f);
+    if (valid) {
+      c = a.pin_cell[pb + lane];
+      p = a.pos[c];
+    }
+    const float mx = seg_allreduce(p.x, lane, end, head, OpMax());
+    const float mn = seg_allreduce(p.x, lane, end, head, OpMin());
+    const float my = seg_allreduce(p.y, lane, end, head, OpMax());
+    const float ny = seg_allreduce(p.y, lane, end, head, OpMin());
+    const float ux = p.x - mx, vx = p.x - mn, uy = p.y - my, vy = p.y - ny;
+    const float epx = exp2f(kg * ux), emx = exp2f(-kg * vx);
+    const float epy = exp2f(kg * uy), emy = exp2f(-kg * vy);
+    const float Spx = seg_allreduce(epx, lane, end, head, OpAdd());
+    const float Apx = seg_allreduce(ux * epx, lane, end, head, OpAdd());
+    const float Smx = seg_allreduce(emx, lane, end, head, OpAdd());
+    const float Amx = seg_allreduce(vx * emx, lane, end, head, OpAdd());
+    const float Spy = seg_allreduce(epy, lane, end, head, OpAdd());
+    const float Apy = seg_allreduce(uy * epy, lane, end, head, OpAdd());
+    const float Smy = seg_allreduce(emy, lane, end, head, OpAdd());
+    const float Amy = seg_allreduce(vy * emy, lane, end, head, OpAdd());
+    // Nets with fewer than two pins are skipped, as in the reference.
+    if (valid && c < a.N && end - head >= 2) {
+      float gx = wa_pin_grad(ux, vx, epx, emx, Spx, Apx, Smx, Amx, a.gamma);
+      float gy = wa_pin_grad(uy, vy, epy, emy, Spy, Apy, Smy, Amy, a.gamma);
+      atomicAdd(&a.acc[2 * c], to_fix(gx));
+      atomicAdd(&a.acc[2 * c + 1], to_fix(gy));
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Footprint helpers shared by the scatter and the gather.  Footprint
+// [x - w/2, x + w/2] x [y - h/2, y + h/2] in sites; bin b covers
+// [b*s, (b+1)*s).  With w = h = s = 1 this is cell_bin_overlap /
+// bin_overlap_area (density.rs:20-48) in FP32.
+// ---------------------------------------------------------------------------
+struct Foot {
+  float xlo, xhi, ylo, yhi;
+  int bx0, bx1, by0, by1;
+};
+
+__device__ __forceinline__ Foot make_foot(float2 p, float hw, float hh, int BX, int BY,
+                                          float inv_sx, float inv_sy) {
+  Foot f;
+  f.xlo = p.x - hw;
+  f.xhi = p.x + hw;
+  f.ylo = p.y - hh;
+  f.yhi = p.y + hh;
+  f.bx0 = max(0, (int)floorf(f.xlo * inv_sx));
+  f.bx1 = min(BX, max(0, (int)ceilf(f.xhi * inv_sx)));
+  f.by0 = max(0, (int)floorf(f.ylo * inv_sy));
+  f.by1 = min(BY, max(0, (int)ceilf(f.yhi * inv_sy)));
+  return f;
+}
+
+__device__ __forceinline__ float overlap_1d(float lo, float hi, int b, float s) {
+  float b0 = (float)b * s;
+  return fmaxf(fminf(hi, b0 + s) - fmaxf(lo, b0), 0.0f);
+}
+
+__global__ void __launch_bounds__(kScatterBlock) k_scatter(const ScatterArgs a) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < a.N; i += gridDim.x * blockDim.x) {
+    const float2 p = a.pos[i];
+    const float2 hf = a.half ? a.half[i] : make_float2(0.5f, 0.5f);
+    const Foot f = make_foot(p, hf.x, hf.y, a.BX, a.BY, a.inv_sx, a.inv_sy);
+    for (int by = f.by0; by < f.by1; ++by) {
+      const float oy = overlap_1d(f.ylo, f.yhi, by, a.sy);
+      for (int bx = f.bx0; bx < f.bx1; ++bx) {
+        const float ar = overlap_1d(f.xlo, f.xhi, bx, a.sx) * oy;
+        if (ar > 0.0f) atomicAdd(&a.dens[(size_t)by * a.BX + bx], to_fix(ar));
+      }
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kFinalBlock) k_density_final(const FinalArgs a) {
+  __shared__ double sm[64];
+  __shared__ bool last;
+  double v[2] = {0.0, 0.0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.nb; i += gridDim.x * blockDim.x) {
+    const double d = from_fix(a.dens[i]);
+    a.dens[i] = 0ull;
+    a.rho[i] = (float)(d - a.c0);
+    if (a.dens_out) a.dens_out[i] = d;
+    v[0] += d;
+    v[1] += fmax(d - a.cap, 0.0);
+  }
+  block_sum<2>(v, sm);
+  if (threadIdx.x == 0) {
+    a.part[2 * blockIdx.x] = v[0];
+    a.part[2 * blockIdx.x + 1] = v[1];
+    __threadfence();
+    last = atomicAdd(a.ticket, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (last && threadIdx.x == 0) {
+    __threadfence();
+    double s = 0.0, o = 0.0;
+    for (unsigned b = 0; b < gridDim.x; ++b) {
+      s += ((volatile double *)a.part)[2 * b];
+      o += ((volatile double *)a.part)[2 * b + 1];
+    }
+    const double ov = (s < 1e-30) ? 0.0 : o / s;  // compute_overlap
+    a.sc->overlap = ov;
+    a.log[a.sc->iter].overlap = ov;
+    *a.ticket = 0u;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// FP32 SIMT GEMM: 64x64 CTA tile, BK = 16, 256 threads with 4x4 outputs,
+// double-buffered shared memory.  Bounds are checked on every load and
+// store, so any M, N, K works; multiples of 64 / 16 take the float4 path.
+// ---------------------------------------------------------------------------
+constexpr int GT = 64, GK = 16;
+
+template <bool SPECTRAL>
+__global__ void __launch_bounds__(256) k_sgemm(const GemmOp *ops, int M, int N, int K,
+                                               SpectralArgs sp) {
+  const GemmOp op = ops[blockIdx.z];
+  __shared__ __align__(16) float As[2][GK][GT + 4];
+  __shared__ __align__(16) float Bs[2][GK][GT + 4];
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  const int bm = blockIdx.y * GT, bn = blockIdx.x * GT;
+  const bool vec = ((K & 3) == 0) && ((N & 3) == 0);
+  // A tile: 64 rows x 16 k; thread -> row tid/4, k (tid%4)*4..+3
+  const int ar = tid >> 2, ak = (tid & 3) * 4;
+  // B tile: 16 k x 64 cols; thread -> k tid/16, col (tid%16)*4..+3
+  const int bk = tid >> 4, bc = (tid & 15) * 4;
+  float ra[4], rb[4];
+  auto load = [&](int k0) {
+    const int gr = bm + ar, gk = k0 + ak;
+    if (vec && gr < M && gk + 3 < K) {
+      float4 t = *reinterpret_cast<const float4 *>(op.A + (size_t)gr * K + gk);
+      ra[0] = t.x; ra[1] = t.y; ra[2] = t.z; ra[3] = t.w;
+    } else {
+#pragma unroll
+      for (int j = 0; j < 4; ++j) ra[j] = (gr < M && gk + j < K) ? op.A[(size_t)gr * K + gk + j] : 0.0f;
+    }
+    const int gk2 = k0 + bk, gc = bn + bc;
+    if (vec && gk2 < K && gc + 3 < N) {
+      float4 t = *reinterpret_cast<const float4 *>(op.B + (size_t)gk2 * N + gc);
+      rb[0] = t.x; rb[1] = t.y; rb[2] = t.z; rb[3] = t.w;
+    } else {
+#pragma unroll
+      for (int j = 0; j < 4; ++j) rb[j] = (gk2 < K && gc + j < N) ? op.B[(size_t)gk2 * N + gc + j] : 0.0f;
+    }
+  };
+  auto store = [&](int buf) {
+#pragma unroll
+    for (int j = 0; j < 4; ++j) As[buf][ak + j][ar] = ra[j];
+    *reinterpret_cast<float4 *>(&Bs[buf][bk][bc]) = make_float4(rb[0], rb[1], rb[2], rb[3]);
+  };
+  float acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = 0.0f;
+  const int nk = (K + GK - 1) / GK;
+  load(0);
+  store(0);
+  __syncthreads();
+  for (int kt = 0; kt < nk; ++kt) {
+    const int cur = kt & 1;
+    if (kt + 1 < nk) load((kt + 1) * GK);
+#pragma unroll
+    for (int kk = 0; kk < GK; ++kk) {
+      const float4 a4 = *reinterpret_cast<const float4 *>(&As[cur][kk][ty * 4]);
+      const float4 b4 = *reinterpret_cast<const float4 *>(&Bs[cur][kk][tx * 4]);
+      const float av[4] = {a4.x, a4.y, a4.z, a4.w}, bv[4] = {b4.x, b4.y, b4.z, b4.w};
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
+    }
+    if (kt + 1 < nk) {
+      store(cur ^ 1);
+      __syncthreads();
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int r = bm + ty * 4 + i;
+    if (r >= M) continue;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int cidx = bn + tx * 4 + j;
+      if (cidx >= N) continue;
+      const size_t o = (size_t)r * N + cidx;
+      if (SPECTRAL) {
+        // density.rs:114-153: scale 4/(WH), x1/2 on the kx = 0 and ky = 0
+        // lines, phi = a / (2(1-cos wx) + 2(1-cos wy)), E = phi * w.
+        float s = sp.scale;
+        if (cidx == 0) s *= 0.5f;
+        if (r == 0) s *= 0.5f;
+        const float den = sp.gx2[cidx] + sp.gy2[r];
+        float phi = 0.0f, ex = 0.0f, ey = 0.0f;
+        if (!(den < 1e-30f)) {
+          phi = acc[i][j] * s / den;
+          ex = phi * sp.wx[cidx];
+          ey = phi * sp.wy[r];
+        }
+        op.C[o] = ex;
+        op.C2[o] = ey;
+        if (sp.phi) sp.phi[o] = phi;
+      } else {
+        op.C[o] = acc[i][j];
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Grid barrier for the cooperative step kernel.  Every wait is bounded: on
+// timeout the block records the error in sc->err and carries on, so the
+// kernel always terminates and the host reports EPLACE_ERR_TIMEOUT.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void grid_barrier(unsigned *bar, DevScalars *sc) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned *vgen = bar + 1;
+    const unsigned gen = *vgen;
+    __threadfence();
+    const unsigned arrived = atomicAdd(bar, 1u);
+    if (arrived == gridDim.x - 1) {
+      atomicExch(bar, 0u);
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    } else {
+      const long long t0 = clock64();
+      while (*vgen == gen) {
+        if (clock64() - t0 > kSpinCycles) {
+          atomicExch(&sc->err, 1);
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+}
+
+// Weighted-mean field gather for one cell, scaled by its area
+// (compute_density_gradient, density.rs:171-206).
+__device__ __forceinline__ float2 gather_cell(const StepArgs &a, uint32_t i, float2 p) {
+  const float2 hf = a.half ? a.half[i] : make_float2(0.5f, 0.5f);
+  const Foot f = make_foot(p, hf.x, hf.y, a.BX, a.BY, a.inv_sx, a.inv_sy);
+  float fx = 0.f, fy = 0.f, wt = 0.f;
+  for (int by = f.by0; by < f.by1; ++by) {
+    const float oy = overlap_1d(f.ylo, f.yhi, by, a.sy);
+    for (int bx = f.bx0; bx < f.bx1; ++bx) {
+      const float w = overlap_1d(f.xlo, f.xhi, bx, a.sx) * oy;
+      if (w > 0.0f) {
+        const size_t idx = (size_t)by * a.BX + bx;
+        fx = fmaf(w, a.Ex[idx], fx);
+        fy = fmaf(w, a.Ey[idx], fy);
+        wt += w;
+      }
+    }
+  }
+  float2 g = make_float2(0.f, 0.f);
+  if (wt > 1e-10f) {
+    const float ar = a.area ? a.area[i] : 1.0f;
+    g.x = ar * (fx / wt);
+    g.y = ar * (fy / wt);
+  }
+  return g;
+}
+
+// g = (g_wl + lam g_den) / max(1, pw + lam area)   (mod.rs:145-156)
+__device__ __forceinline__ float2 combine(const StepArgs &a, uint32_t i, float2 gw, float2 gd,
+                                          double lam) {
+  const double ar = a.area ? (double)a.area[i] : 1.0;
+  const double pc = fmax((double)a.pw[i] + lam * ar, 1.0);
+  return make_float2((float)(((double)gw.x + lam * (double)gd.x) / pc),
+                     (float)(((double)gw.y + lam * (double)gd.y) / pc));
+}
+
+__global__ void __launch_bounds__(kStepBlock) k_step(const StepArgs a) {
+  __shared__ double sm[32 * 4];
+  __shared__ bool last;
+  const uint32_t tid0 = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t gstride = gridDim.x * blockDim.x;
+  const int it = a.sc->iter;
+  const bool was_init = a.sc->lam_init != 0;
+  double lam = a.sc->lam;
+  bool lam_init = was_init;
+  if (was_init) lam = (lam < 50.0) ? lam * 1.025 : lam + 1.0;  // mod.rs:139-143
+
+  // A bounded wait already gave up in an earlier launch: every block sees the
+  // same flag here and leaves before any barrier, so the rest of the
+  // interval drains quickly and the host reports EPLACE_ERR_TIMEOUT.
+  if (a.sc->err) return;
+  if (a.mode == 1) {  // gather only: no barrier is reached
+    for (uint32_t i = tid0; i < a.N; i += gstride) a.tmp_den[i] = gather_cell(a, i, a.look[i]);
+    return;
+  }
+  // Phase A: gather, read + clear the WA accumulator, combine.
+  double v[4] = {0.0, 0.0, 0.0, 0.0};
+  for (uint32_t i = tid0; i < a.N; i += gstride) {
+    const float2 p = a.look[i];
+    const float2 gd = gather_cell(a, i, p);
+    const float2 gw = make_float2((float)from_fix(a.acc[2 * i]), (float)from_fix(a.acc[2 * i + 1]));
+    a.acc[2 * i] = 0ull;
+    a.acc[2 * i + 1] = 0ull;
+    if (was_init) {
+      const float2 g = combine(a, i, gw, gd, lam);
+      a.g[i] = g;
+      const float2 x = a.x[i], xp = a.xp[i], gp = a.gprev[i];
+      const double dx = (double)x.x - xp.x, dy = (double)x.y - xp.y;
+      v[0] += dx * dx;
+      v[1] += dx * ((double)g.x - gp.x);
+      v[2] += dy * dy;
+      v[3] += dy * ((double)g.y - gp.y);
+    } else {
+      a.tmp_wl[i] = gw;
+      a.tmp_den[i] = gd;
+      v[0] += (double)gw.x * gw.x + (double)gw.y * gw.y;
+      v[1] += (double)gd.x * gd.x + (double)gd.y * gd.y;
+    }
+  }
+  block_sum<4>(v, sm);
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 4; ++k) a.part[4 * blockIdx.x + k] = v[k];
+  grid_barrier(a.bar, a.sc);
+
+  if (!was_init) {
+    // First penalty: 0.1 * |g_wl| / |g_den| when |g_den| > 1e-30 (mod.rs:132-138).
+    double wl = 0.0, dn = 0.0;
+    for (unsigned b = 0; b < gridDim.x; ++b) {
+      wl += ((volatile double *)a.part)[4 * b];
+      dn += ((volatile double *)a.part)[4 * b + 1];
+    }
+    wl = sqrt(wl);
+    dn = sqrt(dn);
+    if (dn > 1e-30) {
+      lam = 0.1 * wl / dn;
+      lam_init = true;
+    }
+    grid_barrier(a.bar, a.sc);  // everyone has read part[] before it is reused
+    for (int k = 0; k < 4; ++k) v[k] = 0.0;
+    for (uint32_t i = tid0; i < a.N; i += gstride) {
+      const float2 g = combine(a, i, a.tmp_wl[i], a.tmp_den[i], lam);
+      a.g[i] = g;
+      const float2 x = a.x[i], xp = a.xp[i], gp = a.gprev[i];
+      const double dx = (double)x.x - xp.x, dy = (double)x.y - xp.y;
+      v[0] += dx * dx;
+      v[1] += dx * ((double)g.x - gp.x);
+      v[2] += dy * dy;
+      v[3] += dy * ((double)g.y - gp.y);
+    }
+    block_sum<4>(v, sm);
+    if (threadIdx.x == 0)
+      for (int k = 0; k < 4; ++k) a.part[4 * blockIdx.x + k] = v[k];
+    grid_barrier(a.bar, a.sc);
+  }
+
+  // Barzilai-Borwein per axis after the first iteration (mod.rs:158-166,
+  // nesterov.rs:199-218): |dx.dx / dx.dg| clamped to [1e-4, 1], kept when
+  // |dx.dg| < 1e-30.
+  double t[4] = {0.0, 0.0, 0.0, 0.0};
+  for (unsigned b = 0; b < gridDim.x; ++b)
+    for (int k = 0; k < 4; ++k) t[k] += ((volatile double *)a.part)[4 * b + k];
+  double alpha[2] = {a.sc->step[0], a.sc->step[1]};
+  if (it > 0) {
+    for (int ax = 0; ax < 2; ++ax) {
+      const double dxdx = t[2 * ax], dxdg = t[2 * ax + 1];
+      if (!(fabs(dxdg) < 1e-30)) alpha[ax] = fmin(fmax(fabs(dxdx / dxdg), 1e-4), 1.0);
+    }
+  }
+  // FISTA step (nesterov.rs:41-64), clamp (:67-72), next look-ahead
+  // (:95-101) clamped to the chip (common.rs:410-415).
+  const double m = a.mom[it], mn = a.mom[it + 1];
+  double nrm[2] = {0.0, 0.0};
+  for (uint32_t i = tid0; i < a.N; i += gstride) {
+    const float2 x = a.x[i], xp = a.xp[i], g = a.g[i];
+    const double yx = (double)x.x + m * ((double)x.x - xp.x);
+    const double yy = (double)x.y + m * ((double)x.y - xp.y);
+    const double nx = yx - alpha[0] * g.x, ny = yy - alpha[1] * g.y;
+    nrm[0] += (nx - x.x) * (nx - x.x);
+    nrm[1] += (ny - x.y) * (ny - x.y);
+    const float cx = fminf(fmaxf((float)nx, 0.0f), a.maxx);
+    const float cy = fminf(fmaxf((float)ny, 0.0f), a.maxy);
+    const float px = fminf(fmaxf(x.x, 0.0f), a.maxx);
+    const float py = fminf(fmaxf(x.y, 0.0f), a.maxy);
+    a.x[i] = make_float2(cx, cy);
+    a.xp[i] = make_float2(px, py);
+    a.gprev[i] = g;
+    const double lx = (double)cx + mn * ((double)cx - px);
+    const double ly = (double)cy + mn * ((double)cy - py);
+    a.look[i] = make_float2(fminf(fmaxf((float)lx, 0.0f), a.maxx), fminf(fmaxf((float)ly, 0.0f), a.maxy));
+  }
+  double w2[2] = {nrm[0], nrm[1]};
+  block_sum<2>(w2, sm);
+  grid_barrier(a.bar, a.sc);  // all blocks done reading part[] (phase C sums)
+  if (threadIdx.x == 0) {
+    a.part[4 * blockIdx.x] = w2[0];
+    a.part[4 * blockIdx.x + 1] = w2[1];
+    __threadfence();
+    last = atomicAdd(a.ticket, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (last && threadIdx.x == 0) {
+    __threadfence();
+    double s0 = 0.0, s1 = 0.0;
+    for (unsigned b = 0; b < gridDim.x; ++b) {
+      s0 += ((volatile double *)a.part)[4 * b];
+      s1 += ((volatile double *)a.part)[4 * b + 1];
+    }
+    IterLog &L = a.log[it];
+    L.lam = lam;
+    L.step_norm[0] = sqrt(s0);
+    L.step_norm[1] = sqrt(s1);
+    L.alpha[0] = alpha[0];
+    L.alpha[1] = alpha[1];
+    a.sc->lam = lam;
+    a.sc->lam_init = lam_init ? 1 : 0;
+    a.sc->step[0] = alpha[0];
+    a.sc->step[1] = alpha[1];
+    a.sc->iter = it + 1;
+    *a.ticket = 0u;
+  }
+}
+
+__global__ void __launch_bounds__(kHpwlBlock) k_hpwl(const HpwlArgs a) {
+  __shared__ double sm[32];
+  double v[1] = {0.0};
+  for (uint32_t n = blockIdx.x * blockDim.x + threadIdx.x; n < a.NN; n += gridDim.x * blockDim.x) {
+    const uint32_t b = a.net_off[n], e = a.net_off[n + 1];
+    if ((a.has_driver && !a.has_driver[n]) || e - b < 2) continue;
+    int x0 = INT_MAX, x1 = INT_MIN, y0 = INT_MAX, y1 = INT_MIN;
+    for (uint32_t q = b; q < e; ++q) {
+      const int2 l = a.loc[a.pin_cell[q]];
+      x0 = min(x0, l.x);
+      x1 = max(x1, l.x);
+      y0 = min(y0, l.y);
+      y1 = max(y1, l.y);
+    }
+    v[0] += (double)((long long)(x1 - x0) + (long long)(y1 - y0));
+  }
+  // Per-thread partials are integers below 2^53, so the FP64 block sum is exact.
+  block_sum<1>(v, sm);
+  if (threadIdx.x == 0) atomicAdd(a.total, (unsigned long long)(long long)v[0]);
+}
+
+}  // namespace
+
+cudaError_t launch_wa(const WaArgs &a, int grid, cudaStream_t s) {
+  if (a.ntasks == 0) return cudaSuccess;
+  k_wa<<<grid, kWaBlock, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_scatter(const ScatterArgs &a, int grid, cudaStream_t s) {
+  if (a.N == 0) return cudaSuccess;
+  k_scatter<<<grid, kScatterBlock, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_density_final(const FinalArgs &a, int grid, cudaStream_t s) {
+  k_density_final<<<grid, kFinalBlock, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sgemm(const GemmOp *ops, int nb, int M, int N, int K, cudaStream_t s) {
+  dim3 grid((N + GT - 1) / GT, (M + GT - 1) / GT, nb);
+  k_sgemm<false><<<grid, 256, 0, s>>>(ops, M, N, K, SpectralArgs{});
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sgemm_spectral(const GemmOp *ops, int M, int N, int K, const SpectralArgs &sp,
+                                  cudaStream_t s) {
+  dim3 grid((N + GT - 1) / GT, (M + GT - 1) / GT, 1);
+  k_sgemm<true><<<grid, 256, 0, s>>>(ops, M, N, K, sp);
+  return cudaGetLastError();
+}
+
+int step_max_grid(int device) {
+  int sms = 0, occ = 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_step, kStepBlock, 0) != cudaSuccess) return 0;
+  return sms * occ;
+}
+
+cudaError_t launch_step(const StepArgs &a, int grid, cudaStream_t s) {
+  void *args[] = {const_cast<StepArgs *>(&a)};
+  return cudaLaunchCooperativeKernel((const void *)k_step, dim3(grid), dim3(kStepBlock), args, 0, s);
+}
+
+cudaError_t launch_hpwl(const HpwlArgs &a, int grid, cudaStream_t s) {
+  k_hpwl<<<grid, kHpwlBlock, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+}  // namespace eplace

@@ -1,0 +1,132 @@
+// kernels.cuh -- device-side state of one placement context and the launch
+// wrappers of the hot-path kernels (defined in kernels.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace eplace {
+
+// Scalars of the Nesterov loop kept on the device so a whole legalisation
+// interval can be replayed as one CUDA graph without host round trips.
+struct DevScalars {
+  double lam;          // density_penalty (electro_place/mod.rs:100)
+  double step[2];      // current step sizes (NesterovSolver::step_size)
+  double overlap;      // overlap of the current iteration's density
+  int32_t lam_init;    // density_initialized
+  int32_t iter;        // index of the next iteration to execute
+  int32_t err;         // non-zero: a bounded wait gave up
+  int32_t pad_;
+};
+
+// One record per executed iteration (fields of the reference log line).
+struct IterLog {
+  double overlap;
+  double lam;
+  double step_norm[2];  // NesterovSolver::step return values
+  double alpha[2];      // step sizes used by the FISTA step
+};
+
+// Warp task of the WA kernel: a run of whole nets with <= 32 pins in total
+// (x = first pin, y = end pin, z = first net, w = net count <= 32), or one
+// net with more than 32 pins (w = 1).
+using WaTask = int4;
+
+struct WaArgs {
+  const WaTask *tasks;
+  int ntasks;
+  const uint32_t *net_off;
+  const uint32_t *pin_cell;
+  const float2 *pos;        // [N + F]: look-ahead positions, then fixed cells
+  unsigned long long *acc;  // [2N] fixed-point gradient (x, y interleaved)
+  uint32_t N;
+  float gamma;
+};
+
+struct ScatterArgs {
+  const float2 *pos;
+  const float2 *half;       // half extents, nullptr => unit cells
+  uint32_t N;
+  int BX, BY;
+  float sx, sy, inv_sx, inv_sy;
+  unsigned long long *dens; // [BY * BX] fixed point
+};
+
+struct FinalArgs {
+  unsigned long long *dens;
+  int nb;
+  double cap;               // capacity per bin (sites per bin)
+  double c0;                // constant removed before the transform
+  float *rho;
+  double *dens_out;         // optional FP64 copy (stage entry)
+  double *part;             // [2 * grid]
+  unsigned *ticket;
+  DevScalars *sc;
+  IterLog *log;
+};
+
+struct GemmOp {
+  const float *A;
+  const float *B;
+  float *C;
+  float *C2;
+};
+
+struct SpectralArgs {
+  const float *wx, *gx2;   // [BX]: pi kx / W, 2(1 - cos(pi kx / W))
+  const float *wy, *gy2;   // [BY]
+  float scale;             // 4 / (W H)
+  float *phi;              // optional scaled potential spectrum
+};
+
+struct StepArgs {
+  uint32_t N;
+  int BX, BY;
+  float sx, sy, inv_sx, inv_sy;
+  float maxx, maxy;
+  float2 *look;             // [N] (fixed cells follow in the same buffer)
+  const float2 *half;       // nullptr => unit cells
+  const float *area;
+  const float *pw;
+  unsigned long long *acc;  // WA accumulator, read then zeroed
+  const float *Ex, *Ey;
+  float2 *x, *xp, *g, *gprev;
+  float2 *tmp_wl, *tmp_den; // [N] scratch for the penalty-initialisation phase
+  const double *mom;        // momentum per iteration
+  DevScalars *sc;
+  IterLog *log;
+  double *part;             // [4 * grid]
+  unsigned *bar;            // grid barrier {count, generation}
+  unsigned *ticket;
+  int mode;                 // 0: full step; 1: gather only (tmp_den <- density gradient)
+};
+
+struct HpwlArgs {
+  const uint32_t *net_off;
+  const uint32_t *pin_cell;
+  const uint8_t *has_driver;
+  const int2 *loc;          // [N + F] integer pin locations
+  uint32_t NN;
+  unsigned long long *total;
+};
+
+cudaError_t launch_wa(const WaArgs &a, int grid, cudaStream_t s);
+cudaError_t launch_scatter(const ScatterArgs &a, int grid, cudaStream_t s);
+cudaError_t launch_density_final(const FinalArgs &a, int grid, cudaStream_t s);
+// C[b] = A[b] (M x K) * B[b] (K x N), row-major FP32; batches from ops[0..nb).
+cudaError_t launch_sgemm(const GemmOp *ops_dev, int nb, int M, int N, int K, cudaStream_t s);
+// As above with the spectral epilogue: C = Ex_hat, C2 = Ey_hat.
+cudaError_t launch_sgemm_spectral(const GemmOp *ops_dev, int M, int N, int K,
+                                  const SpectralArgs &sp, cudaStream_t s);
+cudaError_t launch_step(const StepArgs &a, int grid, cudaStream_t s);
+int step_max_grid(int device);
+cudaError_t launch_hpwl(const HpwlArgs &a, int grid, cudaStream_t s);
+
+constexpr int kWaBlock = 256;
+constexpr int kScatterBlock = 256;
+constexpr int kFinalBlock = 256;
+constexpr int kStepBlock = 256;
+constexpr int kHpwlBlock = 256;
+
+}  // namespace eplace

@@ -1,0 +1,267 @@
+/*
+ * eplace.h -- C ABI of the B200 (sm_100a) ElectroPlace hot path.
+ *
+ * This is the drop-in boundary for the reference placer entry point
+ *   pub fn place_electro(ctx: &mut Context, cfg: &ElectroPlaceCfg)
+ *       -> Result<(), PlacerError>
+ * (crates/nextpnr/src/placer/electro_place/mod.rs:65) and for
+ *   impl Placer for PlacerElectro { place, place_cells }
+ * (crates/nextpnr/src/placer/electro_place/mod.rs:45-63, trait at
+ * crates/nextpnr/src/placer/mod.rs:31-52).
+ *
+ * The caller flattens its netlist into CSR arrays (movable cells in solver
+ * order, i.e. the order of collect_movable_cells, placer/common.rs:155-174),
+ * creates a context (device upload), runs, and writes the returned BEL
+ * bindings back.  Plain pointers and sizes only; no library types cross the
+ * boundary.  All functions return an eplace_status; none aborts or traps.
+ * Threading: one context is used by one host thread at a time; distinct
+ * contexts are independent.
+ */
+#ifndef EPLACE_H
+#define EPLACE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EPLACE_ABI_VERSION 1
+
+/* Status codes.  1..3 map 1:1 onto PlacerError
+ * (crates/nextpnr/src/placer/mod.rs:20-28); the rest are this library's. */
+typedef enum {
+  EPLACE_OK = 0,
+  EPLACE_ERR_NO_BELS = 1,           /* PlacerError::NoBelsAvailable */
+  EPLACE_ERR_PLACEMENT_FAILED = 2,  /* PlacerError::PlacementFailed */
+  EPLACE_ERR_INITIAL_PLACEMENT = 3, /* PlacerError::InitialPlacementFailed */
+  EPLACE_ERR_INVALID = 4,           /* malformed CSR, NaN input, bad sizes */
+  EPLACE_ERR_OOM = 5,               /* device/host allocation or admission refused */
+  EPLACE_ERR_CUDA = 6,              /* CUDA runtime error (message has details) */
+  EPLACE_ERR_TIMEOUT = 7,           /* a bounded device wait gave up */
+  EPLACE_ERR_NO_DEVICE = 8          /* no usable sm_100 device */
+} eplace_status;
+
+/* ElectroPlaceCfg (crates/nextpnr/src/placer/electro_place/config.rs:5-40):
+ * the same nine fields in the same order.  target_util, timing_driven and
+ * timing_weight are carried but, as in the reference, never read;
+ * target_density only shifts the DC term, which the solve zeroes. */
+typedef struct {
+  uint64_t seed;               /* default 1 */
+  double wl_coeff;             /* default 0.5 */
+  double target_util;          /* default 0.7 (unused, as in the reference) */
+  uint8_t timing_driven;       /* default 0   (unused, as in the reference) */
+  double target_density;       /* default 1.0 */
+  double timing_weight;        /* default 0.0 (unused, as in the reference) */
+  double nesterov_step_size;   /* default 0.1 */
+  uint64_t max_iters;          /* default 500 */
+  uint64_t legalize_interval;  /* default 5; 0 is rejected (EPLACE_ERR_INVALID) */
+} eplace_cfg;
+
+/* Fills the defaults of ElectroPlaceCfg::default() (config.rs:29-40). */
+void eplace_cfg_default(eplace_cfg *cfg);
+
+/* Build-only knobs with no reference counterpart. */
+typedef enum {
+  EPLACE_DCT_FP32_SIMT = 0,    /* FP32 DCT-matrix GEMMs on the CUDA cores */
+  EPLACE_DCT_BF16X3_TC = 1     /* BF16 three-term split GEMMs on tcgen05, FP32 accumulate */
+} eplace_dct_mode;
+
+typedef struct {
+  int32_t dct_mode;            /* eplace_dct_mode; default EPLACE_DCT_FP32_SIMT */
+  int32_t legal_threads;       /* host legaliser threads; 0 = hardware concurrency */
+  int32_t use_graphs;          /* capture each legalise interval as a CUDA graph; default 1 */
+  int32_t verbose;             /* 1 = print the reference's per-legalisation trajectory line */
+  int32_t max_inflight;        /* intervals launched ahead of the host; default 3 */
+  int32_t reserved[3];
+} eplace_opts;
+
+void eplace_opts_default(eplace_opts *opts);
+
+/* Chip: a W x H site grid with one logic BEL (z = 0) per site, tile-major
+ * (tile = y*W + x, chipdb/access.rs:118-126).  IO pads sit on separate BELs
+ * and never occupy logic sites unless fixed_on_logic says so.  The density
+ * grid is bins_x x bins_y (0 => one bin per site, as in the reference,
+ * electro_place/mod.rs:71-76); width and height must be multiples of it. */
+typedef struct {
+  int32_t width, height;
+  int32_t bins_x, bins_y;
+} eplace_chip;
+
+/* Netlist in CSR form.  Pin ids < num_cells are movable cells (solver
+ * order); id num_cells + f is fixed cell f.  Each net lists its driver
+ * first, then its users (NetInfo::driver / users, netlist/net.rs:14-67). */
+typedef struct {
+  uint32_t num_cells;
+  uint32_t num_fixed;
+  uint32_t num_nets;
+  const uint8_t *cell_w, *cell_h;           /* footprint in sites; NULL => all 1x1 */
+  const int32_t *cell_init_x, *cell_init_y; /* pre-bound site or -1; NULL => all unbound */
+  const int32_t *fixed_x, *fixed_y;         /* BEL location of each fixed cell */
+  const uint8_t *fixed_on_logic;            /* 1 => occupies the logic BEL at (x,y); NULL => none */
+  const uint32_t *net_offsets;              /* [num_nets + 1], net_offsets[0] == 0 */
+  const uint32_t *pin_cell;                 /* [net_offsets[num_nets]] */
+  const uint8_t *net_has_driver;            /* NULL => every net's pin 0 drives it */
+} eplace_netlist;
+
+/* One line of the reference trajectory log (electro_place/mod.rs:185-188). */
+typedef struct {
+  int32_t iter;
+  int32_t pad_;
+  double hpwl;
+  double displacement;
+  double step_x, step_y;
+  double density_penalty;
+  double overlap;
+} eplace_traj_entry;
+
+/* Result: the side effects place_electro leaves on Context (cell.bel =
+ * BelId{tile, index}, context/occupancy.rs:58-82), written into caller
+ * buffers.  For a macro the BEL is its lower-left anchor site. */
+typedef struct {
+  int32_t *bel_tile;           /* [num_cells] out: y*W + x */
+  int32_t *bel_index;          /* [num_cells] out: z (always 0), may be NULL */
+  float *x, *y;                /* [num_cells] out: best continuous positions, may be NULL */
+  eplace_traj_entry *traj;     /* [traj_capacity] out, may be NULL */
+  uint32_t traj_capacity;
+  /* scalar outputs */
+  uint32_t traj_len;
+  int64_t hpwl;                /* integer HPWL of the final binding */
+  double overlap;              /* overlap of the last executed iteration */
+  uint32_t iters;              /* Nesterov iterations executed */
+  int32_t best_iter;           /* legalisation checkpoint chosen (-1: initial) */
+  uint8_t converged;           /* overlap < 0.1 after >= 20 iterations */
+  double gpu_seconds;          /* device time of the Nesterov loop */
+  double total_seconds;        /* wall time of eplace_run */
+  uint64_t gpu_launches;       /* kernels this library launched for the run */
+  uint64_t h2d_bytes;          /* host->device bytes copied for the run */
+  uint64_t d2h_bytes;          /* device->host bytes copied for the run */
+} eplace_result;
+
+typedef struct eplace_ctx eplace_ctx;
+
+/* Validates and uploads the netlist to `device`; replaces Context set-up. */
+eplace_status eplace_ctx_create(const eplace_netlist *nl, const eplace_chip *chip,
+                                int32_t device, eplace_ctx **out);
+void eplace_ctx_destroy(eplace_ctx *ctx);
+
+/* place_electro (electro_place/mod.rs:65-204) on the uploaded netlist.
+ * opts may be NULL (defaults). */
+eplace_status eplace_run(eplace_ctx *ctx, const eplace_cfg *cfg, const eplace_opts *opts,
+                         eplace_result *res);
+
+/* One-shot convenience: create, run, destroy (the host-buffer path). */
+eplace_status eplace_place(const eplace_netlist *nl, const eplace_chip *chip,
+                           const eplace_cfg *cfg, const eplace_opts *opts,
+                           int32_t device, eplace_result *res);
+
+/* Copies the last error message (of ctx, or of this thread if ctx is NULL)
+ * into buf; returns its full length. */
+size_t eplace_last_error(const eplace_ctx *ctx, char *buf, size_t len);
+
+int32_t eplace_abi_version(void);
+
+/* ---------------------------------------------------------------------- */
+/* Stage entry points: one hot-path kernel each, host buffers in and out. */
+/* They run on the context's device and stream and are what the parity    */
+/* tests call (teacher forcing: the same inputs the oracle gets).          */
+/* ---------------------------------------------------------------------- */
+
+/* WA gradient, replaces add_wa_wirelength_gradient (placer/common.rs:205-291)
+ * + wa_axis_grad (solver/wa.rs:51-101).  x, y: [num_cells]. */
+eplace_status eplace_stage_wa_grad(eplace_ctx *ctx, double wl_coeff, const float *x,
+                                   const float *y, float *gx, float *gy);
+
+/* Density map + overlap, replaces compute_concrete_density / compute_overlap
+ * (electro_place/density.rs:54-86).  density: [bins_y * bins_x] row-major. */
+eplace_status eplace_stage_density(eplace_ctx *ctx, const float *x, const float *y,
+                                   double *density, double *overlap);
+
+/* Field from a density map, replaces compute_density_field
+ * (electro_place/density.rs:96-166).  phi_hat (scaled potential spectrum)
+ * may be NULL. */
+eplace_status eplace_stage_field(eplace_ctx *ctx, const double *density,
+                                 int32_t dct_mode, float *ex, float *ey, float *phi_hat);
+
+/* Field gather, replaces compute_density_gradient (density.rs:171-206). */
+eplace_status eplace_stage_gather(eplace_ctx *ctx, const float *x, const float *y,
+                                  const float *ex, const float *ey, float *gx, float *gy);
+
+/* One fused iteration tail, teacher-forced: field gather + density-penalty
+ * update + combine + preconditioner + Barzilai-Borwein + FISTA step + clamp
+ * + next look-ahead.  Replaces electro_place/mod.rs:124-173 with
+ * compute_density_gradient (density.rs:171-206), NesterovSolver::step /
+ * clamp_positions_range / look_ahead_into (solver/nesterov.rs:41-101) and
+ * bb_step_size (:199-218).  look_*: the clamped look-ahead positions the
+ * gradients were taken at; gwl_*: the WA gradient there; ex/ey: the field.
+ * Solver state (x, y, x_prev, y_prev, gprev_*) is updated in place.
+ * scal in/out: {density_penalty, density_initialized, step_x, step_y};
+ * out: {step_norm_x, step_norm_y, alpha_x, alpha_y}. */
+eplace_status eplace_stage_step(eplace_ctx *ctx, uint64_t iter, const float *look_x,
+                                const float *look_y, const float *gwl_x, const float *gwl_y,
+                                const float *ex, const float *ey, float *x, float *y,
+                                float *x_prev, float *y_prev, float *gprev_x, float *gprev_y,
+                                double *scal, double *out, float *next_look_x,
+                                float *next_look_y);
+
+/* Integer HPWL of a binding (anchor sites per movable cell), replaces
+ * total_hpwl (metrics/wirelength.rs:10-51). */
+eplace_status eplace_stage_hpwl(eplace_ctx *ctx, const int32_t *site_x,
+                                const int32_t *site_y, int64_t *hpwl);
+
+/* Device time of each kernel of the iteration, measured with CUDA events on
+ * the context's stream over `reps` real iterations started from the initial
+ * placement of cfg.  stage_ms[8] = {WA gradient, density scatter, density
+ * finalise, DCT GEMM 1, DCT GEMM 2 + spectral, DCT GEMM 3 (x2), DCT GEMM 4
+ * (x2), fused gather/step}, mean milliseconds per launch. */
+eplace_status eplace_profile_stages(eplace_ctx *ctx, const eplace_cfg *cfg, int32_t dct_mode,
+                                    uint32_t reps, double *stage_ms);
+
+/* Greedy legalisation of continuous positions (electro_place/mod.rs:206-255),
+ * host ring search with the reference's tie-break. */
+eplace_status eplace_legalize(eplace_ctx *ctx, const float *x, const float *y,
+                              int32_t *site_x, int32_t *site_y, double *displacement);
+
+/* The same legaliser and the host HPWL without a context (no device needed):
+ * host code of the path that callers may run on CPU-only machines. */
+eplace_status eplace_legalize_host(const eplace_netlist *nl, const eplace_chip *chip,
+                                   const float *x, const float *y, int32_t *site_x,
+                                   int32_t *site_y, double *displacement);
+eplace_status eplace_hpwl_host(const eplace_netlist *nl, const eplace_chip *chip,
+                               const int32_t *site_x, const int32_t *site_y, int64_t *hpwl);
+/* The reference's initial placement (placer/common.rs:27-117, xorshift64
+ * Fisher-Yates over the free logic BELs), host only. */
+eplace_status eplace_initial_placement_host(const eplace_netlist *nl, const eplace_chip *chip,
+                                            uint64_t seed, int32_t *site_x, int32_t *site_y);
+
+/* ---------------------------------------------------------------------- */
+/* Synthetic netlist generator (seeded, deterministic), no reference      */
+/* counterpart: the benchmark inputs.  Two calls: sizes, then fill.       */
+/* ---------------------------------------------------------------------- */
+typedef struct {
+  uint64_t seed;
+  uint32_t num_cells, num_nets, num_pads;
+  int32_t width, height, bins_x, bins_y;
+  uint32_t cluster_size;       /* 32 (cfg 1) / 64 (cfg 2+) */
+  double locality;             /* 0.6 */
+  double macro_fraction;       /* 0.05 for cfg 2+, else 0 */
+  uint32_t macro_min, macro_max; /* 2, 8 */
+} eplace_synth_spec;
+
+typedef struct {
+  uint32_t num_pins;           /* out of eplace_synth_size */
+  uint32_t max_degree;
+} eplace_synth_info;
+
+eplace_status eplace_synth_size(const eplace_synth_spec *spec, eplace_synth_info *info);
+/* Buffers: cell_w/cell_h [num_cells], fixed_x/fixed_y [num_pads],
+ * net_offsets [num_nets + 1], pin_cell [num_pins]. */
+eplace_status eplace_synth_fill(const eplace_synth_spec *spec, uint8_t *cell_w,
+                                uint8_t *cell_h, int32_t *fixed_x, int32_t *fixed_y,
+                                uint32_t *net_offsets, uint32_t *pin_cell);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* EPLACE_H */
