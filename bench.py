@@ -51,6 +51,13 @@ def parse():
     ap.add_argument("--workload", default="electro_200k_1024")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-reps", type=int, default=30)
+    ap.add_argument("--dct", default="fp32", choices=["fp32", "bf16x3"],
+                    help="fp32: FP32 SIMT DCT GEMMs (the plain form); bf16x3: tcgen05 three-term split")
+    ap.add_argument("--profile-only", action="store_true",
+                    help="only run the per-kernel stage profiler (for ncu captures)")
+    ap.add_argument("--field-mode", default="potential_gradient", choices=["reference", "potential_gradient"],
+                    help="reference: the reference's field formula (default, parity); potential_gradient: the "
+                         "opt-in extension that spreads cells")
     return ap.parse_args()
 
 
@@ -208,7 +215,7 @@ def ncu_traffic(kernel, workload):
 # ---------------------------------------------------------------------------
 # CPU form (oracle restatement, single thread) on a bounded sample
 # ---------------------------------------------------------------------------
-def cpu_sample(nl, chip, cfg, iters_per_job, checkpoints_per_job, budget_s=25.0):
+def cpu_sample(nl, chip, cfg, iters_per_job, checkpoints_per_job, field_mode=1):
     """Times the FP64 CPU loop on this workload: k Nesterov iterations (no
     intermediate legalisation) and one legalisation, and extrapolates to one
     job of `iters_per_job` iterations with `checkpoints_per_job`
@@ -223,12 +230,12 @@ def cpu_sample(nl, chip, cfg, iters_per_job, checkpoints_per_job, budget_s=25.0)
     c.legalize_interval = 10 ** 9
     c.max_iters = 2
     t0 = time.perf_counter()
-    orc.place(c)
+    orc.place(c, field_mode=field_mode)
     t2 = time.perf_counter() - t0
     k = 4
     c.max_iters = 2 + k
     t0 = time.perf_counter()
-    orc.place(c)
+    orc.place(c, field_mode=field_mode)
     tk = time.perf_counter() - t0
     t_iter = max((tk - t2) / k, 1e-9)
     # one legalisation of a spread-out state
@@ -252,14 +259,15 @@ def reference_arm(args, dist):
     import eisenjoch_b200 as E
 
     nl, chip, cfg = E.workload(args.workload)
-    summary = load_job_summary(args.workload)
+    fm = 1 if args.field_mode == "potential_gradient" else 0
+    summary = load_job_summary(args.workload, fm)
     iters = summary["iters"]
     cps = iters // cfg.legalize_interval + 2
     vals = []
     sample = ""
     t_start = time.perf_counter()
     for i in range(args.warmup + args.steps):
-        v, sample, _, _ = cpu_sample(nl, chip, cfg, iters, cps)
+        v, sample, _, _ = cpu_sample(nl, chip, cfg, iters, cps, fm)
         if i >= args.warmup:
             vals.append(v)
     value = statistics.mean(vals)
@@ -279,7 +287,7 @@ def reference_arm(args, dist):
         "data": "synthetic (seeded generator, benchmark shapes)",
         "config": {"workload": args.workload, "cells": nl.num_cells, "nets": nl.num_nets, "pins": nl.num_pins,
                    "bins": [chip.bins_x, chip.bins_y], "sites": [chip.width, chip.height],
-                   "iters_per_job": iters, "iters_source": summary["source"]},
+                   "iters_per_job": iters, "iters_source": summary["source"], "field_mode": args.field_mode},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "wall_s": time.perf_counter() - t_start,
@@ -287,7 +295,7 @@ def reference_arm(args, dist):
     print(json.dumps(line), flush=True)
 
 
-def load_job_summary(workload):
+def load_job_summary(workload, field_mode=1):
     """Iterations to overflow <= 0.10 of this workload's job: the committed
     FP64 oracle summary when present (tests/golden), else the benchmark
     configuration's iteration cap."""
@@ -295,8 +303,9 @@ def load_job_summary(workload):
     if os.path.exists(p):
         with open(p) as f:
             d = json.load(f)
-        if workload in d:
-            return {"iters": int(d[workload]["iters"]), "source": "FP64 oracle full run (tests/golden/job_summaries.json)"}
+        key = workload if field_mode == 1 else workload + ":reference_field"
+        if key in d:
+            return {"iters": int(d[key]["iters"]), "source": "FP64 oracle full run (tests/golden/job_summaries.json)"}
     import eisenjoch_b200 as E
 
     return {"iters": int(E.WORKLOADS[workload]["cfg"].get("max_iters", 500)), "source": "max_iters"}
@@ -318,11 +327,23 @@ def ours(args, dist):
     cfg = E.ElectroPlaceCfg(**w["cfg"])
     hbm, bf16, peak_src = peaks()
 
+    opts = E.RunOptions(field_mode=1 if args.field_mode == "potential_gradient" else 0,
+                        dct_mode=1 if args.dct == "bf16x3" else 0)
     ctx = E.PlacementContext(nl, chip, device=dev)
     # --- per-kernel device times (CUDA events on the library's stream) ---
-    stage_ms = ctx.profile_stages(cfg, reps=args.profile_reps)
+    stage_ms = ctx.profile_stages(cfg, reps=args.profile_reps, opts=opts)
+    if args.profile_only:
+        if dist.rank == 0:
+            print(json.dumps({"workload": args.workload, "dct": args.dct, "stage_ms": stage_ms}), flush=True)
+        ctx.close()
+        return
+    alt_opts = E.RunOptions(field_mode=opts.field_mode, dct_mode=1 - opts.dct_mode)
+    try:
+        alt_stage_ms = ctx.profile_stages(cfg, reps=args.profile_reps, opts=alt_opts)
+    except E.EplaceError as e:
+        alt_stage_ms = {"unavailable": str(e)}
     for _ in range(args.warmup):
-        ctx.run(cfg)
+        ctx.run(cfg, opts)
 
     clocks = Clocks(dev)
     clocks.start()
@@ -334,7 +355,7 @@ def ours(args, dist):
     lat, results = [], []
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        r = ctx.run(cfg)
+        r = ctx.run(cfg, opts)
         lat.append(time.perf_counter() - t0)
         results.append(r)
     e1.record()
@@ -348,13 +369,13 @@ def ours(args, dist):
 
     # --- end to end through the C ABI with host buffers ---
     for _ in range(1):
-        E.place_electro(nl, chip, cfg, device=dev)
+        E.place_electro(nl, chip, cfg, opts, device=dev)
     dist.barrier()
     torch.cuda.synchronize()
     e0.record()
     e2e_res = []
     for _ in range(args.steps):
-        e2e_res.append(E.place_electro(nl, chip, cfg, device=dev))
+        e2e_res.append(E.place_electro(nl, chip, cfg, opts, device=dev))
     e1.record()
     torch.cuda.synchronize()
     dist.barrier()
@@ -393,7 +414,7 @@ def ours(args, dist):
     cpu = None
     if not args.no_cpu_baseline and dist.world == 1:
         cps = r0.iters // cfg.legalize_interval + 2
-        v, sample, t_iter, t_leg = cpu_sample(nl, chip, cfg, r0.iters, cps)
+        v, sample, t_iter, t_leg = cpu_sample(nl, chip, cfg, r0.iters, cps, opts.field_mode)
         cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "port", "sample": sample}
 
     launches = sum(r.gpu_launches for r in results)
@@ -408,7 +429,7 @@ def ours(args, dist):
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f32 (FP64 global reductions)",
+        "dtype": "f32 (FP64 global reductions)" if args.dct == "fp32" else "bf16x3->f32 (FP64 global reductions)",
         "data": "synthetic (seeded generator, benchmark shapes); replica r uses seed + 7919 r",
         "config": {
             "workload": args.workload,
@@ -418,7 +439,10 @@ def ours(args, dist):
             "parallelism": "replicas x%d" % dist.world,
             "l2": "per-iteration working set is L2-resident at this size; no flush between jobs "
                   "(each job runs hundreds of iterations)",
-            "dct": "fp32 simt gemm",
+            "dct": {"fp32": "fp32 simt gemm", "bf16x3": "tcgen05 bf16 3-term split, fp32 accumulate"}[args.dct],
+            "field_mode": args.field_mode + ("" if args.field_mode == "reference" else
+                                             " (extension: the reference field does not spread cells; on this "
+                                             "workload the reference FP64 loop reaches NaN near iteration 47)"),
         },
         "job": {
             "iters": r0.iters, "converged": r0.converged, "overlap": r0.overlap, "hpwl": r0.hpwl,
@@ -434,6 +458,7 @@ def ours(args, dist):
         },
         "roofline": roof,
         "stages": stages,
+        "stages_other_dct_ms": alt_stage_ms,
         "cpu_baseline": cpu,
         "gpu_launches": int(launches),
         "clocks": ck,

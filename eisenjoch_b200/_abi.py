@@ -25,6 +25,9 @@ EPLACE_ERR_NO_DEVICE = 8
 EPLACE_DCT_FP32_SIMT = 0
 EPLACE_DCT_BF16X3_TC = 1
 
+EPLACE_FIELD_REFERENCE = 0
+EPLACE_FIELD_POTENTIAL_GRADIENT = 1
+
 P = ctypes.POINTER
 c_u8p = P(ctypes.c_uint8)
 c_i32p = P(ctypes.c_int32)
@@ -55,7 +58,8 @@ class Opts(ctypes.Structure):
         ("use_graphs", ctypes.c_int32),
         ("verbose", ctypes.c_int32),
         ("max_inflight", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 3),
+        ("field_mode", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 2),
     ]
 
 
@@ -155,7 +159,7 @@ PROTOTYPES = {
     "eplace_last_error": (ctypes.c_size_t, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t]),
     "eplace_stage_wa_grad": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, c_f32p, c_f32p, c_f32p, c_f32p]),
     "eplace_stage_density": (ctypes.c_int, [ctypes.c_void_p, c_f32p, c_f32p, c_f64p, c_f64p]),
-    "eplace_stage_field": (ctypes.c_int, [ctypes.c_void_p, c_f64p, ctypes.c_int32, c_f32p, c_f32p, c_f32p]),
+    "eplace_stage_field": (ctypes.c_int, [ctypes.c_void_p, c_f64p, ctypes.c_int32, ctypes.c_int32, c_f32p, c_f32p, c_f32p]),
     "eplace_stage_gather": (ctypes.c_int, [ctypes.c_void_p, c_f32p, c_f32p, c_f32p, c_f32p, c_f32p, c_f32p]),
     "eplace_stage_step": (
         ctypes.c_int,
@@ -163,7 +167,7 @@ PROTOTYPES = {
     ),
     "eplace_stage_hpwl": (ctypes.c_int, [ctypes.c_void_p, c_i32p, c_i32p, c_i64p]),
     "eplace_legalize": (ctypes.c_int, [ctypes.c_void_p, c_f32p, c_f32p, c_i32p, c_i32p, c_f64p]),
-    "eplace_profile_stages": (ctypes.c_int, [ctypes.c_void_p, P(Cfg), ctypes.c_int32, ctypes.c_uint32, c_f64p]),
+    "eplace_profile_stages": (ctypes.c_int, [ctypes.c_void_p, P(Cfg), P(Opts), ctypes.c_uint32, c_f64p]),
     "eplace_legalize_host": (ctypes.c_int, [P(Netlist), P(Chip), c_f32p, c_f32p, c_i32p, c_i32p, c_f64p]),
     "eplace_hpwl_host": (ctypes.c_int, [P(Netlist), P(Chip), c_i32p, c_i32p, c_i64p]),
     "eplace_initial_placement_host": (ctypes.c_int, [P(Netlist), P(Chip), ctypes.c_uint64, c_i32p, c_i32p]),

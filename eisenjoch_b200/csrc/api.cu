@@ -28,6 +28,7 @@
 #include <thread>
 #include <vector>
 
+#include "dct_tc.cuh"
 #include "eplace_internal.h"
 #include "kernels.cuh"
 
@@ -157,6 +158,7 @@ struct eplace_ctx {
   DBuf<unsigned long long> acc, dens;
   DBuf<float> rho, T, Exh, Eyh, U, V, Ex, Ey, phi;
   DBuf<float> mB1, mL2, mB3, mL4, mB5, mL6;  // DCT matrices (row-major operands)
+  DBuf<float> mB3g, mL6g;                   // potential-gradient field (extension)
   DBuf<float> wx, gx2, wy, gy2;
   DBuf<GemmOp> ops;                         // 0: GEMM1, 1: GEMM2, 2-3: GEMM3, 4-5: GEMM4
   DBuf<double> mom, part;
@@ -166,6 +168,14 @@ struct eplace_ctx {
   DBuf<int2> loc;
   DBuf<unsigned long long> hp_total;
   size_t log_cap = 0;
+
+  // Tensor-core (BF16x3) transform: operands as hi/lo BF16 planes, all
+  // K-major; *t = transposed (the next GEMM's B^T).
+  bool tc_ready = false;
+  DBuf<__nv_bfloat16> rho_h, rho_l, Tt_h, Tt_l, Exh_h, Exh_l, Eyh_h, Eyh_l, Ut_h, Ut_l, Vt_h, Vt_l;
+  DBuf<__nv_bfloat16> B1t_h, B1t_l, L2_h, L2_l, B3t_h, B3t_l, B5t_h, B5t_l, L4_h, L4_l, L6_h, L6_l;
+  DBuf<__nv_bfloat16> B3gt_h, B3gt_l, L6g_h, L6g_l;
+  TcGemmMaps tm1{}, tm2{}, tm3[2]{}, tm4[2]{};
 
   ~eplace_ctx() {
     if (stream) cudaStreamDestroy(stream);
@@ -218,6 +228,7 @@ void build_matrices(eplace_ctx *c) {
   const double pi = 3.14159265358979323846;
   std::vector<float> B1((size_t)W * W), B3((size_t)W * W), B5((size_t)W * W);
   std::vector<float> L2((size_t)H * H), L4((size_t)H * H), L6((size_t)H * H);
+  std::vector<float> B3g((size_t)W * W), L6g((size_t)H * H);
   // GEMM1  T = rho * B1,     B1[x][kx] = cos(pi kx (x + 1/2) / W)        (row DCT-II)
   // GEMM3a U = Ex^ * B3,     B3[kx][x] = sin(pi (kx+1)(x + 1/2) / W), kx = W-1 halved (row DST-III)
   // GEMM3b V = Ey^ * B5,     B5[kx][x] = cos(pi kx (x + 1/2) / W),    kx = 0 halved   (row DCT-III)
@@ -226,6 +237,8 @@ void build_matrices(eplace_ctx *c) {
       B1[(size_t)a * W + b] = (float)std::cos(pi * b * (a + 0.5) / W);
       B3[(size_t)a * W + b] = (float)(std::sin(pi * (a + 1) * (b + 0.5) / W) * (a == W - 1 ? 0.5 : 1.0));
       B5[(size_t)a * W + b] = (float)(std::cos(pi * a * (b + 0.5) / W) * (a == 0 ? 0.5 : 1.0));
+      // potential-gradient field: B3g[kx][x] = -sin(pi kx (x + 1/2) / W)
+      B3g[(size_t)a * W + b] = (float)(-std::sin(pi * a * (b + 0.5) / W));
     }
   // GEMM2  A  = L2 * T,      L2[ky][y] = cos(pi ky (y + 1/2) / H)        (column DCT-II)
   // GEMM4a Ex = L4 * U,      L4[y][ky] = cos(pi ky (y + 1/2) / H), ky = 0 halved   (column DCT-III)
@@ -235,6 +248,8 @@ void build_matrices(eplace_ctx *c) {
       L2[(size_t)a * H + b] = (float)std::cos(pi * a * (b + 0.5) / H);
       L4[(size_t)a * H + b] = (float)(std::cos(pi * b * (a + 0.5) / H) * (b == 0 ? 0.5 : 1.0));
       L6[(size_t)a * H + b] = (float)(std::sin(pi * (b + 1) * (a + 0.5) / H) * (b == H - 1 ? 0.5 : 1.0));
+      // potential-gradient field: L6g[y][ky] = -sin(pi ky (y + 1/2) / H)
+      L6g[(size_t)a * H + b] = (float)(-std::sin(pi * b * (a + 0.5) / H));
     }
   std::vector<float> wx(W), gx2(W), wy(H), gy2(H);
   for (int k = 0; k < W; ++k) {
@@ -254,20 +269,29 @@ void build_matrices(eplace_ctx *c) {
   c->mL2.alloc(L2.size()); c->mL2.upload(L2.data(), L2.size(), s);
   c->mL4.alloc(L4.size()); c->mL4.upload(L4.data(), L4.size(), s);
   c->mL6.alloc(L6.size()); c->mL6.upload(L6.data(), L6.size(), s);
+  c->mB3g.alloc(B3g.size()); c->mB3g.upload(B3g.data(), B3g.size(), s);
+  c->mL6g.alloc(L6g.size()); c->mL6g.upload(L6g.data(), L6g.size(), s);
   c->wx.alloc(W); c->wx.upload(wx.data(), W, s);
   c->gx2.alloc(W); c->gx2.upload(gx2.data(), W, s);
   c->wy.alloc(H); c->wy.upload(wy.data(), H, s);
   c->gy2.alloc(H); c->gy2.upload(gy2.data(), H, s);
-  GemmOp ops[6] = {
+  // ops[0..5]: reference field; ops[6..11]: potential-gradient field.
+  GemmOp ops[12] = {
       {c->rho.p, c->mB1.p, c->T.p, nullptr},
       {c->mL2.p, c->T.p, c->Exh.p, c->Eyh.p},
       {c->Exh.p, c->mB3.p, c->U.p, nullptr},
       {c->Eyh.p, c->mB5.p, c->V.p, nullptr},
       {c->mL4.p, c->U.p, c->Ex.p, nullptr},
       {c->mL6.p, c->V.p, c->Ey.p, nullptr},
+      {c->rho.p, c->mB1.p, c->T.p, nullptr},
+      {c->mL2.p, c->T.p, c->Exh.p, c->Eyh.p},
+      {c->Exh.p, c->mB3g.p, c->U.p, nullptr},
+      {c->Eyh.p, c->mB5.p, c->V.p, nullptr},
+      {c->mL4.p, c->U.p, c->Ex.p, nullptr},
+      {c->mL6g.p, c->V.p, c->Ey.p, nullptr},
   };
-  c->ops.alloc(6);
-  c->ops.upload(ops, 6, s);
+  c->ops.alloc(12);
+  c->ops.upload(ops, 12, s);
   CK(cudaStreamSynchronize(s));
 }
 
@@ -298,22 +322,188 @@ void launch_scatter_stage(eplace_ctx *c) {
   CK(launch_scatter(a, grid_for((int)hp.N, kScatterBlock, c->num_sms * 16), c->stream));
 }
 
-void launch_final_stage(eplace_ctx *c, double *dens_out) {
+// --- tensor-core transform set-up ------------------------------------------
+using EncodeTiledFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                   const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    CK(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
+    if (!p || q != cudaDriverEntryPointSuccess) throw CudaError{cudaErrorNotSupported, "cuTensorMapEncodeTiled"};
+    fn = reinterpret_cast<EncodeTiledFn>(p);
+  }
+  return fn;
+}
+
+// 2-D map of a row-major BF16 matrix (rows x k), box 64 (k) x box_rows,
+// 128-byte swizzle: the K-major operand layout of k_tc_gemm.
+CUtensorMap make_map(const __nv_bfloat16 *base, int rows, int k, int box_rows) {
+  CUtensorMap m;
+  cuuint64_t dims[2] = {(cuuint64_t)k, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)k * 2};
+  cuuint32_t box[2] = {64, (cuuint32_t)box_rows};
+  cuuint32_t es[2] = {1, 1};
+  CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<__nv_bfloat16 *>(base), dims, strides,
+                           box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) throw CudaError{cudaErrorInvalidValue, "cuTensorMapEncodeTiled"};
+  return m;
+}
+
+void upload_split(DBuf<__nv_bfloat16> &hi, DBuf<__nv_bfloat16> &lo, const std::vector<double> &v, cudaStream_t s) {
+  std::vector<__nv_bfloat16> h(v.size()), l(v.size());
+  for (size_t i = 0; i < v.size(); ++i) {
+    const float f = (float)v[i];
+    h[i] = __float2bfloat16_rn(f);
+    l[i] = __float2bfloat16_rn(f - __bfloat162float(h[i]));
+  }
+  hi.alloc(v.size());
+  lo.alloc(v.size());
+  hi.upload(h.data(), h.size(), s);
+  lo.upload(l.data(), l.size(), s);
+}
+
+bool tc_supported(const HostProblem &hp) { return hp.BY % 128 == 0 && hp.BX % kTcBN == 0 && hp.BX % 64 == 0; }
+
+// Builds the hi/lo DCT matrices, the operand buffers and the tensor maps of
+// the four GEMM launches (two field formulas for the inverse transforms).
+void setup_tc(eplace_ctx *c) {
+  if (c->tc_ready) return;
+  const int W = c->hp.BX, H = c->hp.BY;
+  const double pi = 3.14159265358979323846;
+  cudaStream_t s = c->stream;
+  std::vector<double> B1t((size_t)W * W), B3t((size_t)W * W), B5t((size_t)W * W), B3gt((size_t)W * W);
+  std::vector<double> L2((size_t)H * H), L4((size_t)H * H), L6((size_t)H * H), L6g((size_t)H * H);
+  for (int a = 0; a < W; ++a)      // row a of B^T = output column a
+    for (int b = 0; b < W; ++b) {  // b = K index
+      B1t[(size_t)a * W + b] = std::cos(pi * a * (b + 0.5) / W);                                    // kx=a, x=b
+      B3t[(size_t)a * W + b] = std::sin(pi * (b + 1) * (a + 0.5) / W) * (b == W - 1 ? 0.5 : 1.0);  // x=a, kx=b
+      B5t[(size_t)a * W + b] = std::cos(pi * b * (a + 0.5) / W) * (b == 0 ? 0.5 : 1.0);            // x=a, kx=b
+      B3gt[(size_t)a * W + b] = -std::sin(pi * b * (a + 0.5) / W);                                  // x=a, kx=b
+    }
+  for (int a = 0; a < H; ++a)
+    for (int b = 0; b < H; ++b) {
+      L2[(size_t)a * H + b] = std::cos(pi * a * (b + 0.5) / H);                                     // ky=a, y=b
+      L4[(size_t)a * H + b] = std::cos(pi * b * (a + 0.5) / H) * (b == 0 ? 0.5 : 1.0);             // y=a, ky=b
+      L6[(size_t)a * H + b] = std::sin(pi * (b + 1) * (a + 0.5) / H) * (b == H - 1 ? 0.5 : 1.0);   // y=a, ky=b
+      L6g[(size_t)a * H + b] = -std::sin(pi * b * (a + 0.5) / H);                                   // y=a, ky=b
+    }
+  upload_split(c->B1t_h, c->B1t_l, B1t, s);
+  upload_split(c->B3t_h, c->B3t_l, B3t, s);
+  upload_split(c->B5t_h, c->B5t_l, B5t, s);
+  upload_split(c->B3gt_h, c->B3gt_l, B3gt, s);
+  upload_split(c->L2_h, c->L2_l, L2, s);
+  upload_split(c->L4_h, c->L4_l, L4, s);
+  upload_split(c->L6_h, c->L6_l, L6, s);
+  upload_split(c->L6g_h, c->L6g_l, L6g, s);
+  const size_t nb = (size_t)W * H;
+  for (auto *b : {&c->rho_h, &c->rho_l, &c->Tt_h, &c->Tt_l, &c->Exh_h, &c->Exh_l, &c->Eyh_h, &c->Eyh_l, &c->Ut_h,
+                  &c->Ut_l, &c->Vt_h, &c->Vt_l})
+    b->alloc(nb);
+  auto ops = [&](const DBuf<__nv_bfloat16> &ah, const DBuf<__nv_bfloat16> &al, int mrows, int k,
+                 const DBuf<__nv_bfloat16> &bh, const DBuf<__nv_bfloat16> &bl, int nrows) {
+    TcOperandMaps m;
+    m.a_hi = make_map(ah.p, mrows, k, 128);
+    m.a_lo = make_map(al.p, mrows, k, 128);
+    m.b_hi = make_map(bh.p, nrows, k, kTcBN);
+    m.b_lo = make_map(bl.p, nrows, k, kTcBN);
+    return m;
+  };
+  // GEMM1  T   = rho * B1          A = rho (H x W),  B^T = B1t (W x W)
+  c->tm1.op[0] = ops(c->rho_h, c->rho_l, H, W, c->B1t_h, c->B1t_l, W);
+  // GEMM2  Coef = L2 * T           A = L2 (H x H),   B^T = T^T (W x H)
+  c->tm2.op[0] = ops(c->L2_h, c->L2_l, H, H, c->Tt_h, c->Tt_l, W);
+  // GEMM3  U = Ex^ * B3, V = Ey^ * B5 (reference) / U = Ex^ * B3g (gradient)
+  c->tm3[0].op[0] = ops(c->Exh_h, c->Exh_l, H, W, c->B3t_h, c->B3t_l, W);
+  c->tm3[0].op[1] = ops(c->Eyh_h, c->Eyh_l, H, W, c->B5t_h, c->B5t_l, W);
+  c->tm3[1].op[0] = ops(c->Exh_h, c->Exh_l, H, W, c->B3gt_h, c->B3gt_l, W);
+  c->tm3[1].op[1] = c->tm3[0].op[1];
+  // GEMM4  Ex = L4 * U, Ey = L6 * V (reference) / Ey = L6g * V (gradient)
+  c->tm4[0].op[0] = ops(c->L4_h, c->L4_l, H, H, c->Ut_h, c->Ut_l, W);
+  c->tm4[0].op[1] = ops(c->L6_h, c->L6_l, H, H, c->Vt_h, c->Vt_l, W);
+  c->tm4[1].op[0] = c->tm4[0].op[0];
+  c->tm4[1].op[1] = ops(c->L6g_h, c->L6g_l, H, H, c->Vt_h, c->Vt_l, W);
+  CK(cudaStreamSynchronize(s));
+  c->tc_ready = true;
+}
+
+int *err_ptr(eplace_ctx *c) { return reinterpret_cast<int *>(reinterpret_cast<char *>(c->sc.p) + offsetof(DevScalars, err)); }
+
+void launch_final_stage(eplace_ctx *c, double *dens_out, bool tc = false) {
   const HostProblem &hp = c->hp;
   const int nb = hp.BX * hp.BY;
   const double c0 = c->total_area / (double)nb;
-  FinalArgs a{c->dens.p, nb, (double)hp.sx * hp.sy, c0, c->rho.p, dens_out, c->part.p,
-              c->bar.p + 2, c->sc.p, c->log.p};
+  FinalArgs a{c->dens.p, nb, (double)hp.sx * hp.sy, c0, tc ? nullptr : c->rho.p, tc ? c->rho_h.p : nullptr,
+              tc ? c->rho_l.p : nullptr, dens_out, c->part.p, c->bar.p + 2, c->sc.p, c->log.p};
   CK(launch_density_final(a, grid_for(nb, kFinalBlock, c->num_sms * 2), c->stream));
 }
 
-void launch_field_stage(eplace_ctx *c, float *phi) {
+// One of the four GEMM launches of a field solve (density.rs:96-166):
+//   0: T = rho * B1 (row DCT-II)          1: Coef = L2 * T + spectral epilogue
+//   2: U = Ex^ * B3, V = Ey^ * B5          3: Ex = L4 * U, Ey = L6 * V
+void launch_field_gemm(eplace_ctx *c, int g, float *phi, int field_mode, bool tc) {
   const int W = c->hp.BX, H = c->hp.BY;
-  SpectralArgs sp{c->wx.p, c->gx2.p, c->wy.p, c->gy2.p, (float)(4.0 / ((double)W * H)), phi};
-  CK(launch_sgemm(c->ops.p + 0, 1, H, W, W, c->stream));
-  CK(launch_sgemm_spectral(c->ops.p + 1, H, W, H, sp, c->stream));
-  CK(launch_sgemm(c->ops.p + 2, 2, H, W, W, c->stream));
-  CK(launch_sgemm(c->ops.p + 4, 2, H, W, H, c->stream));
+  const int fm = field_mode == EPLACE_FIELD_POTENTIAL_GRADIENT ? 1 : 0;
+  if (tc) {
+    TcGemmEpi e{};
+    e.err = err_ptr(c);
+    e.wx = c->wx.p;
+    e.gx2 = c->gx2.p;
+    e.wy = c->wy.p;
+    e.gy2 = c->gy2.p;
+    e.scale = (float)(4.0 / ((double)W * H));
+    switch (g) {
+      case 0:
+        e.mode = TC_EPI_SPLIT_T;
+        e.out[0] = TcEpiOut{nullptr, c->Tt_h.p, c->Tt_l.p, nullptr, nullptr};
+        CK(launch_tc_gemm(c->tm1, e, 1, H, W, W, c->stream));
+        break;
+      case 1:
+        e.mode = TC_EPI_SPECTRAL;
+        e.phi = phi;
+        e.out[0] = TcEpiOut{nullptr, c->Exh_h.p, c->Exh_l.p, c->Eyh_h.p, c->Eyh_l.p};
+        CK(launch_tc_gemm(c->tm2, e, 1, H, W, H, c->stream));
+        break;
+      case 2:
+        e.mode = TC_EPI_SPLIT_T;
+        e.out[0] = TcEpiOut{nullptr, c->Ut_h.p, c->Ut_l.p, nullptr, nullptr};
+        e.out[1] = TcEpiOut{nullptr, c->Vt_h.p, c->Vt_l.p, nullptr, nullptr};
+        CK(launch_tc_gemm(c->tm3[fm], e, 2, H, W, W, c->stream));
+        break;
+      default:
+        e.mode = TC_EPI_F32;
+        e.out[0] = TcEpiOut{c->Ex.p, nullptr, nullptr, nullptr, nullptr};
+        e.out[1] = TcEpiOut{c->Ey.p, nullptr, nullptr, nullptr, nullptr};
+        CK(launch_tc_gemm(c->tm4[fm], e, 2, H, W, H, c->stream));
+        break;
+    }
+    return;
+  }
+  const GemmOp *ops = c->ops.p + (fm ? 6 : 0);
+  switch (g) {
+    case 0:
+      CK(launch_sgemm(ops + 0, 1, H, W, W, c->stream));
+      break;
+    case 1: {
+      SpectralArgs sp{c->wx.p, c->gx2.p, c->wy.p, c->gy2.p, (float)(4.0 / ((double)W * H)), phi};
+      CK(launch_sgemm_spectral(ops + 1, H, W, H, sp, c->stream));
+      break;
+    }
+    case 2:
+      CK(launch_sgemm(ops + 2, 2, H, W, W, c->stream));
+      break;
+    default:
+      CK(launch_sgemm(ops + 4, 2, H, W, H, c->stream));
+      break;
+  }
+}
+
+void launch_field_stage(eplace_ctx *c, float *phi, int field_mode, bool tc = false) {
+  for (int g = 0; g < 4; ++g) launch_field_gemm(c, g, phi, field_mode, tc);
 }
 
 StepArgs step_args(eplace_ctx *c) {
@@ -356,11 +546,11 @@ void launch_step_stage(eplace_ctx *c) {
   CK(launch_step(a, c->step_grid, c->stream));
 }
 
-void launch_iteration(eplace_ctx *c, float gamma) {
+void launch_iteration(eplace_ctx *c, float gamma, int field_mode, bool tc) {
   launch_wa_stage(c, gamma);
   launch_scatter_stage(c);
-  launch_final_stage(c, nullptr);
-  launch_field_stage(c, nullptr);
+  launch_final_stage(c, nullptr, tc);
+  launch_field_stage(c, nullptr, field_mode, tc);
   launch_step_stage(c);
 }
 
@@ -411,6 +601,7 @@ void eplace_opts_default(eplace_opts *o) {
   o->use_graphs = 1;
   o->verbose = 0;
   o->max_inflight = 3;
+  o->field_mode = EPLACE_FIELD_REFERENCE;
 }
 
 size_t eplace_last_error(const eplace_ctx *ctx, char *buf, size_t len) {
@@ -522,6 +713,23 @@ void eplace_ctx_destroy(eplace_ctx *ctx) {
   delete ctx;
 }
 
+// Validates the run options against this context.
+static eplace_status check_modes(eplace_ctx *c, const eplace_opts &o) {
+  if (o.dct_mode != EPLACE_DCT_FP32_SIMT && o.dct_mode != EPLACE_DCT_BF16X3_TC) {
+    set_err(c, "unknown dct_mode");
+    return EPLACE_ERR_INVALID;
+  }
+  if (o.dct_mode == EPLACE_DCT_BF16X3_TC && !tc_supported(c->hp)) {
+    set_err(c, "the tensor-core transform needs bins_y % 128 == 0 and bins_x % 64 == 0");
+    return EPLACE_ERR_INVALID;
+  }
+  if (o.field_mode != EPLACE_FIELD_REFERENCE && o.field_mode != EPLACE_FIELD_POTENTIAL_GRADIENT) {
+    set_err(c, "unknown field_mode");
+    return EPLACE_ERR_INVALID;
+  }
+  return EPLACE_OK;
+}
+
 // Resets the loop state on the device for a new run from positions (sx, sy).
 static void reset_state(eplace_ctx *c, const std::vector<int32_t> &sx, const std::vector<int32_t> &sy,
                         const eplace_cfg *cfg) {
@@ -586,10 +794,9 @@ eplace_status eplace_run(eplace_ctx *c, const eplace_cfg *cfg, const eplace_opts
     set_err(c, "wl_coeff / nesterov_step_size must be finite (wl_coeff > 0)");
     return EPLACE_ERR_INVALID;
   }
-  if (opts.dct_mode != EPLACE_DCT_FP32_SIMT) {
-    set_err(c, "dct_mode not available in this build");
-    return EPLACE_ERR_INVALID;
-  }
+  eplace_status mst = check_modes(c, opts);
+  if (mst != EPLACE_OK) return mst;
+  const bool tc = opts.dct_mode == EPLACE_DCT_BF16X3_TC;
   if (!res->bel_tile && hp.N) return EPLACE_ERR_INVALID;
   std::string msg;
   std::vector<int32_t> isx, isy;
@@ -619,6 +826,7 @@ eplace_status eplace_run(eplace_ctx *c, const eplace_cfg *cfg, const eplace_opts
     cudaStream_t s = c->stream;
     ensure_log(c, max_iters);
     upload_momentum(c, max_iters);
+    if (tc) setup_tc(c);
     reset_state(c, isx, isy, cfg);
     for (int i = 0; i < nthreads; ++i) legal.emplace_back(new Legalizer(hp));
     pool.reset(new Pool(nthreads));
@@ -666,7 +874,7 @@ eplace_status eplace_run(eplace_ctx *c, const eplace_cfg *cfg, const eplace_opts
           CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
           bool ok = true;
           try {
-            for (uint64_t k = 0; k < n; ++k) launch_iteration(c, gamma);
+            for (uint64_t k = 0; k < n; ++k) launch_iteration(c, gamma, opts.field_mode, tc);
           } catch (const CudaError &) {
             ok = false;
           }
@@ -678,13 +886,13 @@ eplace_status eplace_run(eplace_ctx *c, const eplace_cfg *cfg, const eplace_opts
             graph = nullptr;
             gexec = nullptr;
             use_graph = false;
-            for (uint64_t k = 0; k < n; ++k) launch_iteration(c, gamma);
+            for (uint64_t k = 0; k < n; ++k) launch_iteration(c, gamma, opts.field_mode, tc);
             return;
           }
         }
         CK(cudaGraphLaunch(gexec, s));
       } else {
-        for (uint64_t k = 0; k < n; ++k) launch_iteration(c, gamma);
+        for (uint64_t k = 0; k < n; ++k) launch_iteration(c, gamma, opts.field_mode, tc);
       }
     };
 
@@ -883,13 +1091,15 @@ eplace_status eplace_place(const eplace_netlist *nl, const eplace_chip *chip, co
   return st;
 }
 
-eplace_status eplace_profile_stages(eplace_ctx *c, const eplace_cfg *cfg, int32_t dct_mode, uint32_t reps,
-                                    double *stage_ms) {
+eplace_status eplace_profile_stages(eplace_ctx *c, const eplace_cfg *cfg, const eplace_opts *opts_in,
+                                    uint32_t reps, double *stage_ms) {
   if (!c || !cfg || !stage_ms || reps == 0) return EPLACE_ERR_INVALID;
-  if (dct_mode != EPLACE_DCT_FP32_SIMT) {
-    set_err(c, "dct_mode not available in this build");
-    return EPLACE_ERR_INVALID;
-  }
+  eplace_opts opts;
+  eplace_opts_default(&opts);
+  if (opts_in) opts = *opts_in;
+  eplace_status mst = check_modes(c, opts);
+  if (mst != EPLACE_OK) return mst;
+  const bool tc = opts.dct_mode == EPLACE_DCT_BF16X3_TC;
   const HostProblem &hp = c->hp;
   if (hp.N == 0) return EPLACE_ERR_INVALID;
   std::vector<cudaEvent_t> ev(9, nullptr);
@@ -905,11 +1115,10 @@ eplace_status eplace_profile_stages(eplace_ctx *c, const eplace_cfg *cfg, int32_
     }
     ensure_log(c, reps);
     upload_momentum(c, reps);
+    if (tc) setup_tc(c);
     reset_state(c, isx, isy, cfg);
     for (auto &e : ev) CK(cudaEventCreate(&e));
     const float gamma = (float)cfg->wl_coeff;
-    const int W = hp.BX, H = hp.BY;
-    SpectralArgs sp{c->wx.p, c->gx2.p, c->wy.p, c->gy2.p, (float)(4.0 / ((double)W * H)), nullptr};
     double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     cudaStream_t s = c->stream;
     for (uint32_t r = 0; r < reps; ++r) {
@@ -918,16 +1127,12 @@ eplace_status eplace_profile_stages(eplace_ctx *c, const eplace_cfg *cfg, int32_
       CK(cudaEventRecord(ev[1], s));
       launch_scatter_stage(c);
       CK(cudaEventRecord(ev[2], s));
-      launch_final_stage(c, nullptr);
+      launch_final_stage(c, nullptr, tc);
       CK(cudaEventRecord(ev[3], s));
-      CK(launch_sgemm(c->ops.p + 0, 1, H, W, W, s));
-      CK(cudaEventRecord(ev[4], s));
-      CK(launch_sgemm_spectral(c->ops.p + 1, H, W, H, sp, s));
-      CK(cudaEventRecord(ev[5], s));
-      CK(launch_sgemm(c->ops.p + 2, 2, H, W, W, s));
-      CK(cudaEventRecord(ev[6], s));
-      CK(launch_sgemm(c->ops.p + 4, 2, H, W, H, s));
-      CK(cudaEventRecord(ev[7], s));
+      for (int g = 0; g < 4; ++g) {
+        launch_field_gemm(c, g, nullptr, opts.field_mode, tc);
+        CK(cudaEventRecord(ev[4 + g], s));
+      }
       launch_step_stage(c);
       CK(cudaEventRecord(ev[8], s));
       CK(cudaEventSynchronize(ev[8]));
@@ -1002,27 +1207,50 @@ eplace_status eplace_stage_density(eplace_ctx *c, const float *x, const float *y
   return EPLACE_OK;
 }
 
-eplace_status eplace_stage_field(eplace_ctx *c, const double *density, int32_t dct_mode, float *ex, float *ey,
+eplace_status eplace_stage_field(eplace_ctx *c, const double *density, int32_t dct_mode, int32_t field_mode,
+                                 float *ex, float *ey,
                                  float *phi_hat) {
   if (!c || !density || !ex || !ey) return EPLACE_ERR_INVALID;
-  if (dct_mode != EPLACE_DCT_FP32_SIMT) {
-    set_err(c, "dct_mode not available in this build");
-    return EPLACE_ERR_INVALID;
-  }
+  eplace_opts o;
+  eplace_opts_default(&o);
+  o.dct_mode = dct_mode;
+  o.field_mode = field_mode;
+  eplace_status mst = check_modes(c, o);
+  if (mst != EPLACE_OK) return mst;
+  const bool tc = dct_mode == EPLACE_DCT_BF16X3_TC;
   try {
     CK(cudaSetDevice(c->device));
     const size_t nb = (size_t)c->hp.BX * c->hp.BY;
     const double c0 = c->total_area / (double)nb;
     std::vector<float> rho(nb);
     for (size_t i = 0; i < nb; ++i) rho[i] = (float)(density[i] - c0);
-    c->rho.upload(rho.data(), nb, c->stream);
+    if (tc) {
+      setup_tc(c);
+      std::vector<__nv_bfloat16> h(nb), l(nb);
+      for (size_t i = 0; i < nb; ++i) {
+        h[i] = __float2bfloat16_rn(rho[i]);
+        l[i] = __float2bfloat16_rn(rho[i] - __bfloat162float(h[i]));
+      }
+      c->rho_h.upload(h.data(), nb, c->stream);
+      c->rho_l.upload(l.data(), nb, c->stream);
+      DevScalars sc{};
+      c->sc.upload(&sc, 1, c->stream);
+    } else {
+      c->rho.upload(rho.data(), nb, c->stream);
+    }
     DBuf<float> phi;
     if (phi_hat) phi.alloc(nb);
-    launch_field_stage(c, phi_hat ? phi.p : nullptr);
+    launch_field_stage(c, phi_hat ? phi.p : nullptr, field_mode, tc);
     CK(cudaMemcpyAsync(ex, c->Ex.p, sizeof(float) * nb, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaMemcpyAsync(ey, c->Ey.p, sizeof(float) * nb, cudaMemcpyDeviceToHost, c->stream));
     if (phi_hat) CK(cudaMemcpyAsync(phi_hat, phi.p, sizeof(float) * nb, cudaMemcpyDeviceToHost, c->stream));
+    DevScalars sc{};
+    CK(cudaMemcpyAsync(&sc, c->sc.p, sizeof(sc), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
+    if (tc && sc.err) {
+      set_err(c, "a bounded device wait timed out in the tensor-core transform");
+      return EPLACE_ERR_TIMEOUT;
+    }
   } catch (const CudaError &e) {
     return cuda_fail(c, e);
   }

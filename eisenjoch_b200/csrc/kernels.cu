@@ -92,6 +92,31 @@ __device__ __forceinline__ void block_sum(double (&v)[K], double *smem /* [32*K]
   __syncthreads();
 }
 
+// Deterministic sum over the per-block partials part[stride*b + k], b <
+// nblocks, for k < K: warp 0 reads them lane-strided and reduces with a
+// fixed tree; the result is broadcast to the whole block through smem.
+template <int K>
+__device__ __forceinline__ void sum_partials(const double *part, int stride, unsigned nblocks,
+                                             double (&out)[K], double *smem /* [K] */) {
+  if (threadIdx.x < 32) {
+    double v[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) v[k] = 0.0;
+    for (unsigned b = threadIdx.x; b < nblocks; b += 32)
+#pragma unroll
+      for (int k = 0; k < K; ++k) v[k] += ((volatile const double *)part)[(size_t)stride * b + k];
+#pragma unroll
+    for (int k = 0; k < K; ++k) v[k] = warp_sum_d(v[k]);
+    if (threadIdx.x == 0)
+#pragma unroll
+      for (int k = 0; k < K; ++k) smem[k] = v[k];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < K; ++k) out[k] = smem[k];
+  __syncthreads();
+}
+
 // Per-axis WA terms with max/min shifts.  The reference shifts by the pin
 // mean (wa.rs:58); shifting the positive exponentials by the maximum and the
 // negative ones by the minimum leaves value and gradient unchanged and keeps
@@ -249,7 +274,13 @@ __global__ void __launch_bounds__(kFinalBlock) k_density_final(const FinalArgs a
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.nb; i += gridDim.x * blockDim.x) {
     const double d = from_fix(a.dens[i]);
     a.dens[i] = 0ull;
-    a.rho[i] = (float)(d - a.c0);
+    const float r = (float)(d - a.c0);
+    if (a.rho) a.rho[i] = r;
+    if (a.rho_hi) {
+      const __nv_bfloat16 h = __float2bfloat16_rn(r);
+      a.rho_hi[i] = h;
+      a.rho_lo[i] = __float2bfloat16_rn(r - __bfloat162float(h));
+    }
     if (a.dens_out) a.dens_out[i] = d;
     v[0] += d;
     v[1] += fmax(d - a.cap, 0.0);
@@ -262,13 +293,13 @@ __global__ void __launch_bounds__(kFinalBlock) k_density_final(const FinalArgs a
     last = atomicAdd(a.ticket, 1u) == gridDim.x - 1;
   }
   __syncthreads();
-  if (last && threadIdx.x == 0) {
-    __threadfence();
-    double s = 0.0, o = 0.0;
-    for (unsigned b = 0; b < gridDim.x; ++b) {
-      s += ((volatile double *)a.part)[2 * b];
-      o += ((volatile double *)a.part)[2 * b + 1];
-    }
+  if (!last) return;
+  __threadfence();
+  __shared__ double red[2];
+  double fin[2];
+  sum_partials<2>(a.part, 2, gridDim.x, fin, red);
+  if (threadIdx.x == 0) {
+    const double s = fin[0], o = fin[1];
     const double ov = (s < 1e-30) ? 0.0 : o / s;  // compute_overlap
     a.sc->overlap = ov;
     a.log[a.sc->iter].overlap = ov;
@@ -494,15 +525,13 @@ __global__ void __launch_bounds__(kStepBlock) k_step(const StepArgs a) {
     for (int k = 0; k < 4; ++k) a.part[4 * blockIdx.x + k] = v[k];
   grid_barrier(a.bar, a.sc);
 
+  __shared__ double red[4];
   if (!was_init) {
     // First penalty: 0.1 * |g_wl| / |g_den| when |g_den| > 1e-30 (mod.rs:132-138).
-    double wl = 0.0, dn = 0.0;
-    for (unsigned b = 0; b < gridDim.x; ++b) {
-      wl += ((volatile double *)a.part)[4 * b];
-      dn += ((volatile double *)a.part)[4 * b + 1];
-    }
-    wl = sqrt(wl);
-    dn = sqrt(dn);
+    double nr[2];
+    sum_partials<2>(a.part, 4, gridDim.x, nr, red);
+    const double wl = sqrt(nr[0]);
+    const double dn = sqrt(nr[1]);
     if (dn > 1e-30) {
       lam = 0.1 * wl / dn;
       lam_init = true;
@@ -528,9 +557,8 @@ __global__ void __launch_bounds__(kStepBlock) k_step(const StepArgs a) {
   // Barzilai-Borwein per axis after the first iteration (mod.rs:158-166,
   // nesterov.rs:199-218): |dx.dx / dx.dg| clamped to [1e-4, 1], kept when
   // |dx.dg| < 1e-30.
-  double t[4] = {0.0, 0.0, 0.0, 0.0};
-  for (unsigned b = 0; b < gridDim.x; ++b)
-    for (int k = 0; k < 4; ++k) t[k] += ((volatile double *)a.part)[4 * b + k];
+  double t[4];
+  sum_partials<4>(a.part, 4, gridDim.x, t, red);
   double alpha[2] = {a.sc->step[0], a.sc->step[1]};
   if (it > 0) {
     for (int ax = 0; ax < 2; ++ax) {
@@ -570,13 +598,12 @@ __global__ void __launch_bounds__(kStepBlock) k_step(const StepArgs a) {
     last = atomicAdd(a.ticket, 1u) == gridDim.x - 1;
   }
   __syncthreads();
-  if (last && threadIdx.x == 0) {
-    __threadfence();
-    double s0 = 0.0, s1 = 0.0;
-    for (unsigned b = 0; b < gridDim.x; ++b) {
-      s0 += ((volatile double *)a.part)[4 * b];
-      s1 += ((volatile double *)a.part)[4 * b + 1];
-    }
+  if (!last) return;
+  __threadfence();
+  double fin[2];
+  sum_partials<2>(a.part, 4, gridDim.x, fin, red);
+  if (threadIdx.x == 0) {
+    const double s0 = fin[0], s1 = fin[1];
     IterLog &L = a.log[it];
     L.lam = lam;
     L.step_norm[0] = sqrt(s0);

@@ -2,6 +2,7 @@
 // wrappers of the hot-path kernels (defined in kernels.cu).
 #pragma once
 
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -58,7 +59,9 @@ struct FinalArgs {
   int nb;
   double cap;               // capacity per bin (sites per bin)
   double c0;                // constant removed before the transform
-  float *rho;
+  float *rho;               // FP32 charge map (SIMT transform), or nullptr
+  __nv_bfloat16 *rho_hi;    // BF16 hi/lo charge map (tensor-core transform), or nullptr
+  __nv_bfloat16 *rho_lo;
   double *dens_out;         // optional FP64 copy (stage entry)
   double *part;             // [2 * grid]
   unsigned *ticket;

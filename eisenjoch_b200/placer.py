@@ -58,6 +58,7 @@ class RunOptions:
     use_graphs: bool = True
     verbose: bool = False
     max_inflight: int = 3
+    field_mode: int = _abi.EPLACE_FIELD_REFERENCE
 
     def to_c(self):
         o = _abi.Opts()
@@ -67,6 +68,7 @@ class RunOptions:
         o.use_graphs = int(bool(self.use_graphs))
         o.verbose = int(bool(self.verbose))
         o.max_inflight = int(self.max_inflight)
+        o.field_mode = int(self.field_mode)
         return o
 
 
@@ -287,13 +289,13 @@ WORKLOADS = {
     "electro_200k_1024": dict(
         spec=SynthSpec(seed=2, num_cells=200000, num_nets=220000, num_pads=2000, width=1024, height=1024,
                        bins_x=512, bins_y=512, cluster_size=64, macro_fraction=0.05),
-        cfg=dict(max_iters=2000),
+        cfg=dict(max_iters=500),
     ),
     # 800,000 cells, 2048^2 sites, 1024^2 bins, 880,000 nets.
     "electro_800k_2048": dict(
         spec=SynthSpec(seed=3, num_cells=800000, num_nets=880000, num_pads=4000, width=2048, height=2048,
                        bins_x=1024, bins_y=1024, cluster_size=64, macro_fraction=0.05),
-        cfg=dict(max_iters=2000),
+        cfg=dict(max_iters=500),
     ),
 }
 
@@ -446,13 +448,13 @@ class PlacementContext:
                                                    _abi.ptr(d, ctypes.c_double), ctypes.byref(ov)))
         return d, ov.value
 
-    def field(self, density, dct_mode=_abi.EPLACE_DCT_FP32_SIMT, want_phi=False):
+    def field(self, density, dct_mode=_abi.EPLACE_DCT_FP32_SIMT, want_phi=False, field_mode=_abi.EPLACE_FIELD_REFERENCE):
         by, bx = self.bins
         d = _abi.f64(density).reshape(by, bx)
         ex, ey = np.zeros((by, bx), np.float32), np.zeros((by, bx), np.float32)
         phi = np.zeros((by, bx), np.float32) if want_phi else None
         F = ctypes.c_float
-        self._check(self._lib.eplace_stage_field(self.handle, _abi.ptr(d, ctypes.c_double), dct_mode,
+        self._check(self._lib.eplace_stage_field(self.handle, _abi.ptr(d, ctypes.c_double), dct_mode, field_mode,
                                                  _abi.ptr(ex, F), _abi.ptr(ey, F), _abi.ptr(phi, F)))
         return (ex, ey, phi) if want_phi else (ex, ey)
 
@@ -505,13 +507,13 @@ class PlacementContext:
     STAGES = ("wa_grad", "density_scatter", "density_final", "dct_gemm1", "dct_gemm2_spectral",
               "dct_gemm3", "dct_gemm4", "gather_step")
 
-    def profile_stages(self, cfg: Optional[ElectroPlaceCfg] = None, reps=20, dct_mode=_abi.EPLACE_DCT_FP32_SIMT):
+    def profile_stages(self, cfg: Optional[ElectroPlaceCfg] = None, reps=20, opts: Optional[RunOptions] = None):
         """Mean device milliseconds per launch of each iteration kernel (CUDA
         events on the context's own stream)."""
         cfg = cfg or ElectroPlaceCfg()
-        cc = cfg.to_c()
+        cc, oc = cfg.to_c(), (opts or RunOptions()).to_c()
         out = np.zeros(8, np.float64)
-        self._check(self._lib.eplace_profile_stages(self.handle, ctypes.byref(cc), dct_mode, reps,
+        self._check(self._lib.eplace_profile_stages(self.handle, ctypes.byref(cc), ctypes.byref(oc), reps,
                                                     _abi.ptr(out, ctypes.c_double)))
         return dict(zip(self.STAGES, out.tolist()))
 

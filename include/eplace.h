@@ -68,13 +68,28 @@ typedef enum {
   EPLACE_DCT_BF16X3_TC = 1     /* BF16 three-term split GEMMs on tcgen05, FP32 accumulate */
 } eplace_dct_mode;
 
+/* Field formula.  EPLACE_FIELD_REFERENCE reproduces density.rs:149-163
+ * exactly: phi_hat(k) * w(k) is fed to DST-III input slot k, which that
+ * transform treats as frequency k + 1, so the resulting "field" is not the
+ * derivative of the potential and does not push cells apart (the reference
+ * loop keeps its overlap well above 0.10 on dense designs).
+ * EPLACE_FIELD_POTENTIAL_GRADIENT (extension, not reference-identical) moves
+ * each spectrum one slot down and flips the sign, giving d(phi)/dx of the
+ * reference's own DCT-III synthesis of phi_hat; with it the unchanged loop
+ * spreads cells and reaches overlap < 0.10. */
+typedef enum {
+  EPLACE_FIELD_REFERENCE = 0,
+  EPLACE_FIELD_POTENTIAL_GRADIENT = 1
+} eplace_field_mode;
+
 typedef struct {
   int32_t dct_mode;            /* eplace_dct_mode; default EPLACE_DCT_FP32_SIMT */
   int32_t legal_threads;       /* host legaliser threads; 0 = hardware concurrency */
   int32_t use_graphs;          /* capture each legalise interval as a CUDA graph; default 1 */
   int32_t verbose;             /* 1 = print the reference's per-legalisation trajectory line */
   int32_t max_inflight;        /* intervals launched ahead of the host; default 3 */
-  int32_t reserved[3];
+  int32_t field_mode;          /* eplace_field_mode; default EPLACE_FIELD_REFERENCE */
+  int32_t reserved[2];
 } eplace_opts;
 
 void eplace_opts_default(eplace_opts *opts);
@@ -182,7 +197,8 @@ eplace_status eplace_stage_density(eplace_ctx *ctx, const float *x, const float 
  * (electro_place/density.rs:96-166).  phi_hat (scaled potential spectrum)
  * may be NULL. */
 eplace_status eplace_stage_field(eplace_ctx *ctx, const double *density,
-                                 int32_t dct_mode, float *ex, float *ey, float *phi_hat);
+                                 int32_t dct_mode, int32_t field_mode, float *ex, float *ey,
+                                 float *phi_hat);
 
 /* Field gather, replaces compute_density_gradient (density.rs:171-206). */
 eplace_status eplace_stage_gather(eplace_ctx *ctx, const float *x, const float *y,
@@ -215,7 +231,7 @@ eplace_status eplace_stage_hpwl(eplace_ctx *ctx, const int32_t *site_x,
  * placement of cfg.  stage_ms[8] = {WA gradient, density scatter, density
  * finalise, DCT GEMM 1, DCT GEMM 2 + spectral, DCT GEMM 3 (x2), DCT GEMM 4
  * (x2), fused gather/step}, mean milliseconds per launch. */
-eplace_status eplace_profile_stages(eplace_ctx *ctx, const eplace_cfg *cfg, int32_t dct_mode,
+eplace_status eplace_profile_stages(eplace_ctx *ctx, const eplace_cfg *cfg, const eplace_opts *opts,
                                     uint32_t reps, double *stage_ms);
 
 /* Greedy legalisation of continuous positions (electro_place/mod.rs:206-255),

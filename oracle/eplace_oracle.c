@@ -424,6 +424,8 @@ static void cols(double *d, size_t w, size_t h, tf1d f, int be) {
   free(buf);
 }
 
+static int g_field_mode = ORC_FIELD_REFERENCE;
+
 /* compute_density_field (density.rs:96-166) */
 int orc_field(const double *d, int32_t bw, int32_t bh, double td, int be,
               double *ex, double *ey, double *phi_hat) {
@@ -465,6 +467,18 @@ int orc_field(const double *d, int32_t bw, int32_t bh, double td, int be,
       if (phi_hat) phi_hat[idx] = ph;
     }
   }
+  if (g_field_mode == ORC_FIELD_POTENTIAL_GRADIENT) {
+    /* Extension (not reference behaviour): DST-III input slot k is frequency
+     * k + 1, so the spectrum of frequency k moves to slot k - 1, and the sign
+     * is flipped, giving d(phi)/dx of the DCT-III synthesis of phi_hat. */
+    for (size_t ky = 0; ky < H; ++ky) {
+      for (size_t kx = 0; kx + 1 < W; ++kx) ex[ky * W + kx] = -ex[ky * W + kx + 1];
+      ex[ky * W + W - 1] = 0.0;
+    }
+    for (size_t ky = 0; ky + 1 < H; ++ky)
+      for (size_t kx = 0; kx < W; ++kx) ey[ky * W + kx] = -ey[(ky + 1) * W + kx];
+    for (size_t kx = 0; kx < W; ++kx) ey[(H - 1) * W + kx] = 0.0;
+  }
   rows(ex, W, H, orc_dst3, be); /* Ex: IDST rows, IDCT cols (:155-158) */
   cols(ex, W, H, orc_dct3, be);
   rows(ey, W, H, orc_dct3, be); /* Ey: IDCT rows, IDST cols (:160-163) */
@@ -472,6 +486,8 @@ int orc_field(const double *d, int32_t bw, int32_t bh, double td, int be,
   free(rho);
   return ORC_OK;
 }
+
+void orc_set_field_mode(int mode) { g_field_mode = mode; }
 
 int orc_potential(const double *phi_hat, int32_t bw, int32_t bh, int be, double *phi) {
   size_t W = (size_t)bw, H = (size_t)bh;

@@ -97,6 +97,13 @@ void orc_dct2(double *v, size_t n, int backend);
 void orc_dct3(double *v, size_t n, int backend);
 void orc_dst3(double *v, size_t n, int backend);
 
+/* Field mode: ORC_FIELD_REFERENCE restates density.rs exactly (default).
+ * ORC_FIELD_POTENTIAL_GRADIENT is an extension with no reference
+ * counterpart: the spectrum is moved one DST-III slot down and negated so
+ * the field is d(phi)/dx of the DCT-III synthesis of phi_hat. */
+enum { ORC_FIELD_REFERENCE = 0, ORC_FIELD_POTENTIAL_GRADIENT = 1 };
+void orc_set_field_mode(int mode);
+
 /* --- Poisson field (density.rs:96-166) ---
  * phi_hat (optional) receives the scaled potential spectrum.  */
 int orc_field(const double *d, int32_t bw, int32_t bh, double target_density,

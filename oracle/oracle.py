@@ -152,6 +152,7 @@ def lib():
         L.orc_hpwl.argtypes = [P(_Problem), P(i32), P(i32)]
         L.orc_place.restype = ctypes.c_int
         L.orc_place.argtypes = [P(_Problem), P(_Cfg), ctypes.c_int, ctypes.c_int, P(_Result), f64p]
+        L.orc_set_field_mode.argtypes = [ctypes.c_int]
         L.orc_step.argtypes = [P(_Problem), P(_State), u64, f64p, f64p, f64p, d, d, f64p]
         L.orc_nesterov_init.argtypes = [P(_Nest), f64p, f64p, ctypes.c_size_t, d]
         L.orc_nesterov_set_positions.argtypes = [P(_Nest), f64p]
@@ -377,13 +378,18 @@ class Oracle:
     def overlap(self, d):
         return overlap_of(d, self.capacity)
 
-    def field(self, d, target_density=1.0, backend=1, want_phi=False):
-        """compute_density_field (density.rs:96-166)."""
+    def field(self, d, target_density=1.0, backend=1, want_phi=False, field_mode=0):
+        """compute_density_field (density.rs:96-166).  field_mode 1 is the
+        potential-gradient extension (not reference behaviour)."""
         d = _d(d).reshape(self.by, self.bx)
         ex, ey = np.zeros_like(d), np.zeros_like(d)
         phi = np.zeros_like(d) if want_phi else None
-        st = self._L.orc_field(_p(d, ctypes.c_double), self.bx, self.by, target_density, backend,
-                               _p(ex, ctypes.c_double), _p(ey, ctypes.c_double), _p(phi, ctypes.c_double))
+        self._L.orc_set_field_mode(field_mode)
+        try:
+            st = self._L.orc_field(_p(d, ctypes.c_double), self.bx, self.by, target_density, backend,
+                                   _p(ex, ctypes.c_double), _p(ey, ctypes.c_double), _p(phi, ctypes.c_double))
+        finally:
+            self._L.orc_set_field_mode(0)
         assert st == 0
         return (ex, ey, phi) if want_phi else (ex, ey)
 
@@ -458,9 +464,10 @@ class Oracle:
         out["look_x"], out["look_y"] = la
         return out, norms
 
-    def place(self, cfg, dct_backend=1, legal_method=1, want_trace=False):
+    def place(self, cfg, dct_backend=1, legal_method=1, want_trace=False, field_mode=0):
         """place_electro (electro_place/mod.rs:65-204).  cfg: any object with
-        the nine ElectroPlaceCfg fields.  Returns (status, dict)."""
+        the nine ElectroPlaceCfg fields.  field_mode 1 is the
+        potential-gradient extension.  Returns (status, dict)."""
         c = _Cfg()
         for name, _ in _Cfg._fields_:
             setattr(c, name, getattr(cfg, name))
@@ -475,8 +482,12 @@ class Oracle:
         r.traj = ctypes.cast(traj, P(_Traj))
         r.traj_capacity = cap
         trace = np.zeros(max(1, int(cfg.max_iters))) if want_trace else None
-        st = self._L.orc_place(ctypes.byref(self.p), ctypes.byref(c), dct_backend, legal_method, ctypes.byref(r),
-                               _p(trace, ctypes.c_double))
+        self._L.orc_set_field_mode(field_mode)
+        try:
+            st = self._L.orc_place(ctypes.byref(self.p), ctypes.byref(c), dct_backend, legal_method,
+                                   ctypes.byref(r), _p(trace, ctypes.c_double))
+        finally:
+            self._L.orc_set_field_mode(0)
         out = dict(
             site_x=sx, site_y=sy, best_x=bx, best_y=by, hpwl=int(r.hpwl), iters=int(r.iters),
             best_iter=int(r.best_iter), converged=bool(r.converged), final_overlap=r.final_overlap,

@@ -68,11 +68,34 @@ def test_wa_gradient(case, clustered):
 
 
 def test_wa_gradient_sharp_coefficient(case):
+    """wl_coeff = 5: the reference shifts exponents by the pin mean
+    (wa.rs:58), so exp() overflows to inf -> NaN in FP64 once a pin sits
+    more than ~142 sites from its net's mean.  The kernel's max/min shift is
+    mathematically identical and stays finite; parity is checked on every
+    cell the reference computes, finiteness on the rest."""
     name, nl, chip, ctx, orc = case
     x, y = positions(nl, chip, 12)
     gx, gy = ctx.wa_grad(x, y, 5.0)
     rx, ry = orc.wa_gradient(x, y, 5.0)
-    assert rel_err(gx, rx) <= 1e-4 and rel_err(gy, ry) <= 1e-4
+    ok = np.isfinite(rx) & np.isfinite(ry)
+    assert np.isfinite(gx).all() and np.isfinite(gy).all()
+    assert ok.sum() >= 50
+    assert rel_err(gx[ok], rx[ok]) <= 1e-4 and rel_err(gy[ok], ry[ok]) <= 1e-4
+
+
+def test_wa_gradient_where_reference_overflows(case):
+    """Positions spread over the whole chip with wl_coeff = 2: nets whose
+    pins sit > ~177 sites from their mean overflow in the reference's FP64
+    formula.  On the cells the reference computes, parity holds; the kernel
+    is finite everywhere."""
+    name, nl, chip, ctx, orc = case
+    x, y = positions(nl, chip, 19)
+    gx, gy = ctx.wa_grad(x, y, 2.0)
+    rx, ry = orc.wa_gradient(x, y, 2.0)
+    ok = np.isfinite(rx) & np.isfinite(ry)
+    assert np.isfinite(gx).all() and np.isfinite(gy).all()
+    if ok.any():
+        assert rel_err(gx[ok], rx[ok]) <= 1e-4 and rel_err(gy[ok], ry[ok]) <= 1e-4
 
 
 @pytest.mark.parametrize("clustered", [False, True])
@@ -97,6 +120,40 @@ def test_field(case, clustered):
     assert rel_err(ex, rex) <= 1e-4, name
     assert rel_err(ey, rey) <= 1e-4, name
     assert rel_err(phi, rphi) <= 1e-4, name
+
+
+TC = E._abi.EPLACE_DCT_BF16X3_TC
+
+
+@pytest.mark.parametrize("field_mode", [0, 1])
+def test_field_tensor_core_bf16x3(case, field_mode):
+    """The tcgen05 BF16 three-term split GEMMs (FP32 accumulate) against the
+    FP64 oracle: normwise relative error <= 1e-4 on field and potential
+    spectrum.  Bin grids whose height is not a multiple of 128 are refused."""
+    name, nl, chip, ctx, orc = case
+    x, y = positions(nl, chip, 21, True)
+    rd = orc.density(x, y)
+    by, bx = ctx.bins
+    if by % 128 or bx % 64:
+        with pytest.raises(E.EplaceError):
+            ctx.field(rd, dct_mode=TC)
+        return
+    ex, ey, phi = ctx.field(rd, dct_mode=TC, want_phi=True, field_mode=field_mode)
+    rex, rey, rphi = orc.field(rd, 1.0, want_phi=True, field_mode=field_mode)
+    assert rel_err(ex, rex) <= 1e-4, (name, rel_err(ex, rex))
+    assert rel_err(ey, rey) <= 1e-4, (name, rel_err(ey, rey))
+    assert rel_err(phi, rphi) <= 1e-4
+
+
+def test_field_potential_gradient_mode(case):
+    """The opt-in potential-gradient field (extension) against the oracle's
+    same mode."""
+    name, nl, chip, ctx, orc = case
+    x, y = positions(nl, chip, 18, True)
+    rd = orc.density(x, y)
+    ex, ey = ctx.field(rd, field_mode=E._abi.EPLACE_FIELD_POTENTIAL_GRADIENT)
+    rex, rey = orc.field(rd, 1.0, field_mode=1)
+    assert rel_err(ex, rex) <= 1e-4 and rel_err(ey, rey) <= 1e-4
 
 
 def test_gather(case):
@@ -188,6 +245,29 @@ def test_full_run_matches_oracle():
     bx, by = r.bel_tile % chip.width, r.bel_tile // chip.width
     assert orc.hpwl(bx, by) == r.hpwl
     assert len(np.unique(r.bel_tile)) == nl.num_cells
+
+
+def test_full_run_potential_gradient_mode():
+    """Extension mode: the same loop with the potential-gradient field
+    spreads the cells and converges (overlap < 0.10), like the oracle's."""
+    nl, chip, cfg = E.workload("electro_5k_128")
+    opts = E.RunOptions(field_mode=E._abi.EPLACE_FIELD_POTENTIAL_GRADIENT)
+    r = E.place_electro(nl, chip, cfg, opts)
+    st, o = Oracle(nl, chip).place(cfg, field_mode=1)
+    assert st == 0 and o["converged"] and r.converged
+    assert r.overlap < 0.1
+    assert abs(r.hpwl - o["hpwl"]) <= 0.005 * o["hpwl"], (r.hpwl, o["hpwl"])
+
+
+def test_full_run_tensor_core_mode():
+    """Mixed-precision form (BF16x3 tensor-core transform): same job outcome
+    as the FP64 oracle (potential-gradient field, 5k-cell workload)."""
+    nl, chip, cfg = E.workload("electro_5k_128")
+    opts = E.RunOptions(field_mode=E._abi.EPLACE_FIELD_POTENTIAL_GRADIENT, dct_mode=TC)
+    r = E.place_electro(nl, chip, cfg, opts)
+    st, o = Oracle(nl, chip).place(cfg, field_mode=1)
+    assert r.converged and o["converged"]
+    assert abs(r.hpwl - o["hpwl"]) <= 0.005 * o["hpwl"], (r.hpwl, o["hpwl"])
 
 
 def test_deterministic():
