@@ -311,6 +311,14 @@ def load_job_summary(workload, field_mode=1):
     return {"iters": int(E.WORKLOADS[workload]["cfg"].get("max_iters", 500)), "source": "max_iters"}
 
 
+def replica_spec(spec, rank):
+    """Rank r places its own netlist: the workload's generator with seed +
+    7919 r (independent replicas, no data-path collective)."""
+    import dataclasses
+
+    return dataclasses.replace(spec, seed=spec.seed + 7919 * rank)
+
+
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
@@ -322,8 +330,7 @@ def ours(args, dist):
     dev = dist.local
     torch.cuda.set_device(dev)
     w = E.WORKLOADS[args.workload]
-    spec = E.SynthSpec(**{**w["spec"].__dict__, "seed": w["spec"].seed + 7919 * dist.rank})
-    nl, chip = E.synth_netlist(spec)
+    nl, chip = E.synth_netlist(replica_spec(w["spec"], dist.rank))
     cfg = E.ElectroPlaceCfg(**w["cfg"])
     hbm, bf16, peak_src = peaks()
 

@@ -110,6 +110,13 @@ class Pool {
     }
     cv_.notify_one();
   }
+  int size() const { return (int)th_.size(); }
+  // Blocks until the queue is empty and no job is running.
+  void wait_idle() {
+    std::unique_lock<std::mutex> g(m_);
+    idle_cv_.wait(g, [this] { return q_.empty() && active_ == 0; });
+  }
+
  private:
   void loop(int id) {
     for (;;) {
@@ -120,14 +127,21 @@ class Pool {
         if (stop_ && q_.empty()) return;
         f = std::move(q_.front());
         q_.pop_front();
+        ++active_;
       }
       f(id);
+      {
+        std::lock_guard<std::mutex> g(m_);
+        --active_;
+      }
+      idle_cv_.notify_all();
     }
   }
   std::vector<std::thread> th_;
   std::deque<std::function<void(int)>> q_;
   std::mutex m_;
-  std::condition_variable cv_;
+  std::condition_variable cv_, idle_cv_;
+  int active_ = 0;
   bool stop_ = false;
 };
 
@@ -168,6 +182,25 @@ struct eplace_ctx {
   DBuf<int2> loc;
   DBuf<unsigned long long> hp_total;
   size_t log_cap = 0;
+  // Bumped whenever a buffer a captured graph points at is reallocated.
+  uint64_t buf_epoch = 1;
+
+  // Host resources kept across runs: legaliser base map and per-thread
+  // legalisers, the worker pool, pinned snapshot slots and their events, and
+  // the CUDA graph of one legalisation interval.
+  std::unique_ptr<LegalBase> lbase;
+  std::vector<std::unique_ptr<Legalizer>> legal;
+  std::unique_ptr<Pool> pool;
+  std::vector<std::unique_ptr<PinBuf<float2>>> snaps;
+  std::vector<std::unique_ptr<PinBuf<IterLog>>> logs;
+  std::vector<std::unique_ptr<PinBuf<DevScalars>>> scs;
+  std::vector<cudaEvent_t> slot_ev;
+  size_t slot_log_cap = 0;
+  cudaGraphExec_t gexec = nullptr;
+  uint64_t g_epoch = 0, g_interval = 0;
+  int g_field = -1;
+  bool g_tc = false;
+  float g_gamma = 0.f;
 
   // Tensor-core (BF16x3) transform: operands as hi/lo BF16 planes, all
   // K-major; *t = transposed (the next GEMM's B^T).
@@ -178,6 +211,9 @@ struct eplace_ctx {
   TcGemmMaps tm1{}, tm2{}, tm3[2]{}, tm4[2]{};
 
   ~eplace_ctx() {
+    pool.reset();
+    if (gexec) cudaGraphExecDestroy(gexec);
+    for (auto e : slot_ev) cudaEventDestroy(e);
     if (stream) cudaStreamDestroy(stream);
   }
 };
@@ -297,9 +333,10 @@ void build_matrices(eplace_ctx *c) {
 
 void ensure_log(eplace_ctx *c, size_t iters) {
   if (c->log_cap >= iters + 2) return;
-  c->log_cap = std::max<size_t>(iters + 2, 64);
+  c->log_cap = std::max<size_t>(iters + 2, 1024);
   c->log.alloc(c->log_cap);
   c->log.zero(c->stream);
+  ++c->buf_epoch;
 }
 
 int grid_for(int n, int block, int cap) {
@@ -429,6 +466,7 @@ void setup_tc(eplace_ctx *c) {
   c->tm4[1].op[1] = ops(c->L6g_h, c->L6g_l, H, H, c->Vt_h, c->Vt_l, W);
   CK(cudaStreamSynchronize(s));
   c->tc_ready = true;
+  ++c->buf_epoch;
 }
 
 int *err_ptr(eplace_ctx *c) { return reinterpret_cast<int *>(reinterpret_cast<char *>(c->sc.p) + offsetof(DevScalars, err)); }
@@ -567,7 +605,10 @@ void upload_momentum(eplace_ctx *c, uint64_t iters) {
     m[k] = (a - 1.0) / an;
     a = an;
   }
-  if (c->mom.n < m.size()) c->mom.alloc(m.size());
+  if (c->mom.n < m.size()) {
+    c->mom.alloc(std::max<size_t>(m.size(), 1024));
+    ++c->buf_epoch;
+  }
   c->mom.upload(m.data(), m.size(), c->stream);
 }
 
@@ -814,12 +855,7 @@ eplace_status eplace_run(eplace_ctx *c, const eplace_cfg *cfg, const eplace_opts
   int nthreads = opts.legal_threads > 0 ? opts.legal_threads : (int)std::max(1u, std::thread::hardware_concurrency());
   nthreads = std::min(nthreads, 64);
   std::vector<std::unique_ptr<Checkpoint>> cps;
-  std::vector<std::unique_ptr<Legalizer>> legal;
-  std::unique_ptr<Pool> pool;
-  cudaGraphExec_t gexec = nullptr;
-  cudaGraph_t graph = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-  std::vector<cudaEvent_t> evs;
   eplace_status final_st = EPLACE_OK;
   try {
     CK(cudaSetDevice(c->device));
@@ -828,8 +864,15 @@ eplace_status eplace_run(eplace_ctx *c, const eplace_cfg *cfg, const eplace_opts
     upload_momentum(c, max_iters);
     if (tc) setup_tc(c);
     reset_state(c, isx, isy, cfg);
-    for (int i = 0; i < nthreads; ++i) legal.emplace_back(new Legalizer(hp));
-    pool.reset(new Pool(nthreads));
+    // Host resources persist in the context across runs.
+    if (!c->lbase) c->lbase.reset(new LegalBase(hp));
+    while ((int)c->legal.size() < nthreads) c->legal.emplace_back(new Legalizer(hp, *c->lbase));
+    if (!c->pool || c->pool->size() != nthreads) {
+      c->pool.reset();
+      c->pool.reset(new Pool(nthreads));
+    }
+    auto &legal = c->legal;
+    Pool *pool = c->pool.get();
     const float gamma = (float)cfg->wl_coeff;
     CK(cudaEventCreate(&ev0));
     CK(cudaEventCreate(&ev1));
@@ -850,27 +893,45 @@ eplace_status eplace_run(eplace_ctx *c, const eplace_cfg *cfg, const eplace_opts
     }
     // Pinned snapshot ring.
     const int inflight = std::max(1, std::min(opts.max_inflight, 8));
-    std::vector<std::unique_ptr<PinBuf<float2>>> snaps(inflight);
-    std::vector<std::unique_ptr<PinBuf<IterLog>>> logs(inflight);
-    std::vector<std::unique_ptr<PinBuf<DevScalars>>> scs(inflight);
-    for (int i = 0; i < inflight; ++i) {
-      snaps[i].reset(new PinBuf<float2>());
-      snaps[i]->alloc(hp.N);
-      logs[i].reset(new PinBuf<IterLog>());
-      logs[i]->alloc(interval + 1);
-      scs[i].reset(new PinBuf<DevScalars>());
-      scs[i]->alloc(1);
-      cudaEvent_t e;
-      CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-      evs.push_back(e);
+    if ((int)c->snaps.size() < inflight || c->slot_log_cap < interval + 1 ||
+        (!c->snaps.empty() && c->snaps[0]->n < hp.N)) {
+      c->snaps.clear();
+      c->logs.clear();
+      c->scs.clear();
+      for (auto e : c->slot_ev) cudaEventDestroy(e);
+      c->slot_ev.clear();
+      c->slot_log_cap = std::max<uint64_t>(interval + 1, 16);
+      for (int i = 0; i < inflight; ++i) {
+        c->snaps.emplace_back(new PinBuf<float2>());
+        c->snaps.back()->alloc(hp.N);
+        c->logs.emplace_back(new PinBuf<IterLog>());
+        c->logs.back()->alloc(c->slot_log_cap);
+        c->scs.emplace_back(new PinBuf<DevScalars>());
+        c->scs.back()->alloc(1);
+        cudaEvent_t e;
+        CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        c->slot_ev.push_back(e);
+      }
     }
+    auto &snaps = c->snaps;
+    auto &logs = c->logs;
+    auto &scs = c->scs;
+    auto &evs = c->slot_ev;
+    // The interval graph is reused while nothing it bakes in has changed:
+    // buffers (epoch), interval length, field formula, transform, wl_coeff.
     bool use_graph = opts.use_graphs != 0 && interval > 1;
+    if (c->gexec && (c->g_epoch != c->buf_epoch || c->g_interval != interval || c->g_field != opts.field_mode ||
+                     c->g_tc != tc || c->g_gamma != gamma)) {
+      cudaGraphExecDestroy(c->gexec);
+      c->gexec = nullptr;
+    }
     uint64_t launched_iters = 0;
     auto launch_chunk = [&](const Chunk &ch) {
       uint64_t n = ch.last - ch.first + 1;
       launched_iters += n;
       if (use_graph && n == interval) {
-        if (!gexec) {
+        if (!c->gexec) {
+          cudaGraph_t graph = nullptr;
           CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
           bool ok = true;
           try {
@@ -879,18 +940,23 @@ eplace_status eplace_run(eplace_ctx *c, const eplace_cfg *cfg, const eplace_opts
             ok = false;
           }
           cudaError_t ce = cudaStreamEndCapture(s, &graph);
-          if (!ok || ce != cudaSuccess || cudaGraphInstantiate(&gexec, graph, 0) != cudaSuccess) {
+          if (!ok || ce != cudaSuccess || cudaGraphInstantiate(&c->gexec, graph, 0) != cudaSuccess) {
             // Capture not available (e.g. cooperative nodes): plain launches.
             cudaGetLastError();
             if (graph) cudaGraphDestroy(graph);
-            graph = nullptr;
-            gexec = nullptr;
+            c->gexec = nullptr;
             use_graph = false;
             for (uint64_t k = 0; k < n; ++k) launch_iteration(c, gamma, opts.field_mode, tc);
             return;
           }
+          cudaGraphDestroy(graph);
+          c->g_epoch = c->buf_epoch;
+          c->g_interval = interval;
+          c->g_field = opts.field_mode;
+          c->g_tc = tc;
+          c->g_gamma = gamma;
         }
-        CK(cudaGraphLaunch(gexec, s));
+        CK(cudaGraphLaunch(c->gexec, s));
       } else {
         for (uint64_t k = 0; k < n; ++k) launch_iteration(c, gamma, opts.field_mode, tc);
       }
@@ -1019,7 +1085,7 @@ eplace_status eplace_run(eplace_ctx *c, const eplace_cfg *cfg, const eplace_opts
     res->converged = converged_chunk < chunks.size() ? 1 : 0;
     res->overlap = last_overlap;
     // Wait for the legaliser, then fold the remaining checkpoints.
-    pool.reset();
+    pool->wait_idle();
     fold();
     if (final_st == EPLACE_OK) {
       if (opts.verbose && res->converged)
@@ -1042,7 +1108,7 @@ eplace_status eplace_run(eplace_ctx *c, const eplace_cfg *cfg, const eplace_opts
           by[i] = (float)isy[i];
         }
         double d = 0.0;
-        eplace_status ls = legal[0]->run(bx.data(), by.data(), fsx.data(), fsy.data(), &d);
+        eplace_status ls = c->legal[0]->run(bx.data(), by.data(), fsx.data(), fsy.data(), &d);
         if (ls != EPLACE_OK) {
           final_st = ls;
           set_err(c, "logic");
@@ -1061,12 +1127,10 @@ eplace_status eplace_run(eplace_ctx *c, const eplace_cfg *cfg, const eplace_opts
   } catch (const CudaError &e) {
     final_st = cuda_fail(c, e);
   }
-  pool.reset();
-  if (gexec) cudaGraphExecDestroy(gexec);
-  if (graph) cudaGraphDestroy(graph);
+  // Queued legalisation jobs point into cps: let them finish on every path.
+  if (c->pool) c->pool->wait_idle();
   if (ev0) cudaEventDestroy(ev0);
   if (ev1) cudaEventDestroy(ev1);
-  for (auto e : evs) cudaEventDestroy(e);
   res->total_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
   res->h2d_bytes = g_h2d - h2d0;
   res->d2h_bytes = g_d2h - d2h0;
@@ -1400,7 +1464,8 @@ eplace_status eplace_stage_hpwl(eplace_ctx *c, const int32_t *sx, const int32_t 
 eplace_status eplace_legalize(eplace_ctx *c, const float *x, const float *y, int32_t *sx, int32_t *sy,
                               double *disp) {
   if (!c || (c->hp.N && (!x || !y || !sx || !sy))) return EPLACE_ERR_INVALID;
-  Legalizer L(c->hp);
+  if (!c->lbase) c->lbase.reset(new LegalBase(c->hp));
+  Legalizer L(c->hp, *c->lbase);
   eplace_status st = L.run(x, y, sx, sy, disp);
   if (st != EPLACE_OK) set_err(c, "logic");
   return st;
@@ -1416,7 +1481,8 @@ eplace_status eplace_legalize_host(const eplace_netlist *nl, const eplace_chip *
     return st;
   }
   if (hp.N && (!x || !y || !sx || !sy)) return EPLACE_ERR_INVALID;
-  Legalizer L(hp);
+  LegalBase base(hp);
+  Legalizer L(hp, base);
   st = L.run(x, y, sx, sy, disp);
   if (st != EPLACE_OK) set_err(nullptr, "logic");
   return st;

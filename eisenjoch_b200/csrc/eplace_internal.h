@@ -43,19 +43,28 @@ eplace_status initial_placement(const HostProblem &hp, uint64_t seed, std::vecto
 // compute_pin_weights (placer/common.rs:381-407).
 void pin_weights(const HostProblem &hp, std::vector<double> &w);
 
-// Greedy legaliser (electro_place/mod.rs:206-255), exact ring search.
+// Immutable part of the greedy legaliser, built once per problem: the free
+// map of logic sites with only the fixed cells bound, and the cell order
+// (macros first, then unit cells, each in solver order).
+struct LegalBase {
+  explicit LegalBase(const HostProblem &hp);
+  int32_t W = 0, H = 0, WR = 0;       // WR: 64-bit words per row
+  std::vector<uint64_t> free0;        // per-row bitmaps, bit set = free
+  std::vector<uint32_t> order;
+};
+
+// Greedy legaliser (electro_place/mod.rs:206-255) with the reference's
+// choice and tie-break.  One instance per thread (owns its working map).
 struct Legalizer {
-  explicit Legalizer(const HostProblem &hp);
+  Legalizer(const HostProblem &hp, const LegalBase &base);
   // Returns EPLACE_OK or EPLACE_ERR_NO_BELS.
   eplace_status run(const float *x, const float *y, int32_t *site_x, int32_t *site_y,
                     double *displacement);
 
  private:
   const HostProblem &hp_;
-  std::vector<uint64_t> base_free_;  // per-row bitmaps of free logic sites
+  const LegalBase &base_;
   std::vector<uint64_t> free_;
-  std::vector<uint32_t> order_;      // macros first, then unit cells (solver order)
-  int32_t words_per_row_ = 0;
 };
 
 // total_hpwl (metrics/wirelength.rs:10-51) on the host.

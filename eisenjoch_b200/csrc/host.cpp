@@ -156,26 +156,37 @@ void pin_weights(const HostProblem &hp, std::vector<double> &w) {
 // ---------------------------------------------------------------------------
 // Greedy legaliser (electro_place/mod.rs:206-255).
 // The reference scans every bucket BEL in chipdb order and keeps the first
-// strict minimum of (bx - x)^2 + (by - y)^2.  The same minimum and tie-break
-// (lowest tile index) are found here by visiting rows outward from the
-// target: in one row the best free site is the nearest free bit left of or
-// right of floor(x) (per-row 64-bit free maps), and a row whose dy^2 already
-// exceeds the best cost cannot win or tie.  Macros (w*h > 1, an extension)
-// go first onto fully free blocks, cost measured at the block centre.
+// strict minimum of (bx - x)^2 + (by - y)^2 (f64).  The same choice is found
+// here in two steps per cell:
+//  * fast path: the sites of minimum cost over the whole grid are the
+//    nearest integer point(s) to (x, y) (two per axis only when the
+//    coordinate is exactly k + 1/2).  If one of them is free it is the
+//    answer, and among tied ones the lowest tile wins, as in the scan.
+//  * otherwise rows are visited outward from the target; in one row the
+//    best free site is the nearest free bit left of or right of floor(x)
+//    (64-bit free maps), and a row whose dy^2 already exceeds the best cost
+//    cannot win or tie.
+// Macros (w*h > 1, an extension) go first onto fully free blocks, cost
+// measured at the block centre.
 // ---------------------------------------------------------------------------
-Legalizer::Legalizer(const HostProblem &hp) : hp_(hp) {
-  words_per_row_ = (hp.W + 63) / 64;
-  base_free_.assign((size_t)words_per_row_ * hp.H, 0);
-  for (int32_t y = 0; y < hp.H; ++y)
-    for (int32_t x = 0; x < hp.W; ++x) base_free_[(size_t)y * words_per_row_ + (x >> 6)] |= 1ull << (x & 63);
+LegalBase::LegalBase(const HostProblem &hp) : W(hp.W), H(hp.H) {
+  WR = (W + 63) / 64;
+  free0.assign((size_t)WR * H, ~0ull);
+  if (W % 64) {
+    const uint64_t tail = (1ull << (W % 64)) - 1;
+    for (int32_t y = 0; y < H; ++y) free0[(size_t)y * WR + WR - 1] = tail;
+  }
   for (uint32_t f = 0; f < hp.F; ++f)
-    if (hp.f_logic[f])
-      base_free_[(size_t)hp.fy[f] * words_per_row_ + (hp.fx[f] >> 6)] &= ~(1ull << (hp.fx[f] & 63));
-  order_.reserve(hp.N);
+    if (hp.f_logic[f]) free0[(size_t)hp.fy[f] * WR + (hp.fx[f] >> 6)] &= ~(1ull << (hp.fx[f] & 63));
+  order.reserve(hp.N);
   for (uint32_t i = 0; i < hp.N; ++i)
-    if (hp.cw[i] * hp.ch[i] > 1) order_.push_back(i);
+    if (hp.cw[i] * hp.ch[i] > 1) order.push_back(i);
   for (uint32_t i = 0; i < hp.N; ++i)
-    if (hp.cw[i] * hp.ch[i] == 1) order_.push_back(i);
+    if (hp.cw[i] * hp.ch[i] == 1) order.push_back(i);
+}
+
+Legalizer::Legalizer(const HostProblem &hp, const LegalBase &base) : hp_(hp), base_(base) {
+  free_.resize(base.free0.size());
 }
 
 namespace {
@@ -205,61 +216,103 @@ inline int32_t free_at_or_right(const uint64_t *row, int32_t pos, int32_t W, int
     m = row[w];
   }
 }
+inline bool is_free(const uint64_t *fm, int32_t WR, int32_t x, int32_t y) {
+  return (fm[(size_t)y * WR + (x >> 6)] >> (x & 63)) & 1;
+}
+// Nearest integer(s) to t in [0, n): one, or two when t is exactly k + 1/2.
+inline int nearest_ints(double t, int32_t n, int32_t (&out)[2]) {
+  double f = std::floor(t);
+  int32_t lo = (int32_t)f;
+  double fr = t - f;
+  int k = 0;
+  if (fr < 0.5) {
+    out[k++] = lo;
+  } else if (fr > 0.5) {
+    out[k++] = lo + 1;
+  } else {
+    out[k++] = lo;
+    out[k++] = lo + 1;
+  }
+  int m = 0;
+  for (int i = 0; i < k; ++i)
+    if (out[i] >= 0 && out[i] < n) out[m++] = out[i];
+  return m;
+}
 }  // namespace
 
 eplace_status Legalizer::run(const float *x, const float *y, int32_t *site_x, int32_t *site_y,
                              double *displacement) {
-  const int32_t W = hp_.W, H = hp_.H, WR = words_per_row_;
-  free_ = base_free_;
+  const int32_t W = hp_.W, H = hp_.H, WR = base_.WR;
+  std::copy(base_.free0.begin(), base_.free0.end(), free_.begin());
   uint64_t *fm = free_.data();
   double total = 0.0;
-  for (uint32_t i : order_) {
+  for (uint32_t i : base_.order) {
     const double tx = (double)x[i], ty = (double)y[i];
     const int w = hp_.cw[i], h = hp_.ch[i];
     double best = INFINITY;
     int64_t best_t = -1;
     if (w == 1 && h == 1) {
-      int32_t cy = (int32_t)std::floor(ty + 0.5);
-      cy = std::min(std::max(cy, 0), H - 1);
-      const int32_t fx0 = (int32_t)std::floor(tx);
-      auto scan_row = [&](int32_t row) {
-        const uint64_t *r = fm + (size_t)row * WR;
-        const double dy = (double)row - ty;
-        const double dy2 = dy * dy;
-        int32_t l = free_at_or_left(r, std::min(fx0, W - 1));
-        int32_t rr = free_at_or_right(r, fx0 + 1, W, WR);
-        for (int32_t c : {l, rr}) {
-          if (c < 0) continue;
-          double dx = (double)c - tx;
-          double cost = dx * dx + dy2;
-          int64_t t = (int64_t)row * W + c;
-          if (cost < best || (cost == best && t < best_t)) {
-            best = cost;
-            best_t = t;
+      // fast path: a free site of minimum cost over the whole grid
+      int32_t xs[2], ys[2];
+      const int nx = (tx >= 0.0 && tx <= (double)(W - 1)) ? nearest_ints(tx, W, xs) : 0;
+      const int ny = (ty >= 0.0 && ty <= (double)(H - 1)) ? nearest_ints(ty, H, ys) : 0;
+      for (int a = 0; a < ny && best_t < 0; ++a)
+        for (int b = 0; b < nx; ++b)
+          if (is_free(fm, WR, xs[b], ys[a])) {
+            const double dx = (double)xs[b] - tx, dy = (double)ys[a] - ty;
+            best = dx * dx + dy * dy;
+            best_t = (int64_t)ys[a] * W + xs[b];
+            break;
           }
-        }
-      };
-      scan_row(cy);
-      bool up = true, down = true;
-      for (int32_t d = 1; up || down; ++d) {
-        if (down) {
-          int32_t row = cy - d;
-          if (row < 0) {
-            down = false;
-          } else {
-            double dy = (double)row - ty;
-            if (best_t >= 0 && dy * dy > best) down = false;
-            else scan_row(row);
+      if (best_t < 0) {
+        int32_t cy = (int32_t)std::floor(ty + 0.5);
+        cy = std::min(std::max(cy, 0), H - 1);
+        const int32_t fx0 = (int32_t)std::floor(tx);
+        auto scan_row = [&](int32_t row) {
+          const uint64_t *r = fm + (size_t)row * WR;
+          const double dy = (double)row - ty;
+          const double dy2 = dy * dy;
+          const int32_t l = free_at_or_left(r, std::min(fx0, W - 1));
+          const int32_t rr = free_at_or_right(r, fx0 + 1, W, WR);
+          if (l >= 0) {
+            const double dx = (double)l - tx, cost = dx * dx + dy2;
+            const int64_t t = (int64_t)row * W + l;
+            if (cost < best || (cost == best && t < best_t)) {
+              best = cost;
+              best_t = t;
+            }
           }
-        }
-        if (up) {
-          int32_t row = cy + d;
-          if (row >= H) {
-            up = false;
-          } else {
-            double dy = (double)row - ty;
-            if (best_t >= 0 && dy * dy > best) up = false;
-            else scan_row(row);
+          if (rr >= 0) {
+            const double dx = (double)rr - tx, cost = dx * dx + dy2;
+            const int64_t t = (int64_t)row * W + rr;
+            if (cost < best || (cost == best && t < best_t)) {
+              best = cost;
+              best_t = t;
+            }
+          }
+        };
+        scan_row(cy);
+        bool up = true, down = true;
+        for (int32_t d = 1; up || down; ++d) {
+          if (down) {
+            const int32_t row = cy - d;
+            if (row < 0) {
+              down = false;
+            } else {
+              const double dy = (double)row - ty;
+              if (best_t >= 0 && dy * dy > best) down = false;
+              else scan_row(row);
+            }
+          }
+          if (up) {
+            const int32_t row = cy + d;
+            if (row >= H) {
+              up = false;
+            } else {
+              const double dy = (double)row - ty;
+              if (best_t >= 0 && dy * dy > best) up = false;
+              else scan_row(row);
+            }
           }
         }
       }
@@ -268,13 +321,13 @@ eplace_status Legalizer::run(const float *x, const float *y, int32_t *site_x, in
       const double ox = 0.5 * (w - 1), oy = 0.5 * (h - 1);
       const int32_t AW = W - w + 1, AH = H - h + 1;
       if (AW > 0 && AH > 0) {
-        int32_t cx = std::min(std::max((int32_t)std::floor(tx - ox + 0.5), 0), AW - 1);
-        int32_t cy = std::min(std::max((int32_t)std::floor(ty - oy + 0.5), 0), AH - 1);
+        const int32_t cx = std::min(std::max((int32_t)std::floor(tx - ox + 0.5), 0), AW - 1);
+        const int32_t cy = std::min(std::max((int32_t)std::floor(ty - oy + 0.5), 0), AH - 1);
         auto block_free = [&](int32_t ax, int32_t ay) {
           for (int dy = 0; dy < h; ++dy) {
             const uint64_t *r = fm + (size_t)(ay + dy) * WR;
             for (int dx = 0; dx < w; ++dx) {
-              int32_t xx = ax + dx;
+              const int32_t xx = ax + dx;
               if (!((r[xx >> 6] >> (xx & 63)) & 1)) return false;
             }
           }
@@ -283,16 +336,16 @@ eplace_status Legalizer::run(const float *x, const float *y, int32_t *site_x, in
         const int32_t rmax = std::max(AW, AH);
         for (int32_t r = 0; r <= rmax; ++r) {
           if (best_t >= 0 && r >= 1 && (double)(r - 1) * (double)(r - 1) > best) break;
-          int32_t y0 = cy - r, y1 = cy + r, x0 = cx - r, x1 = cx + r;
+          const int32_t y0 = cy - r, y1 = cy + r, x0 = cx - r, x1 = cx + r;
           for (int32_t ay = std::max(y0, 0); ay <= std::min(y1, AH - 1); ++ay) {
-            bool full = (ay == y0 || ay == y1);
-            int32_t stepx = full ? 1 : std::max(x1 - x0, 1);
+            const bool full = (ay == y0 || ay == y1);
+            const int32_t stepx = full ? 1 : std::max(x1 - x0, 1);
             for (int32_t ax = x0; ax <= x1; ax += stepx) {
               if (ax < 0 || ax >= AW) continue;
               if (!block_free(ax, ay)) continue;
-              double dx = ((double)ax + ox) - tx, dy = ((double)ay + oy) - ty;
-              double cost = dx * dx + dy * dy;
-              int64_t t = (int64_t)ay * W + ax;
+              const double dx = ((double)ax + ox) - tx, dy = ((double)ay + oy) - ty;
+              const double cost = dx * dx + dy * dy;
+              const int64_t t = (int64_t)ay * W + ax;
               if (cost < best || (cost == best && t < best_t)) {
                 best = cost;
                 best_t = t;
@@ -306,7 +359,7 @@ eplace_status Legalizer::run(const float *x, const float *y, int32_t *site_x, in
     const int32_t bx = (int32_t)(best_t % W), by = (int32_t)(best_t / W);
     for (int dy = 0; dy < h; ++dy)
       for (int dx = 0; dx < w; ++dx) {
-        int32_t xx = bx + dx;
+        const int32_t xx = bx + dx;
         fm[(size_t)(by + dy) * WR + (xx >> 6)] &= ~(1ull << (xx & 63));
       }
     site_x[i] = bx;

@@ -1,0 +1,157 @@
+"""CPU tests of the product library without a GPU: the C ABI loads and
+exports every function include/eplace.h declares, the config defaults,
+and the host parts of the path (initial placement, legaliser, HPWL,
+generator, the place_cells flattening) against the oracle."""
+
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+import eisenjoch_b200 as E
+from eisenjoch_b200 import _abi
+from oracle import oracle as O
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def header_functions():
+    with open(os.path.join(ROOT, "include", "eplace.h")) as f:
+        text = f.read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(eplace_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_function():
+    L = _abi.lib()
+    names = header_functions()
+    assert len(names) >= 20
+    for n in names:
+        assert hasattr(L, n), n
+    assert set(names) == set(_abi.PROTOTYPES), set(names) ^ set(_abi.PROTOTYPES)
+    assert L.eplace_abi_version() == 1
+
+
+def test_config_defaults_match_reference():  # tests/electro_place_tests.rs:97-109
+    c = _abi.Cfg()
+    _abi.lib().eplace_cfg_default(ctypes.byref(c))
+    py = E.ElectroPlaceCfg()
+    assert (c.seed, c.wl_coeff, c.target_util, c.timing_driven, c.target_density, c.timing_weight,
+            c.nesterov_step_size, c.max_iters, c.legalize_interval) == (1, 0.5, 0.7, 0, 1.0, 0.0, 0.1, 500, 5)
+    assert (py.seed, py.wl_coeff, py.target_util, py.timing_driven, py.target_density, py.timing_weight,
+            py.nesterov_step_size, py.max_iters, py.legalize_interval) == (1, 0.5, 0.7, False, 1.0, 0.0, 0.1, 500, 5)
+
+
+def test_context_needs_a_device_here():
+    nl, chip = E.synth_netlist(E.SynthSpec(seed=1, num_cells=10, num_nets=11, num_pads=2, width=8, height=8))
+    with pytest.raises(E.EplaceError) as e:
+        E.PlacementContext(nl, chip)
+    assert e.value.status == _abi.EPLACE_ERR_NO_DEVICE
+
+
+# --- generator --------------------------------------------------------------
+def test_generator_is_deterministic_and_well_formed():
+    spec = E.SynthSpec(seed=3, num_cells=5000, num_nets=5500, num_pads=400, width=128, height=128)
+    a, chip = E.synth_netlist(spec)
+    b, _ = E.synth_netlist(spec)
+    assert np.array_equal(a.pin_cell, b.pin_cell) and np.array_equal(a.net_offsets, b.net_offsets)
+    deg = np.diff(a.net_offsets.astype(np.int64))
+    # cell pins only (pads are appended users)
+    cell_deg = np.array([(a.pin_cell[a.net_offsets[n]:a.net_offsets[n + 1]] < 5000).sum() for n in range(5500)])
+    frac2 = (cell_deg == 2).mean()
+    assert 0.55 < frac2 < 0.65
+    assert ((cell_deg >= 21) & (cell_deg <= 200)).mean() < 0.05
+    assert deg.sum() == a.num_pins == cell_deg.sum() + 400
+    for n in range(0, 5500, 37):
+        cells = a.pin_cell[a.net_offsets[n]:a.net_offsets[n + 1]]
+        assert len(np.unique(cells)) == len(cells)
+        assert cells[0] < 5000  # the driver is a cell
+    # pads on the perimeter walk, all distinct
+    on_edge = (a.fixed_x == 0) | (a.fixed_x == 127) | (a.fixed_y == 0) | (a.fixed_y == 127)
+    assert on_edge.all() and len(set(zip(a.fixed_x, a.fixed_y))) == 400
+
+
+def test_generator_macros():
+    nl, _ = E.synth_netlist(E.SynthSpec(seed=2, num_cells=20000, num_nets=22000, num_pads=100, width=512,
+                                        height=512, bins_x=256, bins_y=256, cluster_size=64, macro_fraction=0.05))
+    m = nl.cell_w > 1
+    assert 0.04 < m.mean() < 0.06
+    assert nl.cell_w[m].min() == 2 and nl.cell_w[m].max() == 8 and (nl.cell_w == nl.cell_h).all()
+
+
+# --- host parts against the oracle -------------------------------------------
+def _case(seed, n, w, macro=0.0, fixed_logic=0):
+    nl, chip = E.synth_netlist(E.SynthSpec(seed=seed, num_cells=n, num_nets=int(1.1 * n), num_pads=12, width=w,
+                                           height=w, cluster_size=16, macro_fraction=macro))
+    if fixed_logic:
+        rng = np.random.default_rng(seed)
+        tiles = rng.choice(w * w, fixed_logic, replace=False)
+        nl.fixed_x = np.concatenate([nl.fixed_x, (tiles % w).astype(np.int32)])
+        nl.fixed_y = np.concatenate([nl.fixed_y, (tiles // w).astype(np.int32)])
+        nl.fixed_on_logic = np.concatenate([np.zeros(12, np.uint8), np.ones(fixed_logic, np.uint8)])
+    return nl, chip
+
+
+@pytest.mark.parametrize("macro,fixed", [(0.0, 0), (0.05, 0), (0.0, 40), (0.05, 40)])
+def test_host_legaliser_equals_reference_scan(macro, fixed):
+    nl, chip = _case(21, 220, 32, macro, fixed)
+    o = O.Oracle(nl, chip)
+    rng = np.random.default_rng(7)
+    for trial in range(9):
+        if trial % 3 == 0:
+            x = (rng.integers(0, 62, nl.num_cells) / 2.0).astype(np.float32)
+            y = (rng.integers(0, 62, nl.num_cells) / 2.0).astype(np.float32)
+        elif trial % 3 == 1:
+            x = np.clip(rng.normal(9, 2.5, nl.num_cells), 0, 31).astype(np.float32)
+            y = np.clip(rng.normal(22, 2.5, nl.num_cells), 0, 31).astype(np.float32)
+        else:
+            x = rng.uniform(0, 31, nl.num_cells).astype(np.float32)
+            y = rng.uniform(0, 31, nl.num_cells).astype(np.float32)
+        st, ox, oy, od = o.legalize(x, y, 0)
+        if st != 0:  # fragmentation left no block for a macro: both must fail alike
+            assert st == 1
+            with pytest.raises(E.NoBelsAvailable):
+                E.placer.legalize_host(nl, chip, x, y)
+            continue
+        sx, sy, d = E.placer.legalize_host(nl, chip, x, y)
+        assert np.array_equal(sx, ox) and np.array_equal(sy, oy) and d == od
+        assert E.placer.hpwl_host(nl, chip, sx, sy) == o.hpwl(sx, sy)
+
+
+@pytest.mark.parametrize("seed", [1, 7, 99])
+def test_host_initial_placement_equals_oracle(seed):
+    nl, chip = _case(22, 400, 32, 0.05, 30)
+    sx, sy = E.placer.initial_placement_host(nl, chip, seed)
+    st, ox, oy = O.Oracle(nl, chip).initial_placement(seed)
+    assert st == 0 and np.array_equal(sx, ox) and np.array_equal(sy, oy)
+
+
+def test_host_errors():
+    nl, chip = _case(23, 20, 8)
+    bad = E.Netlist(num_cells=2, net_offsets=np.array([0, 2], np.uint32), pin_cell=np.array([0, 9], np.uint32))
+    with pytest.raises(E.EplaceError):
+        E.placer.hpwl_host(bad, chip, np.zeros(2, np.int32), np.zeros(2, np.int32))
+    full = E.Netlist(num_cells=70, net_offsets=np.array([0], np.uint32), pin_cell=np.zeros(0, np.uint32))
+    with pytest.raises(E.NoBelsAvailable):
+        E.placer.initial_placement_host(full, chip, 1)
+
+
+def test_lock_others_flattening():
+    """with_locked_others (placer/common.rs:502-530): bound cells outside the
+    set become fixed cells on their logic BELs; pin ids are remapped."""
+    nl, chip = _case(24, 30, 8)
+    nl.cell_init_x = (np.arange(30) % 8).astype(np.int32)
+    nl.cell_init_y = (np.arange(30) // 8).astype(np.int32)
+    sub, target = E.lock_others(nl, [3, 5, 11])
+    assert sub.num_cells == 3 and sub.num_fixed == nl.num_fixed + 27
+    assert (sub.fixed_on_logic[nl.num_fixed:] == 1).all()
+    # every pin still names the same physical location
+    def loc(n, pid):
+        if pid < n.num_cells:
+            return (int(n.cell_init_x[pid]), int(n.cell_init_y[pid]))
+        f = pid - n.num_cells
+        return (int(n.fixed_x[f]), int(n.fixed_y[f]))
+    for p in range(nl.num_pins):
+        assert loc(nl, nl.pin_cell[p]) == loc(sub, sub.pin_cell[p])
