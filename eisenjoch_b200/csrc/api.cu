@@ -164,6 +164,7 @@ struct eplace_ctx {
   DBuf<uint32_t> net_off, pin_cell;
   DBuf<uint8_t> has_driver;
   DBuf<WaTask> wa_tasks;
+  DBuf<uint32_t> wa_off, wa_pins;  // CSR copy, nets ordered by pin count
   DBuf<float2> half;
   DBuf<float> area, pw;
   // state
@@ -175,7 +176,7 @@ struct eplace_ctx {
   DBuf<float> mB3g, mL6g;                   // potential-gradient field (extension)
   DBuf<float> wx, gx2, wy, gy2;
   DBuf<GemmOp> ops;                         // 0: GEMM1, 1: GEMM2, 2-3: GEMM3, 4-5: GEMM4
-  DBuf<double> mom, part;
+  DBuf<double> mom, part, part2;
   DBuf<DevScalars> sc;
   DBuf<IterLog> log;
   DBuf<unsigned> bar;  // [0..1] grid barrier, [2] finalise ticket, [3] step ticket
@@ -234,25 +235,48 @@ eplace_status cuda_fail(eplace_ctx *c, const CudaError &e) {
 
 // Packs whole nets into warp tasks of at most 32 pins (and 32 nets); a net
 // with more than 32 pins gets a task of its own.
-std::vector<WaTask> build_wa_tasks(const HostProblem &hp) {
+// The WA kernel works on a copy of the CSR with the nets ordered by pin
+// count (stable), so each warp task holds nets of similar size.  Net order
+// does not change the result: the gradient accumulates in fixed point.
+void degree_sorted_csr(const HostProblem &hp, std::vector<uint32_t> &off, std::vector<uint32_t> &pins) {
+  std::vector<uint32_t> order(hp.NN);
+  for (uint32_t n = 0; n < hp.NN; ++n) order[n] = n;
+  std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
+    return hp.net_off[a + 1] - hp.net_off[a] < hp.net_off[b + 1] - hp.net_off[b];
+  });
+  off.assign(hp.NN + 1, 0);
+  pins.resize(hp.P);
+  uint32_t k = 0;
+  for (uint32_t i = 0; i < hp.NN; ++i) {
+    const uint32_t n = order[i];
+    for (uint32_t q = hp.net_off[n]; q < hp.net_off[n + 1]; ++q) pins[k++] = hp.pin_cell[q];
+    off[i + 1] = k;
+  }
+}
+
+// Packs whole nets into warp tasks of at most 32 pins (and 32 nets); a net
+// with more than 32 pins gets a task of its own.
+std::vector<WaTask> build_wa_tasks(const std::vector<uint32_t> &off) {
   std::vector<WaTask> t;
+  const uint32_t NN = (uint32_t)off.size() - 1;
   uint32_t n = 0;
-  while (n < hp.NN) {
-    const uint32_t b = hp.net_off[n];
-    const uint32_t d = hp.net_off[n + 1] - b;
+  while (n < NN) {
+    const uint32_t b = off[n];
+    const uint32_t d = off[n + 1] - b;
     if (d > 32) {
       t.push_back(make_int4((int)b, (int)(b + d), (int)n, 1));
       ++n;
       continue;
     }
     uint32_t m = n, e = b;
-    while (m < hp.NN && m - n < 32) {
-      const uint32_t dd = hp.net_off[m + 1] - hp.net_off[m];
-      if (dd > 32 || (hp.net_off[m + 1] - b) > 32) break;
-      e = hp.net_off[m + 1];
+    while (m < NN && m - n < 32) {
+      const uint32_t dd = off[m + 1] - off[m];
+      if (dd > 32 || (off[m + 1] - b) > 32) break;
+      e = off[m + 1];
       ++m;
     }
     if (e > b) t.push_back(make_int4((int)b, (int)e, (int)n, (int)(m - n)));
+    if (m == n) ++m;  // a run of empty nets
     n = m;
   }
   return t;
@@ -348,7 +372,7 @@ int grid_for(int n, int block, int cap) {
 
 // --- kernel sequence of one iteration ------------------------------------
 void launch_wa_stage(eplace_ctx *c, float gamma) {
-  WaArgs a{c->wa_tasks.p, (int)c->wa_tasks.n, c->net_off.p, c->pin_cell.p, c->look.p, c->acc.p, c->hp.N, gamma};
+  WaArgs a{c->wa_tasks.p, (int)c->wa_tasks.n, c->wa_off.p, c->wa_pins.p, c->look.p, c->acc.p, c->hp.N, gamma};
   CK(launch_wa(a, grid_for((int)c->wa_tasks.n * 32, kWaBlock, c->num_sms * 16), c->stream));
 }
 
@@ -477,7 +501,7 @@ void launch_final_stage(eplace_ctx *c, double *dens_out, bool tc = false) {
   const double c0 = c->total_area / (double)nb;
   FinalArgs a{c->dens.p, nb, (double)hp.sx * hp.sy, c0, tc ? nullptr : c->rho.p, tc ? c->rho_h.p : nullptr,
               tc ? c->rho_l.p : nullptr, dens_out, c->part.p, c->bar.p + 2, c->sc.p, c->log.p};
-  CK(launch_density_final(a, grid_for(nb, kFinalBlock, c->num_sms * 2), c->stream));
+  CK(launch_density_final(a, grid_for(nb, kFinalBlock, c->num_sms * 4), c->stream));
 }
 
 // One of the four GEMM launches of a field solve (density.rs:96-166):
@@ -573,6 +597,7 @@ StepArgs step_args(eplace_ctx *c) {
   a.sc = c->sc.p;
   a.log = c->log.p;
   a.part = c->part.p;
+  a.part2 = c->part2.p;
   a.bar = c->bar.p;
   a.ticket = c->bar.p + 3;
   a.mode = 0;
@@ -694,7 +719,13 @@ eplace_status eplace_ctx_create(const eplace_netlist *nl, const eplace_chip *chi
     c->pin_cell.upload(hp.pin_cell.data(), hp.P, s);
     c->has_driver.alloc(hp.NN);
     c->has_driver.upload(hp.has_driver.data(), hp.NN, s);
-    std::vector<WaTask> tasks = build_wa_tasks(hp);
+    std::vector<uint32_t> soff, spins;
+    degree_sorted_csr(hp, soff, spins);
+    c->wa_off.alloc(soff.size());
+    c->wa_off.upload(soff.data(), soff.size(), s);
+    c->wa_pins.alloc(spins.size());
+    c->wa_pins.upload(spins.data(), spins.size(), s);
+    std::vector<WaTask> tasks = build_wa_tasks(soff);
     c->wa_tasks.alloc(tasks.size());
     c->wa_tasks.upload(tasks.data(), tasks.size(), s);
     std::vector<float2> half(hp.N);
@@ -727,8 +758,12 @@ eplace_status eplace_ctx_create(const eplace_netlist *nl, const eplace_chip *chi
     c->dens.zero(s);
     for (auto *b : {&c->rho, &c->T, &c->Exh, &c->Eyh, &c->U, &c->V, &c->Ex, &c->Ey}) b->alloc(nb);
     build_matrices(c.get());
-    c->step_grid = std::max(1, std::min(step_max_grid(device), grid_for((int)hp.N, kStepBlock, 1 << 30)));
-    c->part.alloc(4 * (size_t)std::max(c->step_grid, c->num_sms * 2) + 8);
+    // Two blocks per SM: enough to stream the cells, few arrivals per grid
+    // barrier (the grid must stay co-resident for the cooperative launch).
+    c->step_grid = std::max(1, std::min({step_max_grid(device), c->num_sms * 2,
+                                         grid_for((int)hp.N, kStepBlock, 1 << 30)}));
+    c->part.alloc(4 * (size_t)std::max(c->step_grid, c->num_sms * 4) + 8);
+    c->part2.alloc(2 * (size_t)c->step_grid + 8);
     c->sc.alloc(1);
     c->bar.alloc(4);
     c->bar.zero(s);
@@ -805,6 +840,7 @@ struct Checkpoint {
   std::vector<int32_t> sx, sy;
   double disp = 0.0;
   int64_t hpwl = 0;
+  double secs = 0.0;  // host time of its legalisation + HPWL
   eplace_status st = EPLACE_OK;
   std::atomic<bool> done{false};
 };
@@ -839,9 +875,15 @@ eplace_status eplace_run(eplace_ctx *c, const eplace_cfg *cfg, const eplace_opts
   if (mst != EPLACE_OK) return mst;
   const bool tc = opts.dct_mode == EPLACE_DCT_BF16X3_TC;
   if (!res->bel_tile && hp.N) return EPLACE_ERR_INVALID;
+  // Host phase times, printed with verbose >= 2.
+  std::vector<std::pair<const char *, double>> marks;
+  auto mark = [&](const char *what) {
+    marks.emplace_back(what, std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count());
+  };
   std::string msg;
   std::vector<int32_t> isx, isy;
   eplace_status st = initial_placement(hp, cfg->seed, isx, isy, msg);
+  mark("initial_placement");
   if (st != EPLACE_OK) {
     set_err(c, msg);
     return st;
@@ -864,6 +906,7 @@ eplace_status eplace_run(eplace_ctx *c, const eplace_cfg *cfg, const eplace_opts
     upload_momentum(c, max_iters);
     if (tc) setup_tc(c);
     reset_state(c, isx, isy, cfg);
+    mark("device_reset");
     // Host resources persist in the context across runs.
     if (!c->lbase) c->lbase.reset(new LegalBase(hp));
     while ((int)c->legal.size() < nthreads) c->legal.emplace_back(new Legalizer(hp, *c->lbase));
@@ -1061,10 +1104,12 @@ eplace_status eplace_run(eplace_ctx *c, const eplace_cfg *cfg, const eplace_opts
       Checkpoint *raw = cp.get();
       cps.push_back(std::move(cp));
       pool->submit([raw, &legal, &hp](int tid) {
+        const auto t0 = std::chrono::steady_clock::now();
         raw->sx.resize(hp.N);
         raw->sy.resize(hp.N);
         raw->st = legal[tid]->run(raw->xs.data(), raw->ys.data(), raw->sx.data(), raw->sy.data(), &raw->disp);
         if (raw->st == EPLACE_OK) raw->hpwl = hpwl_host(hp, raw->sx.data(), raw->sy.data());
+        raw->secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         raw->done.store(true, std::memory_order_release);
       });
       // Convergence (mod.rs:190-195).
@@ -1077,6 +1122,7 @@ eplace_status eplace_run(eplace_ctx *c, const eplace_cfg *cfg, const eplace_opts
     }
     CK(cudaEventRecord(ev1, s));
     CK(cudaStreamSynchronize(s));
+    mark("device_loop_done");
     float ms = 0.f;
     CK(cudaEventElapsedTime(&ms, ev0, ev1));
     res->gpu_seconds = ms * 1e-3;
@@ -1086,6 +1132,7 @@ eplace_status eplace_run(eplace_ctx *c, const eplace_cfg *cfg, const eplace_opts
     res->overlap = last_overlap;
     // Wait for the legaliser, then fold the remaining checkpoints.
     pool->wait_idle();
+    mark("legalisation_done");
     fold();
     if (final_st == EPLACE_OK) {
       if (opts.verbose && res->converged)
@@ -1121,7 +1168,7 @@ eplace_status eplace_run(eplace_ctx *c, const eplace_cfg *cfg, const eplace_opts
           if (res->x) res->x[i] = bx[i];
           if (res->y) res->y[i] = by[i];
         }
-        res->hpwl = hpwl_host(hp, fsx.data(), fsy.data());
+        res->hpwl = best ? best->hpwl : hpwl_host(hp, fsx.data(), fsy.data());
       }
     }
   } catch (const CudaError &e) {
@@ -1132,6 +1179,18 @@ eplace_status eplace_run(eplace_ctx *c, const eplace_cfg *cfg, const eplace_opts
   if (ev0) cudaEventDestroy(ev0);
   if (ev1) cudaEventDestroy(ev1);
   res->total_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+  if (opts.verbose >= 2) {
+    std::fprintf(stderr, "eplace_run phases (ms from start):");
+    for (auto &m : marks) std::fprintf(stderr, " %s=%.2f", m.first, m.second * 1e3);
+    std::fprintf(stderr, " end=%.2f\n", res->total_seconds * 1e3);
+    double sum = 0.0, mx = 0.0;
+    for (auto &cp : cps) {
+      sum += cp->secs;
+      mx = std::max(mx, cp->secs);
+    }
+    std::fprintf(stderr, "eplace_run legalisations: %zu, mean %.2f ms, max %.2f ms, threads %d\n", cps.size(),
+                 cps.empty() ? 0.0 : 1e3 * sum / cps.size(), 1e3 * mx, nthreads);
+  }
   res->h2d_bytes = g_h2d - h2d0;
   res->d2h_bytes = g_d2h - d2h0;
   return final_st;

@@ -232,24 +232,42 @@ __global__ void __launch_bounds__(128, 1)
         for (int i = 0; i < 32; ++i) split_store(out.hi, out.lo, (size_t)(n0 + c0 + i) * M + r, v[i]);
       } else {
         // Spectral scaling + Poisson + field spectra (density.rs:114-153),
-        // written split and row-major as the A operands of the next GEMMs.
+        // written split and row-major as the A operands of the next GEMMs,
+        // 8 BF16 per 16-byte store.
+        const int ky = r;
+        const float gy2 = epi.gy2[ky], wy = epi.wy[ky];
+        const float sy = (ky == 0) ? 0.5f * epi.scale : epi.scale;
+#pragma unroll 1
+        for (int j = 0; j < 32; j += 8) {
+          uint32_t exh[4], exl[4], eyh[4], eyl[4];
 #pragma unroll
-        for (int i = 0; i < 32; ++i) {
-          const int kx = n0 + c0 + i, ky = r;
-          float s = epi.scale;
-          if (kx == 0) s *= 0.5f;
-          if (ky == 0) s *= 0.5f;
-          const float den = epi.gx2[kx] + epi.gy2[ky];
-          float phi = 0.f, ex = 0.f, ey = 0.f;
-          if (!(den < 1e-30f)) {
-            phi = v[i] * s / den;
-            ex = phi * epi.wx[kx];
-            ey = phi * epi.wy[ky];
+          for (int i = 0; i < 8; i += 2) {
+            float e_x[2], e_y[2];
+#pragma unroll
+            for (int t = 0; t < 2; ++t) {
+              const int kx = n0 + c0 + j + i + t;
+              const float s = (kx == 0) ? 0.5f * sy : sy;
+              const float den = epi.gx2[kx] + gy2;
+              float phi = 0.f;
+              if (!(den < 1e-30f)) phi = v[j + i + t] * s / den;
+              e_x[t] = phi * epi.wx[kx];
+              e_y[t] = phi * wy;
+              if (epi.phi) epi.phi[(size_t)ky * N + kx] = phi;
+            }
+            const __nv_bfloat162 hx = __floats2bfloat162_rn(e_x[0], e_x[1]);
+            const __nv_bfloat162 lx = __floats2bfloat162_rn(e_x[0] - __low2float(hx), e_x[1] - __high2float(hx));
+            const __nv_bfloat162 hy = __floats2bfloat162_rn(e_y[0], e_y[1]);
+            const __nv_bfloat162 ly = __floats2bfloat162_rn(e_y[0] - __low2float(hy), e_y[1] - __high2float(hy));
+            exh[i / 2] = *reinterpret_cast<const uint32_t *>(&hx);
+            exl[i / 2] = *reinterpret_cast<const uint32_t *>(&lx);
+            eyh[i / 2] = *reinterpret_cast<const uint32_t *>(&hy);
+            eyl[i / 2] = *reinterpret_cast<const uint32_t *>(&ly);
           }
-          const size_t o = (size_t)ky * N + kx;
-          split_store(out.hi, out.lo, o, ex);
-          split_store(out.hi2, out.lo2, o, ey);
-          if (epi.phi) epi.phi[o] = phi;
+          const size_t o = (size_t)ky * N + n0 + c0 + j;  // multiple of 8 elements: 16-byte aligned
+          *reinterpret_cast<uint4 *>(out.hi + o) = make_uint4(exh[0], exh[1], exh[2], exh[3]);
+          *reinterpret_cast<uint4 *>(out.lo + o) = make_uint4(exl[0], exl[1], exl[2], exl[3]);
+          *reinterpret_cast<uint4 *>(out.hi2 + o) = make_uint4(eyh[0], eyh[1], eyh[2], eyh[3]);
+          *reinterpret_cast<uint4 *>(out.lo2 + o) = make_uint4(eyl[0], eyl[1], eyl[2], eyl[3]);
         }
       }
     }

@@ -317,39 +317,88 @@ eplace_status Legalizer::run(const float *x, const float *y, int32_t *site_x, in
         }
       }
     } else {
-      // Macro: ring search over anchors around the target anchor.
+      // Macro: anchor rows outward from the target anchor row.  In anchor
+      // row ay, anchor a is valid when sites [a, a + w) are free in rows
+      // ay .. ay + h - 1: AND the rows' free words, then AND w shifted copies
+      // (carrying bits in from the next word).  The best anchor of the row is
+      // the nearest valid bit left of or right of the target anchor column.
       const double ox = 0.5 * (w - 1), oy = 0.5 * (h - 1);
       const int32_t AW = W - w + 1, AH = H - h + 1;
       if (AW > 0 && AH > 0) {
-        const int32_t cx = std::min(std::max((int32_t)std::floor(tx - ox + 0.5), 0), AW - 1);
-        const int32_t cy = std::min(std::max((int32_t)std::floor(ty - oy + 0.5), 0), AH - 1);
-        auto block_free = [&](int32_t ax, int32_t ay) {
+        const double ux = tx - ox, uy = ty - oy;  // target anchor
+        const int32_t cy = std::min(std::max((int32_t)std::floor(uy + 0.5), 0), AH - 1);
+        const int32_t fa = std::min(std::max((int32_t)std::floor(ux), -1), AW - 1);
+        const int32_t lastw = (AW - 1) >> 6;
+        auto valid_word = [&](int32_t ay, int32_t j) -> uint64_t {
+          uint64_t m = ~0ull, mn = ~0ull;
           for (int dy = 0; dy < h; ++dy) {
             const uint64_t *r = fm + (size_t)(ay + dy) * WR;
-            for (int dx = 0; dx < w; ++dx) {
-              const int32_t xx = ax + dx;
-              if (!((r[xx >> 6] >> (xx & 63)) & 1)) return false;
+            m &= r[j];
+            mn &= (j + 1 < WR) ? r[j + 1] : 0ull;
+          }
+          uint64_t v = m;
+          for (int k = 1; k < w; ++k) v &= (m >> k) | (mn << (64 - k));
+          if (j == lastw && ((AW - 1) & 63) != 63) v &= (2ull << ((AW - 1) & 63)) - 1;
+          return v;
+        };
+        auto scan_anchor_row = [&](int32_t ay) {
+          const double dy = ((double)ay + oy) - ty;
+          const double dy2 = dy * dy;
+          auto consider = [&](int32_t a) {
+            const double dx = ((double)a + ox) - tx, cost = dx * dx + dy2;
+            const int64_t t = (int64_t)ay * W + a;
+            if (cost < best || (cost == best && t < best_t)) {
+              best = cost;
+              best_t = t;
+            }
+          };
+          if (fa >= 0) {  // nearest valid anchor <= fa
+            int32_t j = fa >> 6;
+            uint64_t v = valid_word(ay, j) & (((fa & 63) == 63) ? ~0ull : ((2ull << (fa & 63)) - 1));
+            while (true) {
+              if (v) {
+                consider((j << 6) + 63 - __builtin_clzll(v));
+                break;
+              }
+              if (--j < 0) break;
+              v = valid_word(ay, j);
             }
           }
-          return true;
-        };
-        const int32_t rmax = std::max(AW, AH);
-        for (int32_t r = 0; r <= rmax; ++r) {
-          if (best_t >= 0 && r >= 1 && (double)(r - 1) * (double)(r - 1) > best) break;
-          const int32_t y0 = cy - r, y1 = cy + r, x0 = cx - r, x1 = cx + r;
-          for (int32_t ay = std::max(y0, 0); ay <= std::min(y1, AH - 1); ++ay) {
-            const bool full = (ay == y0 || ay == y1);
-            const int32_t stepx = full ? 1 : std::max(x1 - x0, 1);
-            for (int32_t ax = x0; ax <= x1; ax += stepx) {
-              if (ax < 0 || ax >= AW) continue;
-              if (!block_free(ax, ay)) continue;
-              const double dx = ((double)ax + ox) - tx, dy = ((double)ay + oy) - ty;
-              const double cost = dx * dx + dy * dy;
-              const int64_t t = (int64_t)ay * W + ax;
-              if (cost < best || (cost == best && t < best_t)) {
-                best = cost;
-                best_t = t;
+          if (fa + 1 <= AW - 1) {  // nearest valid anchor >= fa + 1
+            const int32_t p = fa + 1;
+            int32_t j = p >> 6;
+            uint64_t v = valid_word(ay, j) & (~0ull << (p & 63));
+            while (true) {
+              if (v) {
+                consider((j << 6) + __builtin_ctzll(v));
+                break;
               }
+              if (++j > lastw) break;
+              v = valid_word(ay, j);
+            }
+          }
+        };
+        scan_anchor_row(cy);
+        bool up = true, down = true;
+        for (int32_t d = 1; up || down; ++d) {
+          if (down) {
+            const int32_t row = cy - d;
+            if (row < 0) {
+              down = false;
+            } else {
+              const double dy = ((double)row + oy) - ty;
+              if (best_t >= 0 && dy * dy > best) down = false;
+              else scan_anchor_row(row);
+            }
+          }
+          if (up) {
+            const int32_t row = cy + d;
+            if (row >= AH) {
+              up = false;
+            } else {
+              const double dy = ((double)row + oy) - ty;
+              if (best_t >= 0 && dy * dy > best) up = false;
+              else scan_anchor_row(row);
             }
           }
         }

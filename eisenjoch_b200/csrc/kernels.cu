@@ -45,19 +45,6 @@ struct OpAdd {
   __device__ float operator()(float a, float b) const { return a + b; }
 };
 
-// Reduction over the lanes [head, end) of a warp segment, result broadcast
-// to every lane of the segment.  Lane l accumulates [l, min(l + 2o, end))
-// at step o, so the head ends with the segment total.
-template <typename Op>
-__device__ __forceinline__ float seg_allreduce(float v, int lane, int end, int head, Op op) {
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    float u = __shfl_down_sync(kFull, v, o);
-    if (lane + o < end) v = op(v, u);
-  }
-  return __shfl_sync(kFull, v, head);
-}
-
 template <typename Op>
 __device__ __forceinline__ float warp_allreduce(float v, Op op) {
 #pragma unroll
@@ -93,27 +80,26 @@ __device__ __forceinline__ void block_sum(double (&v)[K], double *smem /* [32*K]
 }
 
 // Deterministic sum over the per-block partials part[stride*b + k], b <
-// nblocks, for k < K: warp 0 reads them lane-strided and reduces with a
-// fixed tree; the result is broadcast to the whole block through smem.
+// nblocks, for k < K, by the whole block: thread t reads blocks t, t +
+// blockDim, ... with L1-bypassing loads (the partials were written by other
+// SMs), then a fixed-tree block reduction; every thread gets the result.
 template <int K>
 __device__ __forceinline__ void sum_partials(const double *part, int stride, unsigned nblocks,
-                                             double (&out)[K], double *smem /* [K] */) {
-  if (threadIdx.x < 32) {
-    double v[K];
+                                             double (&out)[K], double *smem /* [32*K] */) {
+  double v[K];
 #pragma unroll
-    for (int k = 0; k < K; ++k) v[k] = 0.0;
-    for (unsigned b = threadIdx.x; b < nblocks; b += 32)
+  for (int k = 0; k < K; ++k) v[k] = 0.0;
+  for (unsigned b = threadIdx.x; b < nblocks; b += blockDim.x)
 #pragma unroll
-      for (int k = 0; k < K; ++k) v[k] += ((volatile const double *)part)[(size_t)stride * b + k];
+    for (int k = 0; k < K; ++k) v[k] += __ldcg(part + (size_t)stride * b + k);
+  block_sum<K>(v, smem);
+  __shared__ double bc[K];
+  if (threadIdx.x == 0)
 #pragma unroll
-    for (int k = 0; k < K; ++k) v[k] = warp_sum_d(v[k]);
-    if (threadIdx.x == 0)
-#pragma unroll
-      for (int k = 0; k < K; ++k) smem[k] = v[k];
-  }
+    for (int k = 0; k < K; ++k) bc[k] = v[k];
   __syncthreads();
 #pragma unroll
-  for (int k = 0; k < K; ++k) out[k] = smem[k];
+  for (int k = 0; k < K; ++k) out[k] = bc[k];
   __syncthreads();
 }
 
@@ -123,18 +109,49 @@ __device__ __forceinline__ void sum_partials(const double *part, int stride, uns
 // every exponential in (0, 1], so FP32 cannot overflow.
 //   d_max_i = e+_i/S+ (1 + g (u_i - A+/S+)),  u = x - max
 //   d_min_i = e-_i/S- (1 - g (v_i - A-/S-)),  v = x - min
-__device__ __forceinline__ float wa_pin_grad(float u, float v, float ep, float em, float Sp,
-                                             float Ap, float Sm, float Am, float gamma) {
-  float dmax = (ep / Sp) * (1.0f + gamma * (u - Ap / Sp));
-  float dmin = (em / Sm) * (1.0f - gamma * (v - Am / Sm));
+// iSp / iSm are 1/S+ and 1/S- (one reciprocal per segment).
+__device__ __forceinline__ float wa_pin_grad(float u, float v, float ep, float em, float iSp, float Ap,
+                                             float iSm, float Am, float gamma) {
+  const float dmax = ep * iSp * (1.0f + gamma * (u - Ap * iSp));
+  const float dmin = em * iSm * (1.0f - gamma * (v - Am * iSm));
   return dmax - dmin;
+}
+
+// 2^x for x <= 0 (MUFU.EX2; subnormal results flush to zero, harmless here).
+__device__ __forceinline__ float ex2(float x) {
+  float r;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
+// Segment max / min over the lanes of `mask` (one mask per segment; the
+// segments partition the warp).
+__device__ __forceinline__ float seg_max(float v, unsigned mask) {
+  float r;
+  asm volatile("redux.sync.max.f32 %0, %1, %2;" : "=f"(r) : "f"(v), "r"(mask));
+  return r;
+}
+__device__ __forceinline__ float seg_min(float v, unsigned mask) {
+  float r;
+  asm volatile("redux.sync.min.f32 %0, %1, %2;" : "=f"(r) : "f"(v), "r"(mask));
+  return r;
+}
+
+// Segment sum over [head, end) with `steps` shuffle rounds (2^steps >= the
+// longest segment of the warp), broadcast from the head lane.
+__device__ __forceinline__ float seg_sum(float v, int lane, int end, int head, int steps) {
+  for (int s = 0, o = 1; s < steps; ++s, o <<= 1) {
+    const float u = __shfl_down_sync(kFull, v, o);
+    if (lane + o < end) v += u;
+  }
+  return __shfl_sync(kFull, v, head);
 }
 
 __device__ void wa_big_net(const WaArgs &a, int pb, int pe, int lane) {
   const float kg = a.gamma * kLog2e;
   float mx = -INFINITY, mn = INFINITY, my = -INFINITY, ny = INFINITY;
   for (int q = pb + lane; q < pe; q += 32) {
-    float2 p = a.pos[a.pin_cell[q]];
+    const float2 p = a.pos[a.pin_cell[q]];
     mx = fmaxf(mx, p.x);
     mn = fminf(mn, p.x);
     my = fmaxf(my, p.y);
@@ -146,27 +163,31 @@ __device__ void wa_big_net(const WaArgs &a, int pb, int pe, int lane) {
   ny = warp_allreduce(ny, OpMin());
   float s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   for (int q = pb + lane; q < pe; q += 32) {
-    float2 p = a.pos[a.pin_cell[q]];
-    float ux = p.x - mx, vx = p.x - mn, uy = p.y - my, vy = p.y - ny;
-    float epx = exp2f(kg * ux), emx = exp2f(-kg * vx);
-    float epy = exp2f(kg * uy), emy = exp2f(-kg * vy);
+    const float2 p = a.pos[a.pin_cell[q]];
+    const float ux = p.x - mx, vx = p.x - mn, uy = p.y - my, vy = p.y - ny;
+    const float epx = ex2(kg * ux), emx = ex2(-kg * vx);
+    const float epy = ex2(kg * uy), emy = ex2(-kg * vy);
     s[0] += epx; s[1] += ux * epx; s[2] += emx; s[3] += vx * emx;
     s[4] += epy; s[5] += uy * epy; s[6] += emy; s[7] += vy * emy;
   }
 #pragma unroll
   for (int k = 0; k < 8; ++k) s[k] = warp_allreduce(s[k], OpAdd());
+  const float ipx = 1.0f / s[0], imx = 1.0f / s[2], ipy = 1.0f / s[4], imy = 1.0f / s[6];
   for (int q = pb + lane; q < pe; q += 32) {
-    uint32_t c = a.pin_cell[q];
+    const uint32_t c = a.pin_cell[q];
     if (c >= a.N) continue;
-    float2 p = a.pos[c];
-    float ux = p.x - mx, vx = p.x - mn, uy = p.y - my, vy = p.y - ny;
-    float gx = wa_pin_grad(ux, vx, exp2f(kg * ux), exp2f(-kg * vx), s[0], s[1], s[2], s[3], a.gamma);
-    float gy = wa_pin_grad(uy, vy, exp2f(kg * uy), exp2f(-kg * vy), s[4], s[5], s[6], s[7], a.gamma);
+    const float2 p = a.pos[c];
+    const float ux = p.x - mx, vx = p.x - mn, uy = p.y - my, vy = p.y - ny;
+    const float gx = wa_pin_grad(ux, vx, ex2(kg * ux), ex2(-kg * vx), ipx, s[1], imx, s[3], a.gamma);
+    const float gy = wa_pin_grad(uy, vy, ex2(kg * uy), ex2(-kg * vy), ipy, s[5], imy, s[7], a.gamma);
     atomicAdd(&a.acc[2 * c], to_fix(gx));
     atomicAdd(&a.acc[2 * c + 1], to_fix(gy));
   }
 }
 
+// Warp tasks come from nets ordered by degree, so the nets of one task have
+// similar pin counts and the segmented sums need only ceil(log2(longest
+// net)) shuffle rounds (one for a task of 2-pin nets).
 __global__ void __launch_bounds__(kWaBlock) k_wa(const WaArgs a) {
   const int lane = threadIdx.x & 31;
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -182,40 +203,48 @@ __global__ void __launch_bounds__(kWaBlock) k_wa(const WaArgs a) {
     // Segment heads: bit j set where a net starts at lane j.
     uint32_t bits = 0;
     if (lane < tk.w) {
-      uint32_t off = a.net_off[tk.z + lane] - (uint32_t)pb;
+      const uint32_t off = a.net_off[tk.z + lane] - (uint32_t)pb;
       if (off < (uint32_t)npin) bits = 1u << off;
     }
     bits = __reduce_or_sync(kFull, bits);
-    const uint32_t le = kFull >> (31 - lane);
-    const int head = 31 - __clz(bits & le);
-    const uint32_t above = bits & ~le;
-    const int end = above ? (__ffs(above) - 1) : npin;
     const bool valid = lane < npin;
+    int head, end;
+    if (valid) {
+      const uint32_t le = kFull >> (31 - lane);
+      head = 31 - __clz(bits & le);
+      const uint32_t above = bits & ~le;
+      end = above ? (__ffs(above) - 1) : npin;
+    } else {  // idle lanes form segments of their own
+      head = lane;
+      end = lane + 1;
+    }
+    const int len = end - head;
+    const unsigned mask = (len == 32) ? kFull : (((1u << len) - 1u) << head);
+    const int maxlen = (int)__reduce_max_sync(kFull, (unsigned)len);
+    const int steps = 32 - __clz(maxlen - 1);  // ceil(log2(maxlen)), 0 for 1
     uint32_t c = 0xffffffffu;
     float2 p = make_float2(0.f, 0.f);
     if (valid) {
       c = a.pin_cell[pb + lane];
       p = a.pos[c];
     }
-    const float mx = seg_allreduce(p.x, lane, end, head, OpMax());
-    const float mn = seg_allreduce(p.x, lane, end, head, OpMin());
-    const float my = seg_allreduce(p.y, lane, end, head, OpMax());
-    const float ny = seg_allreduce(p.y, lane, end, head, OpMin());
+    const float mx = seg_max(p.x, mask), mn = seg_min(p.x, mask);
+    const float my = seg_max(p.y, mask), ny = seg_min(p.y, mask);
     const float ux = p.x - mx, vx = p.x - mn, uy = p.y - my, vy = p.y - ny;
-    const float epx = exp2f(kg * ux), emx = exp2f(-kg * vx);
-    const float epy = exp2f(kg * uy), emy = exp2f(-kg * vy);
-    const float Spx = seg_allreduce(epx, lane, end, head, OpAdd());
-    const float Apx = seg_allreduce(ux * epx, lane, end, head, OpAdd());
-    const float Smx = seg_allreduce(emx, lane, end, head, OpAdd());
-    const float Amx = seg_allreduce(vx * emx, lane, end, head, OpAdd());
-    const float Spy = seg_allreduce(epy, lane, end, head, OpAdd());
-    const float Apy = seg_allreduce(uy * epy, lane, end, head, OpAdd());
-    const float Smy = seg_allreduce(emy, lane, end, head, OpAdd());
-    const float Amy = seg_allreduce(vy * emy, lane, end, head, OpAdd());
+    const float epx = ex2(kg * ux), emx = ex2(-kg * vx);
+    const float epy = ex2(kg * uy), emy = ex2(-kg * vy);
+    const float Spx = seg_sum(epx, lane, end, head, steps);
+    const float Apx = seg_sum(ux * epx, lane, end, head, steps);
+    const float Smx = seg_sum(emx, lane, end, head, steps);
+    const float Amx = seg_sum(vx * emx, lane, end, head, steps);
+    const float Spy = seg_sum(epy, lane, end, head, steps);
+    const float Apy = seg_sum(uy * epy, lane, end, head, steps);
+    const float Smy = seg_sum(emy, lane, end, head, steps);
+    const float Amy = seg_sum(vy * emy, lane, end, head, steps);
     // Nets with fewer than two pins are skipped, as in the reference.
-    if (valid && c < a.N && end - head >= 2) {
-      float gx = wa_pin_grad(ux, vx, epx, emx, Spx, Apx, Smx, Amx, a.gamma);
-      float gy = wa_pin_grad(uy, vy, epy, emy, Spy, Apy, Smy, Amy, a.gamma);
+    if (valid && c < a.N && len >= 2) {
+      const float gx = wa_pin_grad(ux, vx, epx, emx, 1.0f / Spx, Apx, 1.0f / Smx, Amx, a.gamma);
+      const float gy = wa_pin_grad(uy, vy, epy, emy, 1.0f / Spy, Apy, 1.0f / Smy, Amy, a.gamma);
       atomicAdd(&a.acc[2 * c], to_fix(gx));
       atomicAdd(&a.acc[2 * c + 1], to_fix(gy));
     }
@@ -295,9 +324,8 @@ __global__ void __launch_bounds__(kFinalBlock) k_density_final(const FinalArgs a
   __syncthreads();
   if (!last) return;
   __threadfence();
-  __shared__ double red[2];
   double fin[2];
-  sum_partials<2>(a.part, 2, gridDim.x, fin, red);
+  sum_partials<2>(a.part, 2, gridDim.x, fin, sm);
   if (threadIdx.x == 0) {
     const double s = fin[0], o = fin[1];
     const double ov = (s < 1e-30) ? 0.0 : o / s;  // compute_overlap
@@ -418,8 +446,8 @@ __global__ void __launch_bounds__(256) k_sgemm(const GemmOp *ops, int M, int N, 
 __device__ __forceinline__ void grid_barrier(unsigned *bar, DevScalars *sc) {
   __syncthreads();
   if (threadIdx.x == 0) {
-    volatile unsigned *vgen = bar + 1;
-    const unsigned gen = *vgen;
+    unsigned gen;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(gen) : "l"(bar + 1) : "memory");
     __threadfence();
     const unsigned arrived = atomicAdd(bar, 1u);
     if (arrived == gridDim.x - 1) {
@@ -428,12 +456,15 @@ __device__ __forceinline__ void grid_barrier(unsigned *bar, DevScalars *sc) {
       atomicAdd(bar + 1, 1u);
     } else {
       const long long t0 = clock64();
-      while (*vgen == gen) {
+      while (true) {
+        unsigned g;
+        asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(g) : "l"(bar + 1) : "memory");
+        if (g != gen) break;
         if (clock64() - t0 > kSpinCycles) {
           atomicExch(&sc->err, 1);
           break;
         }
-        __nanosleep(64);
+        __nanosleep(32);
       }
     }
     __threadfence();
@@ -447,6 +478,39 @@ __device__ __forceinline__ float2 gather_cell(const StepArgs &a, uint32_t i, flo
   const float2 hf = a.half ? a.half[i] : make_float2(0.5f, 0.5f);
   const Foot f = make_foot(p, hf.x, hf.y, a.BX, a.BY, a.inv_sx, a.inv_sy);
   float fx = 0.f, fy = 0.f, wt = 0.f;
+  if (hf.x == 0.5f && hf.y == 0.5f) {
+    // A 1x1 footprint touches at most 2 x 2 bins (bins are >= 1 site wide):
+    // weights first, then all field loads at once, summed in the same
+    // row-major order as the general loop below.
+    float w[4];
+    size_t id[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int by = f.by0 + (k >> 1), bx = f.bx0 + (k & 1);
+      const bool in = by < f.by1 && bx < f.bx1;
+      w[k] = in ? overlap_1d(f.xlo, f.xhi, bx, a.sx) * overlap_1d(f.ylo, f.yhi, by, a.sy) : 0.0f;
+      id[k] = (w[k] > 0.0f) ? (size_t)by * a.BX + bx : 0;
+    }
+    float e[4], h[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      e[k] = (w[k] > 0.0f) ? a.Ex[id[k]] : 0.0f;
+      h[k] = (w[k] > 0.0f) ? a.Ey[id[k]] : 0.0f;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      if (w[k] > 0.0f) {
+        fx = fmaf(w[k], e[k], fx);
+        fy = fmaf(w[k], h[k], fy);
+        wt += w[k];
+      }
+    float2 g = make_float2(0.f, 0.f);
+    if (wt > 1e-10f) {
+      g.x = fx / wt;
+      g.y = fy / wt;
+    }
+    return g;
+  }
   for (int by = f.by0; by < f.by1; ++by) {
     const float oy = overlap_1d(f.ylo, f.yhi, by, a.sy);
     for (int bx = f.bx0; bx < f.bx1; ++bx) {
@@ -472,9 +536,9 @@ __device__ __forceinline__ float2 gather_cell(const StepArgs &a, uint32_t i, flo
 __device__ __forceinline__ float2 combine(const StepArgs &a, uint32_t i, float2 gw, float2 gd,
                                           double lam) {
   const double ar = a.area ? (double)a.area[i] : 1.0;
-  const double pc = fmax((double)a.pw[i] + lam * ar, 1.0);
-  return make_float2((float)(((double)gw.x + lam * (double)gd.x) / pc),
-                     (float)(((double)gw.y + lam * (double)gd.y) / pc));
+  const double ipc = 1.0 / fmax((double)a.pw[i] + lam * ar, 1.0);
+  return make_float2((float)(((double)gw.x + lam * (double)gd.x) * ipc),
+                     (float)(((double)gw.y + lam * (double)gd.y) * ipc));
 }
 
 __global__ void __launch_bounds__(kStepBlock) k_step(const StepArgs a) {
@@ -525,11 +589,10 @@ __global__ void __launch_bounds__(kStepBlock) k_step(const StepArgs a) {
     for (int k = 0; k < 4; ++k) a.part[4 * blockIdx.x + k] = v[k];
   grid_barrier(a.bar, a.sc);
 
-  __shared__ double red[4];
   if (!was_init) {
     // First penalty: 0.1 * |g_wl| / |g_den| when |g_den| > 1e-30 (mod.rs:132-138).
     double nr[2];
-    sum_partials<2>(a.part, 4, gridDim.x, nr, red);
+    sum_partials<2>(a.part, 4, gridDim.x, nr, sm);
     const double wl = sqrt(nr[0]);
     const double dn = sqrt(nr[1]);
     if (dn > 1e-30) {
@@ -558,7 +621,7 @@ __global__ void __launch_bounds__(kStepBlock) k_step(const StepArgs a) {
   // nesterov.rs:199-218): |dx.dx / dx.dg| clamped to [1e-4, 1], kept when
   // |dx.dg| < 1e-30.
   double t[4];
-  sum_partials<4>(a.part, 4, gridDim.x, t, red);
+  sum_partials<4>(a.part, 4, gridDim.x, t, sm);
   double alpha[2] = {a.sc->step[0], a.sc->step[1]};
   if (it > 0) {
     for (int ax = 0; ax < 2; ++ax) {
@@ -590,10 +653,11 @@ __global__ void __launch_bounds__(kStepBlock) k_step(const StepArgs a) {
   }
   double w2[2] = {nrm[0], nrm[1]};
   block_sum<2>(w2, sm);
-  grid_barrier(a.bar, a.sc);  // all blocks done reading part[] (phase C sums)
+  // Step norms go to a second partials buffer, so no block has to wait for
+  // the others to finish reading part[]; the last block to arrive sums them.
   if (threadIdx.x == 0) {
-    a.part[4 * blockIdx.x] = w2[0];
-    a.part[4 * blockIdx.x + 1] = w2[1];
+    a.part2[2 * blockIdx.x] = w2[0];
+    a.part2[2 * blockIdx.x + 1] = w2[1];
     __threadfence();
     last = atomicAdd(a.ticket, 1u) == gridDim.x - 1;
   }
@@ -601,7 +665,7 @@ __global__ void __launch_bounds__(kStepBlock) k_step(const StepArgs a) {
   if (!last) return;
   __threadfence();
   double fin[2];
-  sum_partials<2>(a.part, 4, gridDim.x, fin, red);
+  sum_partials<2>(a.part2, 2, gridDim.x, fin, sm);
   if (threadIdx.x == 0) {
     const double s0 = fin[0], s1 = fin[1];
     IterLog &L = a.log[it];

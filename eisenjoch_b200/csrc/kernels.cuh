@@ -100,6 +100,7 @@ struct StepArgs {
   DevScalars *sc;
   IterLog *log;
   double *part;             // [4 * grid]
+  double *part2;            // [2 * grid] step-norm partials
   unsigned *bar;            // grid barrier {count, generation}
   unsigned *ticket;
   int mode;                 // 0: full step; 1: gather only (tmp_den <- density gradient)
@@ -129,7 +130,7 @@ cudaError_t launch_hpwl(const HpwlArgs &a, int grid, cudaStream_t s);
 constexpr int kWaBlock = 256;
 constexpr int kScatterBlock = 256;
 constexpr int kFinalBlock = 256;
-constexpr int kStepBlock = 256;
+constexpr int kStepBlock = 512;
 constexpr int kHpwlBlock = 256;
 
 }  // namespace eplace

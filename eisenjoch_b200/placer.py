@@ -56,7 +56,7 @@ class RunOptions:
     dct_mode: int = _abi.EPLACE_DCT_FP32_SIMT
     legal_threads: int = 0
     use_graphs: bool = True
-    verbose: bool = False
+    verbose: int = 0
     max_inflight: int = 3
     field_mode: int = _abi.EPLACE_FIELD_REFERENCE
 
@@ -66,7 +66,7 @@ class RunOptions:
         o.dct_mode = int(self.dct_mode)
         o.legal_threads = int(self.legal_threads)
         o.use_graphs = int(bool(self.use_graphs))
-        o.verbose = int(bool(self.verbose))
+        o.verbose = int(self.verbose)
         o.max_inflight = int(self.max_inflight)
         o.field_mode = int(self.field_mode)
         return o
