@@ -11,6 +11,8 @@ from .placer import (  # noqa: F401
     ElectroPlaceCfg,
     EplaceError,
     InitialPlacementFailed,
+    JobInfo,
+    JobServer,
     Netlist,
     NoBelsAvailable,
     PlacementContext,
@@ -20,9 +22,17 @@ from .placer import (  # noqa: F401
     PlacerError,
     RunOptions,
     SynthSpec,
+    batched_specs,
+    footprint,
+    hpwl_host,
+    initial_placement_host,
+    legalize_host,
     lock_others,
+    mixed_job_spec,
+    mixed_job_specs,
     place,
     place_electro,
+    served_stream,
     synth_netlist,
     workload,
 )

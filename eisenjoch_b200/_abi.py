@@ -9,6 +9,13 @@ import os
 
 import numpy as np
 
+# The library runs long legalisation kernels and several jobs on separate
+# streams.  With the driver's default of 8 hardware work queues, streams
+# share queues and a short kernel can wait behind a long one of another
+# stream; 32 queues keep them independent.  Read once, when the process
+# creates its CUDA context, so it must be set before any CUDA use.
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libeplace.so")
 
@@ -21,12 +28,15 @@ EPLACE_ERR_OOM = 5
 EPLACE_ERR_CUDA = 6
 EPLACE_ERR_TIMEOUT = 7
 EPLACE_ERR_NO_DEVICE = 8
+EPLACE_PENDING = 9
 
 EPLACE_DCT_FP32_SIMT = 0
 EPLACE_DCT_BF16X3_TC = 1
 
 EPLACE_FIELD_REFERENCE = 0
 EPLACE_FIELD_POTENTIAL_GRADIENT = 1
+EPLACE_LEGAL_HOST = 0
+EPLACE_LEGAL_GPU = 1
 
 P = ctypes.POINTER
 c_u8p = P(ctypes.c_uint8)
@@ -59,7 +69,8 @@ class Opts(ctypes.Structure):
         ("verbose", ctypes.c_int32),
         ("max_inflight", ctypes.c_int32),
         ("field_mode", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 2),
+        ("legal_mode", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 1),
     ]
 
 
@@ -147,6 +158,37 @@ class SynthInfo(ctypes.Structure):
     _fields_ = [("num_pins", ctypes.c_uint32), ("max_degree", ctypes.c_uint32)]
 
 
+class ServerCfg(ctypes.Structure):
+    _fields_ = [
+        ("device", ctypes.c_int32),
+        ("max_jobs", ctypes.c_int32),
+        ("hbm_budget", ctypes.c_uint64),
+        ("legal_threads", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+        ("opts", Opts),
+    ]
+
+
+class JobInfo(ctypes.Structure):
+    _fields_ = [
+        ("queued_seconds", ctypes.c_double),
+        ("run_seconds", ctypes.c_double),
+        ("latency_seconds", ctypes.c_double),
+        ("footprint_bytes", ctypes.c_uint64),
+    ]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [
+        ("submitted", ctypes.c_uint64),
+        ("finished", ctypes.c_uint64),
+        ("running", ctypes.c_uint64),
+        ("queued", ctypes.c_uint64),
+        ("contexts", ctypes.c_uint64),
+        ("device_bytes", ctypes.c_uint64),
+    ]
+
+
 # Every exported symbol of the C ABI with its prototype.
 PROTOTYPES = {
     "eplace_abi_version": (ctypes.c_int32, []),
@@ -167,6 +209,8 @@ PROTOTYPES = {
     ),
     "eplace_stage_hpwl": (ctypes.c_int, [ctypes.c_void_p, c_i32p, c_i32p, c_i64p]),
     "eplace_legalize": (ctypes.c_int, [ctypes.c_void_p, c_f32p, c_f32p, c_i32p, c_i32p, c_f64p]),
+    "eplace_ctx_load": (ctypes.c_int, [ctypes.c_void_p, P(Netlist), P(Chip)]),
+    "eplace_stage_legalize": (ctypes.c_int, [ctypes.c_void_p, c_f32p, c_f32p, c_i32p, c_i32p, c_f64p, c_i64p]),
     "eplace_profile_stages": (ctypes.c_int, [ctypes.c_void_p, P(Cfg), P(Opts), ctypes.c_uint32, c_f64p]),
     "eplace_legalize_host": (ctypes.c_int, [P(Netlist), P(Chip), c_f32p, c_f32p, c_i32p, c_i32p, c_f64p]),
     "eplace_hpwl_host": (ctypes.c_int, [P(Netlist), P(Chip), c_i32p, c_i32p, c_i64p]),
@@ -176,6 +220,13 @@ PROTOTYPES = {
         [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
          ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
     ),
+    "eplace_server_cfg_default": (None, [P(ServerCfg)]),
+    "eplace_server_create": (ctypes.c_int, [P(ServerCfg), P(ctypes.c_void_p)]),
+    "eplace_server_destroy": (None, [ctypes.c_void_p]),
+    "eplace_server_submit": (ctypes.c_int, [ctypes.c_void_p, P(Netlist), P(Chip), P(Cfg), P(ctypes.c_uint64)]),
+    "eplace_server_wait": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int32, P(Result), P(JobInfo)]),
+    "eplace_server_stats_get": (ctypes.c_int, [ctypes.c_void_p, P(ServerStats)]),
+    "eplace_footprint": (ctypes.c_uint64, [P(Netlist), P(Chip)]),
     "eplace_synth_size": (ctypes.c_int, [P(SynthSpec), P(SynthInfo)]),
     "eplace_synth_fill": (ctypes.c_int, [P(SynthSpec), c_u8p, c_u8p, c_i32p, c_i32p, c_u32p, c_u32p]),
 }

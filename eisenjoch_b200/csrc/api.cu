@@ -30,7 +30,9 @@
 
 #include "dct_tc.cuh"
 #include "eplace_internal.h"
+#include "job.h"
 #include "kernels.cuh"
+#include "legalize.cuh"
 
 namespace eplace {
 namespace {
@@ -53,7 +55,8 @@ struct CudaError {
 template <typename T>
 struct DBuf {
   T *p = nullptr;
-  size_t n = 0;
+  size_t n = 0;    // elements in use
+  size_t cap = 0;  // elements allocated
   DBuf() = default;
   DBuf(const DBuf &) = delete;
   DBuf &operator=(const DBuf &) = delete;
@@ -61,8 +64,17 @@ struct DBuf {
   void alloc(size_t count) {
     if (p) cudaFree(p);
     p = nullptr;
-    n = count;
+    n = cap = 0;
     if (count) CK(cudaMalloc(&p, sizeof(T) * count));
+    n = cap = count;
+  }
+  // Room for count elements; reallocates only when the capacity is short.
+  void ensure(size_t count) {
+    if (p && count <= cap) {
+      n = count;
+      return;
+    }
+    alloc(count);
   }
   void upload(const T *h, size_t count, cudaStream_t s) {
     if (count) CK(cudaMemcpyAsync(p, h, sizeof(T) * count, cudaMemcpyHostToDevice, s));
@@ -89,60 +101,36 @@ struct PinBuf {
   }
 };
 
-// Simple FIFO worker pool for the host legaliser.
-class Pool {
- public:
-  explicit Pool(int n) {
-    for (int i = 0; i < n; ++i) th_.emplace_back([this, i] { loop(i); });
-  }
-  ~Pool() {
-    {
-      std::lock_guard<std::mutex> g(m_);
-      stop_ = true;
-    }
-    cv_.notify_all();
-    for (auto &t : th_) t.join();
-  }
-  void submit(std::function<void(int)> f) {
-    {
-      std::lock_guard<std::mutex> g(m_);
-      q_.push_back(std::move(f));
-    }
-    cv_.notify_one();
-  }
-  int size() const { return (int)th_.size(); }
-  // Blocks until the queue is empty and no job is running.
-  void wait_idle() {
-    std::unique_lock<std::mutex> g(m_);
-    idle_cv_.wait(g, [this] { return q_.empty() && active_ == 0; });
-  }
+// What one device legalisation reports back (24 bytes, one copy).
+struct LegalOut {
+  unsigned long long hpwl;  // HPWL accumulator (k_hpwl)
+  double disp;
+  int32_t status;           // 0 ok, 1 no free site
+  int32_t pad_;
+};
 
- private:
-  void loop(int id) {
-    for (;;) {
-      std::function<void(int)> f;
-      {
-        std::unique_lock<std::mutex> g(m_);
-        cv_.wait(g, [this] { return stop_ || !q_.empty(); });
-        if (stop_ && q_.empty()) return;
-        f = std::move(q_.front());
-        q_.pop_front();
-        ++active_;
-      }
-      f(id);
-      {
-        std::lock_guard<std::mutex> g(m_);
-        --active_;
-      }
-      idle_cv_.notify_all();
-    }
+// Device resources of one legalisation in flight: its own copy of the
+// positions, the binding, the cost of each placement and its stream.
+struct LegalSlot {
+  DBuf<float2> pos;
+  DBuf<int2> sites;
+  DBuf<int2> loc;       // [N + F]: pin locations, fixed cells at the end
+  DBuf<double> cost;
+  DBuf<uint64_t> work;  // map in global memory for chips beyond shared memory
+  DBuf<LegalOut> out;
+  PinBuf<LegalOut> hout;
+  uint64_t gen = ~0ull;  // problem load this slot is prepared for
+  cudaStream_t stream = nullptr;
+  cudaEvent_t snap = nullptr, start = nullptr, done = nullptr;
+  LegalSlot() = default;
+  LegalSlot(const LegalSlot &) = delete;
+  LegalSlot &operator=(const LegalSlot &) = delete;
+  ~LegalSlot() {
+    if (snap) cudaEventDestroy(snap);
+    if (start) cudaEventDestroy(start);
+    if (done) cudaEventDestroy(done);
+    if (stream) cudaStreamDestroy(stream);
   }
-  std::vector<std::thread> th_;
-  std::deque<std::function<void(int)>> q_;
-  std::mutex m_;
-  std::condition_variable cv_, idle_cv_;
-  int active_ = 0;
-  bool stop_ = false;
 };
 
 }  // namespace
@@ -176,7 +164,7 @@ struct eplace_ctx {
   DBuf<float> mB3g, mL6g;                   // potential-gradient field (extension)
   DBuf<float> wx, gx2, wy, gy2;
   DBuf<GemmOp> ops;                         // 0: GEMM1, 1: GEMM2, 2-3: GEMM3, 4-5: GEMM4
-  DBuf<double> mom, part, part2;
+  DBuf<double> mom, part, part2, part_b;
   DBuf<DevScalars> sc;
   DBuf<IterLog> log;
   DBuf<unsigned> bar;  // [0..1] grid barrier, [2] finalise ticket, [3] step ticket
@@ -211,7 +199,33 @@ struct eplace_ctx {
   DBuf<__nv_bfloat16> B3gt_h, B3gt_l, L6g_h, L6g_l;
   TcGemmMaps tm1{}, tm2{}, tm3[2]{}, tm4[2]{};
 
+  // Device legaliser: cell order, macro footprints and the base free map
+  // (from lbase), and the slots of legalisations in flight.
+  bool lg_ready = false;
+  DBuf<uint32_t> lg_order;
+  DBuf<uchar2> lg_msize;
+  DBuf<uint64_t> lg_free0;
+  uint32_t lg_nmacro = 0;
+  std::vector<std::unique_ptr<LegalSlot>> lslots;
+  int step_grid_full = 0;
+  // Step as three ordinary launches instead of one cooperative launch: used
+  // whenever other long-running kernels share the device (device legaliser,
+  // several jobs at once), where a grid barrier could wait on blocks that
+  // cannot become resident.
+  bool split_step = false;
+  bool shared_device = false;  // set by the job engine: other jobs' kernels run beside this one
+  int mat_bx = -1, mat_by = -1;  // bin grid the DCT matrices were built for
+  uint64_t load_gen = 0;         // bumped by every (re)load of a problem
+  int n_wa_tasks = 0;
+
+  // Device memory this context holds (allocated capacities).
+  uint64_t device_bytes() const;
+
   ~eplace_ctx() {
+    if (stream) cudaStreamSynchronize(stream);
+    for (auto &l : lslots)
+      if (l && l->stream) cudaStreamSynchronize(l->stream);
+    lslots.clear();
     pool.reset();
     if (gexec) cudaGraphExecDestroy(gexec);
     for (auto e : slot_ev) cudaEventDestroy(e);
@@ -323,18 +337,18 @@ void build_matrices(eplace_ctx *c) {
     gy2[k] = (float)(2.0 * (1.0 - std::cos(w)));
   }
   cudaStream_t s = c->stream;
-  c->mB1.alloc(B1.size()); c->mB1.upload(B1.data(), B1.size(), s);
-  c->mB3.alloc(B3.size()); c->mB3.upload(B3.data(), B3.size(), s);
-  c->mB5.alloc(B5.size()); c->mB5.upload(B5.data(), B5.size(), s);
-  c->mL2.alloc(L2.size()); c->mL2.upload(L2.data(), L2.size(), s);
-  c->mL4.alloc(L4.size()); c->mL4.upload(L4.data(), L4.size(), s);
-  c->mL6.alloc(L6.size()); c->mL6.upload(L6.data(), L6.size(), s);
-  c->mB3g.alloc(B3g.size()); c->mB3g.upload(B3g.data(), B3g.size(), s);
-  c->mL6g.alloc(L6g.size()); c->mL6g.upload(L6g.data(), L6g.size(), s);
-  c->wx.alloc(W); c->wx.upload(wx.data(), W, s);
-  c->gx2.alloc(W); c->gx2.upload(gx2.data(), W, s);
-  c->wy.alloc(H); c->wy.upload(wy.data(), H, s);
-  c->gy2.alloc(H); c->gy2.upload(gy2.data(), H, s);
+  c->mB1.ensure(B1.size()); c->mB1.upload(B1.data(), B1.size(), s);
+  c->mB3.ensure(B3.size()); c->mB3.upload(B3.data(), B3.size(), s);
+  c->mB5.ensure(B5.size()); c->mB5.upload(B5.data(), B5.size(), s);
+  c->mL2.ensure(L2.size()); c->mL2.upload(L2.data(), L2.size(), s);
+  c->mL4.ensure(L4.size()); c->mL4.upload(L4.data(), L4.size(), s);
+  c->mL6.ensure(L6.size()); c->mL6.upload(L6.data(), L6.size(), s);
+  c->mB3g.ensure(B3g.size()); c->mB3g.upload(B3g.data(), B3g.size(), s);
+  c->mL6g.ensure(L6g.size()); c->mL6g.upload(L6g.data(), L6g.size(), s);
+  c->wx.ensure(W); c->wx.upload(wx.data(), W, s);
+  c->gx2.ensure(W); c->gx2.upload(gx2.data(), W, s);
+  c->wy.ensure(H); c->wy.upload(wy.data(), H, s);
+  c->gy2.ensure(H); c->gy2.upload(gy2.data(), H, s);
   // ops[0..5]: reference field; ops[6..11]: potential-gradient field.
   GemmOp ops[12] = {
       {c->rho.p, c->mB1.p, c->T.p, nullptr},
@@ -350,7 +364,7 @@ void build_matrices(eplace_ctx *c) {
       {c->mL4.p, c->U.p, c->Ex.p, nullptr},
       {c->mL6g.p, c->V.p, c->Ey.p, nullptr},
   };
-  c->ops.alloc(12);
+  c->ops.ensure(12);
   c->ops.upload(ops, 12, s);
   CK(cudaStreamSynchronize(s));
 }
@@ -372,8 +386,8 @@ int grid_for(int n, int block, int cap) {
 
 // --- kernel sequence of one iteration ------------------------------------
 void launch_wa_stage(eplace_ctx *c, float gamma) {
-  WaArgs a{c->wa_tasks.p, (int)c->wa_tasks.n, c->wa_off.p, c->wa_pins.p, c->look.p, c->acc.p, c->hp.N, gamma};
-  CK(launch_wa(a, grid_for((int)c->wa_tasks.n * 32, kWaBlock, c->num_sms * 16), c->stream));
+  WaArgs a{c->wa_tasks.p, c->n_wa_tasks, c->wa_off.p, c->wa_pins.p, c->look.p, c->acc.p, c->hp.N, gamma};
+  CK(launch_wa(a, grid_for(c->n_wa_tasks * 32, kWaBlock, c->num_sms * 16), c->stream));
 }
 
 void launch_scatter_stage(eplace_ctx *c) {
@@ -422,8 +436,8 @@ void upload_split(DBuf<__nv_bfloat16> &hi, DBuf<__nv_bfloat16> &lo, const std::v
     h[i] = __float2bfloat16_rn(f);
     l[i] = __float2bfloat16_rn(f - __bfloat162float(h[i]));
   }
-  hi.alloc(v.size());
-  lo.alloc(v.size());
+  hi.ensure(v.size());
+  lo.ensure(v.size());
   hi.upload(h.data(), h.size(), s);
   lo.upload(l.data(), l.size(), s);
 }
@@ -464,7 +478,7 @@ void setup_tc(eplace_ctx *c) {
   const size_t nb = (size_t)W * H;
   for (auto *b : {&c->rho_h, &c->rho_l, &c->Tt_h, &c->Tt_l, &c->Exh_h, &c->Exh_l, &c->Eyh_h, &c->Eyh_l, &c->Ut_h,
                   &c->Ut_l, &c->Vt_h, &c->Vt_l})
-    b->alloc(nb);
+    b->ensure(nb);
   auto ops = [&](const DBuf<__nv_bfloat16> &ah, const DBuf<__nv_bfloat16> &al, int mrows, int k,
                  const DBuf<__nv_bfloat16> &bh, const DBuf<__nv_bfloat16> &bl, int nrows) {
     TcOperandMaps m;
@@ -598,6 +612,7 @@ StepArgs step_args(eplace_ctx *c) {
   a.log = c->log.p;
   a.part = c->part.p;
   a.part2 = c->part2.p;
+  a.part_b = c->part_b.p;
   a.bar = c->bar.p;
   a.ticket = c->bar.p + 3;
   a.mode = 0;
@@ -606,7 +621,8 @@ StepArgs step_args(eplace_ctx *c) {
 
 void launch_step_stage(eplace_ctx *c) {
   StepArgs a = step_args(c);
-  CK(launch_step(a, c->step_grid, c->stream));
+  if (c->split_step) CK(launch_step_split(a, c->step_grid, c->stream));
+  else CK(launch_step(a, c->step_grid, c->stream));
 }
 
 void launch_iteration(eplace_ctx *c, float gamma, int field_mode, bool tc) {
@@ -617,7 +633,7 @@ void launch_iteration(eplace_ctx *c, float gamma, int field_mode, bool tc) {
   launch_step_stage(c);
 }
 
-constexpr int kLaunchesPerIter = 8;
+constexpr int kLaunchesPerIter = 8;  // with the cooperative step; +2 with the split step
 
 void upload_momentum(eplace_ctx *c, uint64_t iters) {
   // FISTA sequence a_0 = 1, a_{k+1} = (1 + sqrt(1 + 4 a_k^2)) / 2; the
@@ -630,11 +646,190 @@ void upload_momentum(eplace_ctx *c, uint64_t iters) {
     m[k] = (a - 1.0) / an;
     a = an;
   }
-  if (c->mom.n < m.size()) {
+  if (c->mom.cap < m.size()) {
     c->mom.alloc(std::max<size_t>(m.size(), 1024));
     ++c->buf_epoch;
   }
   c->mom.upload(m.data(), m.size(), c->stream);
+}
+
+// Uploads what every device legalisation reads: the cell order (macros
+// first), the macros' footprints and the free map with the fixed cells.
+void setup_gpu_legal(eplace_ctx *c) {
+  if (c->lg_ready) return;
+  const HostProblem &hp = c->hp;
+  if (!c->lbase) c->lbase.reset(new LegalBase(hp));
+  const LegalBase &b = *c->lbase;
+  std::vector<uchar2> ms;
+  for (uint32_t i : b.order) {
+    if (hp.cw[i] * hp.ch[i] <= 1) break;
+    ms.push_back(make_uchar2(hp.cw[i], hp.ch[i]));
+  }
+  c->lg_nmacro = (uint32_t)ms.size();
+  c->lg_order.ensure(std::max<size_t>(b.order.size(), 1));
+  c->lg_order.upload(b.order.data(), b.order.size(), c->stream);
+  c->lg_msize.ensure(std::max<size_t>(ms.size(), 1));
+  c->lg_msize.upload(ms.data(), ms.size(), c->stream);
+  c->lg_free0.ensure(b.free0.size());
+  c->lg_free0.upload(b.free0.data(), b.free0.size(), c->stream);
+  CK(cudaStreamSynchronize(c->stream));
+  c->lg_ready = true;
+}
+
+// Sizes slot L for the current problem (capacity reuse) and writes the
+// fixed cells' pin locations after a (re)load.
+void prepare_slot(eplace_ctx *c, LegalSlot &L) {
+  const HostProblem &hp = c->hp;
+  if (L.gen == c->load_gen) return;
+  const size_t N1 = std::max<size_t>(hp.N, 1);
+  L.pos.ensure(N1);
+  L.sites.ensure(N1);
+  L.loc.ensure((size_t)hp.N + hp.F + 1);
+  L.cost.ensure(N1);
+  const int WR = (hp.W + 63) / 64;
+  if (legalize_smem_bytes(WR, hp.H) > kLegalMaxSmem) L.work.ensure((size_t)WR * hp.H + hp.H);
+  std::vector<int2> floc(hp.F);
+  for (uint32_t f = 0; f < hp.F; ++f) floc[f] = make_int2(hp.fx[f], hp.fy[f]);
+  if (hp.F) CK(cudaMemcpyAsync(L.loc.p + hp.N, floc.data(), sizeof(int2) * hp.F, cudaMemcpyHostToDevice, L.stream));
+  g_h2d += sizeof(int2) * hp.F;
+  CK(cudaStreamSynchronize(L.stream));
+  L.gen = c->load_gen;
+}
+
+// Allocates one more legalisation slot (lowest stream priority).
+LegalSlot *new_legal_slot(eplace_ctx *c) {
+  std::unique_ptr<LegalSlot> L(new LegalSlot());
+  int prio_lo = 0, prio_hi = 0;
+  CK(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
+  CK(cudaStreamCreateWithPriority(&L->stream, cudaStreamNonBlocking, prio_lo));
+  CK(cudaEventCreateWithFlags(&L->snap, cudaEventDisableTiming));
+  CK(cudaEventCreate(&L->start));
+  CK(cudaEventCreate(&L->done));
+  L->out.alloc(1);
+  L->hout.alloc(1);
+  prepare_slot(c, *L);
+  c->lslots.push_back(std::move(L));
+  return c->lslots.back().get();
+}
+
+// Legalises slot L's positions and takes the HPWL of the binding, all on
+// L's stream, then copies the 24-byte outcome to pinned memory and records
+// L.done.  The caller has already ordered the positions before this work.
+void launch_gpu_legal(eplace_ctx *c, LegalSlot &L) {
+  const HostProblem &hp = c->hp;
+  CK(cudaMemsetAsync(L.out.p, 0, sizeof(LegalOut), L.stream));
+  CK(cudaEventRecord(L.start, L.stream));
+  LegalArgs a;
+  a.pos = L.pos.p;
+  a.order = c->lg_order.p;
+  a.msize = c->lg_msize.p;
+  a.n_order = (uint32_t)c->lbase->order.size();
+  a.n_macro = c->lg_nmacro;
+  a.free0 = c->lg_free0.p;
+  a.work = L.work.p;
+  a.W = hp.W;
+  a.H = hp.H;
+  a.WR = (hp.W + 63) / 64;
+  a.sites = L.sites.p;
+  a.loc = L.loc.p;
+  a.cost = L.cost.p;
+  a.disp = &L.out.p->disp;
+  a.status = &L.out.p->status;
+  CK(launch_legalize(a, L.stream));
+  HpwlArgs h{c->net_off.p, c->pin_cell.p, c->has_driver.p, L.loc.p, hp.NN, &L.out.p->hpwl};
+  if (hp.NN) CK(launch_hpwl(h, grid_for((int)hp.NN, kHpwlBlock, c->num_sms * 2), L.stream));
+  CK(cudaMemcpyAsync(L.hout.p, L.out.p, sizeof(LegalOut), cudaMemcpyDeviceToHost, L.stream));
+  g_d2h += sizeof(LegalOut);
+  CK(cudaEventRecord(L.done, L.stream));
+}
+
+// (Re)targets a context at a validated problem.  Device buffers only grow
+// (capacity reuse: no frees, which would synchronise the device); the DCT
+// matrices and the tensor-core operands are rebuilt only when the bin grid
+// changes; every captured graph is invalidated.
+void load_into(eplace_ctx *c, HostProblem &&hp_in) {
+  const bool same_bins = c->mat_bx == hp_in.BX && c->mat_by == hp_in.BY;
+  c->hp = std::move(hp_in);
+  const HostProblem &hp = c->hp;
+  cudaStream_t s = c->stream;
+  // host-side structures of the previous problem
+  c->legal.clear();
+  c->lbase.reset();
+  c->lg_ready = false;
+  ++c->load_gen;
+  if (c->gexec) {
+    cudaGraphExecDestroy(c->gexec);
+    c->gexec = nullptr;
+  }
+  ++c->buf_epoch;
+  c->net_off.ensure(hp.net_off.size());
+  c->net_off.upload(hp.net_off.data(), hp.net_off.size(), s);
+  c->pin_cell.ensure(std::max<size_t>(hp.P, 1));
+  c->pin_cell.upload(hp.pin_cell.data(), hp.P, s);
+  c->has_driver.ensure(std::max<size_t>(hp.NN, 1));
+  c->has_driver.upload(hp.has_driver.data(), hp.NN, s);
+  {
+    std::vector<uint32_t> soff, spins;
+    degree_sorted_csr(hp, soff, spins);
+    c->wa_off.ensure(soff.size());
+    c->wa_off.upload(soff.data(), soff.size(), s);
+    c->wa_pins.ensure(std::max<size_t>(spins.size(), 1));
+    c->wa_pins.upload(spins.data(), spins.size(), s);
+    std::vector<WaTask> tasks = build_wa_tasks(soff);
+    c->wa_tasks.ensure(std::max<size_t>(tasks.size(), 1));
+    c->wa_tasks.upload(tasks.data(), tasks.size(), s);
+    c->n_wa_tasks = (int)tasks.size();
+  }
+  const size_t N1 = std::max<size_t>(hp.N, 1);
+  std::vector<float2> half(hp.N);
+  std::vector<float> area(hp.N);
+  double tot = 0.0;
+  for (uint32_t i = 0; i < hp.N; ++i) {
+    half[i] = make_float2(0.5f * hp.cw[i], 0.5f * hp.ch[i]);
+    area[i] = (float)(hp.cw[i] * hp.ch[i]);
+    tot += area[i];
+  }
+  c->total_area = tot;
+  c->half.ensure(N1);
+  c->half.upload(half.data(), hp.N, s);
+  c->area.ensure(N1);
+  c->area.upload(area.data(), hp.N, s);
+  pin_weights(hp, c->pw_host);
+  std::vector<float> pwf(c->pw_host.begin(), c->pw_host.end());
+  c->pw.ensure(N1);
+  c->pw.upload(pwf.data(), hp.N, s);
+  c->look.ensure((size_t)hp.N + hp.F + 1);
+  std::vector<float2> fixed(hp.F);
+  for (uint32_t f = 0; f < hp.F; ++f) fixed[f] = make_float2((float)hp.fx[f], (float)hp.fy[f]);
+  if (hp.F) CK(cudaMemcpyAsync(c->look.p + hp.N, fixed.data(), sizeof(float2) * hp.F, cudaMemcpyHostToDevice, s));
+  g_h2d += sizeof(float2) * hp.F;
+  for (auto *b : {&c->x, &c->xp, &c->g, &c->gprev, &c->tmp_wl, &c->tmp_den}) b->ensure(N1);
+  c->acc.ensure(2 * N1);
+  c->acc.zero(s);
+  const size_t nb = (size_t)hp.BX * hp.BY;
+  c->dens.ensure(nb);
+  c->dens.zero(s);
+  if (!same_bins) {
+    for (auto *b : {&c->rho, &c->T, &c->Exh, &c->Eyh, &c->U, &c->V, &c->Ex, &c->Ey}) b->ensure(nb);
+    build_matrices(c);
+    c->mat_bx = hp.BX;
+    c->mat_by = hp.BY;
+    c->tc_ready = false;
+  }
+  // Two blocks per SM: enough to stream the cells, few arrivals per grid
+  // barrier (the grid must stay co-resident for the cooperative launch).
+  c->step_grid = std::max(1, std::min({step_max_grid(c->device), c->num_sms * 2,
+                                       grid_for((int)hp.N, kStepBlock, 1 << 30)}));
+  c->step_grid_full = c->step_grid;
+  c->part.ensure(4 * (size_t)std::max(c->step_grid, c->num_sms * 4) + 8);
+  c->part2.ensure(2 * (size_t)c->step_grid + 8);
+  c->part_b.ensure(4 * (size_t)c->step_grid + 8);
+  c->bar.zero(s);
+  c->loc.ensure((size_t)hp.N + hp.F + 1);
+  std::vector<int2> floc(hp.F);
+  for (uint32_t f = 0; f < hp.F; ++f) floc[f] = make_int2(hp.fx[f], hp.fy[f]);
+  if (hp.F) CK(cudaMemcpyAsync(c->loc.p + hp.N, floc.data(), sizeof(int2) * hp.F, cudaMemcpyHostToDevice, s));
+  g_h2d += sizeof(int2) * hp.F;
 }
 
 }  // namespace
@@ -684,102 +879,35 @@ eplace_status eplace_ctx_create(const eplace_netlist *nl, const eplace_chip *chi
                                 eplace_ctx **out) {
   if (!out) return EPLACE_ERR_INVALID;
   *out = nullptr;
-  std::unique_ptr<eplace_ctx> c(new eplace_ctx());
   std::string msg;
-  eplace_status st = load_problem(nl, chip, c->hp, msg);
+  HostProblem hp;
+  eplace_status st = load_problem(nl, chip, hp, msg);
   if (st != EPLACE_OK) {
     set_err(nullptr, msg);
     return st;
   }
-  try {
-    int ndev = 0;
-    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
-      set_err(nullptr, "no CUDA device");
-      return EPLACE_ERR_NO_DEVICE;
-    }
-    if (device < 0 || device >= ndev) {
-      set_err(nullptr, "device index out of range");
-      return EPLACE_ERR_INVALID;
-    }
-    c->device = device;
-    CK(cudaSetDevice(device));
-    int major = 0;
-    CK(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device));
-    if (major != 10) {
-      set_err(nullptr, "this library is built for sm_100a (B200) only");
-      return EPLACE_ERR_NO_DEVICE;
-    }
-    CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
-    CK(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device));
-    const HostProblem &hp = c->hp;
-    cudaStream_t s = c->stream;
-    c->net_off.alloc(hp.net_off.size());
-    c->net_off.upload(hp.net_off.data(), hp.net_off.size(), s);
-    c->pin_cell.alloc(hp.P);
-    c->pin_cell.upload(hp.pin_cell.data(), hp.P, s);
-    c->has_driver.alloc(hp.NN);
-    c->has_driver.upload(hp.has_driver.data(), hp.NN, s);
-    std::vector<uint32_t> soff, spins;
-    degree_sorted_csr(hp, soff, spins);
-    c->wa_off.alloc(soff.size());
-    c->wa_off.upload(soff.data(), soff.size(), s);
-    c->wa_pins.alloc(spins.size());
-    c->wa_pins.upload(spins.data(), spins.size(), s);
-    std::vector<WaTask> tasks = build_wa_tasks(soff);
-    c->wa_tasks.alloc(tasks.size());
-    c->wa_tasks.upload(tasks.data(), tasks.size(), s);
-    std::vector<float2> half(hp.N);
-    std::vector<float> area(hp.N);
-    double tot = 0.0;
-    for (uint32_t i = 0; i < hp.N; ++i) {
-      half[i] = make_float2(0.5f * hp.cw[i], 0.5f * hp.ch[i]);
-      area[i] = (float)(hp.cw[i] * hp.ch[i]);
-      tot += area[i];
-    }
-    c->total_area = tot;
-    c->half.alloc(hp.N);
-    c->half.upload(half.data(), hp.N, s);
-    c->area.alloc(hp.N);
-    c->area.upload(area.data(), hp.N, s);
-    pin_weights(hp, c->pw_host);
-    std::vector<float> pwf(c->pw_host.begin(), c->pw_host.end());
-    c->pw.alloc(hp.N);
-    c->pw.upload(pwf.data(), hp.N, s);
-    c->look.alloc((size_t)hp.N + hp.F);
-    std::vector<float2> fixed(hp.F);
-    for (uint32_t f = 0; f < hp.F; ++f) fixed[f] = make_float2((float)hp.fx[f], (float)hp.fy[f]);
-    if (hp.F) CK(cudaMemcpyAsync(c->look.p + hp.N, fixed.data(), sizeof(float2) * hp.F, cudaMemcpyHostToDevice, s));
-    g_h2d += sizeof(float2) * hp.F;
-    for (auto *b : {&c->x, &c->xp, &c->g, &c->gprev, &c->tmp_wl, &c->tmp_den}) b->alloc(hp.N);
-    c->acc.alloc(2 * (size_t)hp.N);
-    c->acc.zero(s);
-    const size_t nb = (size_t)hp.BX * hp.BY;
-    c->dens.alloc(nb);
-    c->dens.zero(s);
-    for (auto *b : {&c->rho, &c->T, &c->Exh, &c->Eyh, &c->U, &c->V, &c->Ex, &c->Ey}) b->alloc(nb);
-    build_matrices(c.get());
-    // Two blocks per SM: enough to stream the cells, few arrivals per grid
-    // barrier (the grid must stay co-resident for the cooperative launch).
-    c->step_grid = std::max(1, std::min({step_max_grid(device), c->num_sms * 2,
-                                         grid_for((int)hp.N, kStepBlock, 1 << 30)}));
-    c->part.alloc(4 * (size_t)std::max(c->step_grid, c->num_sms * 4) + 8);
-    c->part2.alloc(2 * (size_t)c->step_grid + 8);
-    c->sc.alloc(1);
-    c->bar.alloc(4);
-    c->bar.zero(s);
-    c->loc.alloc((size_t)hp.N + hp.F);
-    std::vector<int2> floc(hp.F);
-    for (uint32_t f = 0; f < hp.F; ++f) floc[f] = make_int2(hp.fx[f], hp.fy[f]);
-    if (hp.F) CK(cudaMemcpyAsync(c->loc.p + hp.N, floc.data(), sizeof(int2) * hp.F, cudaMemcpyHostToDevice, s));
-    g_h2d += sizeof(int2) * hp.F;
-    c->hp_total.alloc(1);
-    ensure_log(c.get(), 8);
-    CK(cudaStreamSynchronize(s));
-  } catch (const CudaError &e) {
-    return cuda_fail(nullptr, e);
+  eplace_ctx *c = ctx_new(device, &st);
+  if (!c) return st;
+  st = ctx_load_problem(c, std::move(hp));
+  if (st != EPLACE_OK) {
+    g_thread_error = c->err;
+    delete c;
+    return st;
   }
-  *out = c.release();
+  *out = c;
   return EPLACE_OK;
+}
+
+eplace_status eplace_ctx_load(eplace_ctx *c, const eplace_netlist *nl, const eplace_chip *chip) {
+  if (!c) return EPLACE_ERR_INVALID;
+  std::string msg;
+  HostProblem hp;
+  eplace_status st = load_problem(nl, chip, hp, msg);
+  if (st != EPLACE_OK) {
+    set_err(c, msg);
+    return st;
+  }
+  return ctx_load_problem(c, std::move(hp));
 }
 
 void eplace_ctx_destroy(eplace_ctx *ctx) {
@@ -836,96 +964,136 @@ static void reset_state(eplace_ctx *c, const std::vector<int32_t> &sx, const std
 namespace {
 struct Checkpoint {
   int32_t iter = -1;
+  size_t chunk = 0;
+  // host legaliser: the snapshot and its binding
   std::vector<float> xs, ys;
   std::vector<int32_t> sx, sy;
+  // device legaliser: the slot holding positions and binding
+  int slot = -1;
+  bool discard = false;  // its interval ran past convergence
   double disp = 0.0;
   int64_t hpwl = 0;
-  double secs = 0.0;  // host time of its legalisation + HPWL
+  double secs = 0.0;  // time of its legalisation + HPWL (host clock, or device events)
   eplace_status st = EPLACE_OK;
   std::atomic<bool> done{false};
 };
 }  // namespace
+}  // extern "C"
 
-eplace_status eplace_run(eplace_ctx *c, const eplace_cfg *cfg, const eplace_opts *opts_in,
-                         eplace_result *res) {
-  if (!c || !cfg || !res) return EPLACE_ERR_INVALID;
-  const auto t_start = std::chrono::steady_clock::now();
-  const uint64_t h2d0 = g_h2d, d2h0 = g_d2h;
-  eplace_opts opts;
-  eplace_opts_default(&opts);
-  if (opts_in) opts = *opts_in;
-  const HostProblem &hp = c->hp;
-  res->traj_len = 0;
-  res->iters = 0;
-  res->best_iter = -1;
-  res->converged = 0;
-  res->hpwl = 0;
-  res->overlap = 0.0;
-  res->gpu_seconds = 0.0;
-  res->gpu_launches = 0;
-  if (cfg->legalize_interval == 0) {
-    set_err(c, "legalize_interval must be positive");
-    return EPLACE_ERR_INVALID;
-  }
-  if (!(cfg->wl_coeff > 0) || !std::isfinite(cfg->wl_coeff) || !std::isfinite(cfg->nesterov_step_size)) {
-    set_err(c, "wl_coeff / nesterov_step_size must be finite (wl_coeff > 0)");
-    return EPLACE_ERR_INVALID;
-  }
-  eplace_status mst = check_modes(c, opts);
-  if (mst != EPLACE_OK) return mst;
-  const bool tc = opts.dct_mode == EPLACE_DCT_BF16X3_TC;
-  if (!res->bel_tile && hp.N) return EPLACE_ERR_INVALID;
-  // Host phase times, printed with verbose >= 2.
-  std::vector<std::pair<const char *, double>> marks;
-  auto mark = [&](const char *what) {
-    marks.emplace_back(what, std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count());
+namespace eplace {
+
+// One place_electro run (electro_place/mod.rs:65-204) on a context, as a
+// resumable state machine so that one host thread can drive many runs: the
+// blocking entry point loops pump(true) until done(); the job engine calls
+// pump(false) on each of its jobs in turn.
+//
+// Per interval of legalize_interval iterations (one CUDA graph): the
+// interval's log and scalars are copied to pinned memory, the positions are
+// snapshotted (to pinned memory for the host legaliser, to a device slot for
+// the device legaliser), and the checkpoint is legalised concurrently with
+// the next intervals.  Checkpoints are folded in iteration order (best =
+// first minimum HPWL, common.rs:485-495).
+struct JobState {
+  enum Phase { kInit, kLoop, kLegal, kDone };
+  struct Chunk {
+    uint64_t first, last;
   };
-  std::string msg;
-  std::vector<int32_t> isx, isy;
-  eplace_status st = initial_placement(hp, cfg->seed, isx, isy, msg);
-  mark("initial_placement");
-  if (st != EPLACE_OK) {
-    set_err(c, msg);
-    return st;
-  }
-  if (hp.N == 0) {  // mod.rs:80-82
-    res->total_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
-    return EPLACE_OK;
-  }
-  const uint64_t max_iters = cfg->max_iters;
-  const uint64_t interval = cfg->legalize_interval;
-  int nthreads = opts.legal_threads > 0 ? opts.legal_threads : (int)std::max(1u, std::thread::hardware_concurrency());
-  nthreads = std::min(nthreads, 64);
-  std::vector<std::unique_ptr<Checkpoint>> cps;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-  eplace_status final_st = EPLACE_OK;
-  try {
-    CK(cudaSetDevice(c->device));
-    cudaStream_t s = c->stream;
-    ensure_log(c, max_iters);
-    upload_momentum(c, max_iters);
-    if (tc) setup_tc(c);
-    reset_state(c, isx, isy, cfg);
-    mark("device_reset");
-    // Host resources persist in the context across runs.
-    if (!c->lbase) c->lbase.reset(new LegalBase(hp));
-    while ((int)c->legal.size() < nthreads) c->legal.emplace_back(new Legalizer(hp, *c->lbase));
-    if (!c->pool || c->pool->size() != nthreads) {
-      c->pool.reset();
-      c->pool.reset(new Pool(nthreads));
-    }
-    auto &legal = c->legal;
-    Pool *pool = c->pool.get();
-    const float gamma = (float)cfg->wl_coeff;
-    CK(cudaEventCreate(&ev0));
-    CK(cudaEventCreate(&ev1));
 
-    // Interval boundaries: iterations k with k % interval == 0, plus the last.
-    struct Chunk {
-      uint64_t first, last;
-    };
-    std::vector<Chunk> chunks;
-    {
+  JobState(eplace_ctx *c_, const eplace_cfg &cfg_, const eplace_opts &opts_, eplace_result *res_, Pool *shared)
+      : c(c_), cfg(cfg_), opts(opts_), res(res_), shared_pool(shared) {
+    t_start = std::chrono::steady_clock::now();
+    h2d0 = g_h2d;
+    d2h0 = g_d2h;
+  }
+  ~JobState() {
+    drain();
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+  }
+  bool done() const { return phase == kDone; }
+
+  // Waits until no host legalisation of this job is queued or running and
+  // the device legaliser streams are idle (they read this job's buffers).
+  void drain() {
+    while (outstanding.load(std::memory_order_acquire) != 0) std::this_thread::sleep_for(std::chrono::microseconds(50));
+    for (auto &l : c->lslots)
+      if (l && l->stream) cudaStreamSynchronize(l->stream);
+  }
+
+  void mark(const char *what) {
+    marks.emplace_back(what, std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count());
+  }
+
+  eplace_status start() {
+    const HostProblem &hp = c->hp;
+    res->traj_len = 0;
+    res->iters = 0;
+    res->best_iter = -1;
+    res->converged = 0;
+    res->hpwl = 0;
+    res->overlap = 0.0;
+    res->gpu_seconds = 0.0;
+    res->gpu_launches = 0;
+    phase = kDone;
+    if (cfg.legalize_interval == 0) {
+      set_err(c, "legalize_interval must be positive");
+      return final_st = EPLACE_ERR_INVALID;
+    }
+    if (!(cfg.wl_coeff > 0) || !std::isfinite(cfg.wl_coeff) || !std::isfinite(cfg.nesterov_step_size)) {
+      set_err(c, "wl_coeff / nesterov_step_size must be finite (wl_coeff > 0)");
+      return final_st = EPLACE_ERR_INVALID;
+    }
+    eplace_status mst = check_modes(c, opts);
+    if (mst != EPLACE_OK) return final_st = mst;
+    tc = opts.dct_mode == EPLACE_DCT_BF16X3_TC;
+    gpu_legal = opts.legal_mode == EPLACE_LEGAL_GPU && legalize_supported(hp.W, hp.H);
+    if (!res->bel_tile && hp.N) return final_st = EPLACE_ERR_INVALID;
+    std::string msg;
+    eplace_status st = initial_placement(hp, cfg.seed, isx, isy, msg);
+    mark("initial_placement");
+    if (st != EPLACE_OK) {
+      set_err(c, msg);
+      return final_st = st;
+    }
+    if (hp.N == 0) return EPLACE_OK;  // mod.rs:80-82
+    max_iters = cfg.max_iters;
+    interval = cfg.legalize_interval;
+    gamma = (float)cfg.wl_coeff;
+    try {
+      CK(cudaSetDevice(c->device));
+      cudaStream_t s = c->stream;
+      ensure_log(c, max_iters);
+      upload_momentum(c, max_iters);
+      if (tc) setup_tc(c);
+      const bool want_split = gpu_legal || c->shared_device;
+      if (want_split != c->split_step) {
+        c->split_step = want_split;
+        ++c->buf_epoch;
+      }
+      reset_state(c, isx, isy, &cfg);
+      mark("device_reset");
+      // Host resources persist in the context across runs.
+      if (!c->lbase) c->lbase.reset(new LegalBase(hp));
+      if (gpu_legal) {
+        setup_gpu_legal(c);
+        if (c->legal.empty()) c->legal.emplace_back(new Legalizer(hp, *c->lbase));
+      } else {
+        if (shared_pool) {
+          pool = shared_pool;
+        } else {
+          int n = opts.legal_threads > 0 ? opts.legal_threads : (int)std::max(1u, std::thread::hardware_concurrency());
+          n = std::min(n, 64);
+          if (!c->pool || c->pool->size() != n) {
+            c->pool.reset();
+            c->pool.reset(new Pool(n));
+          }
+          pool = c->pool.get();
+        }
+        while ((int)c->legal.size() < pool->size()) c->legal.emplace_back(new Legalizer(hp, *c->lbase));
+      }
+      CK(cudaEventCreate(&ev0));
+      CK(cudaEventCreate(&ev1));
+      // Interval boundaries: iterations k with k % interval == 0, plus the last.
       uint64_t k = 0;
       while (k < max_iters) {
         uint64_t last = (k == 0) ? 0 : std::min(max_iters - 1, ((k + interval - 1) / interval) * interval);
@@ -933,158 +1101,273 @@ eplace_status eplace_run(eplace_ctx *c, const eplace_cfg *cfg, const eplace_opts
         chunks.push_back({k, last});
         k = last + 1;
       }
-    }
-    // Pinned snapshot ring.
-    const int inflight = std::max(1, std::min(opts.max_inflight, 8));
-    if ((int)c->snaps.size() < inflight || c->slot_log_cap < interval + 1 ||
-        (!c->snaps.empty() && c->snaps[0]->n < hp.N)) {
-      c->snaps.clear();
-      c->logs.clear();
-      c->scs.clear();
-      for (auto e : c->slot_ev) cudaEventDestroy(e);
-      c->slot_ev.clear();
-      c->slot_log_cap = std::max<uint64_t>(interval + 1, 16);
-      for (int i = 0; i < inflight; ++i) {
-        c->snaps.emplace_back(new PinBuf<float2>());
-        c->snaps.back()->alloc(hp.N);
-        c->logs.emplace_back(new PinBuf<IterLog>());
-        c->logs.back()->alloc(c->slot_log_cap);
-        c->scs.emplace_back(new PinBuf<DevScalars>());
-        c->scs.back()->alloc(1);
-        cudaEvent_t e;
-        CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-        c->slot_ev.push_back(e);
+      // Pinned ring of interval outputs (log, scalars, and the positions when
+      // the host legalises).
+      inflight = std::max(1, std::min(opts.max_inflight, 8));
+      if ((int)c->snaps.size() < inflight || c->slot_log_cap < interval + 1 ||
+          (!c->snaps.empty() && c->snaps[0]->n < hp.N)) {
+        c->snaps.clear();
+        c->logs.clear();
+        c->scs.clear();
+        for (auto e : c->slot_ev) cudaEventDestroy(e);
+        c->slot_ev.clear();
+        c->slot_log_cap = std::max<uint64_t>(interval + 1, 16);
+        for (int i = 0; i < inflight; ++i) {
+          c->snaps.emplace_back(new PinBuf<float2>());
+          c->snaps.back()->alloc(hp.N);
+          c->logs.emplace_back(new PinBuf<IterLog>());
+          c->logs.back()->alloc(c->slot_log_cap);
+          c->scs.emplace_back(new PinBuf<DevScalars>());
+          c->scs.back()->alloc(1);
+          cudaEvent_t e;
+          CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+          c->slot_ev.push_back(e);
+        }
       }
+      for (int i = (int)c->lslots.size() - 1; i >= 0; --i) free_slots.push_back(i);
+      // The interval graph is reused while nothing it bakes in has changed:
+      // buffers (epoch), interval length, field formula, transform, wl_coeff.
+      use_graph = opts.use_graphs != 0 && interval > 1;
+      if (c->gexec && (c->g_epoch != c->buf_epoch || c->g_interval != interval || c->g_field != opts.field_mode ||
+                       c->g_tc != tc || c->g_gamma != gamma)) {
+        cudaGraphExecDestroy(c->gexec);
+        c->gexec = nullptr;
+      }
+      converged_chunk = chunks.size();
+      CK(cudaEventRecord(ev0, s));
+      phase = kLoop;
+    } catch (const CudaError &e) {
+      final_st = cuda_fail(c, e);
+      return final_st;
     }
+    return EPLACE_OK;
+  }
+
+  bool slot_available() const { return !free_slots.empty() || (int)c->lslots.size() < kMaxLegalSlots; }
+  int acquire_slot() {
+    if (free_slots.empty()) {
+      new_legal_slot(c);
+      return (int)c->lslots.size() - 1;
+    }
+    const int k = free_slots.back();
+    free_slots.pop_back();
+    prepare_slot(c, *c->lslots[k]);
+    return k;
+  }
+
+  void launch_chunk(const Chunk &ch) {
+    cudaStream_t s = c->stream;
+    const uint64_t n = ch.last - ch.first + 1;
+    launched_iters += n;
+    if (use_graph && n == interval) {
+      if (!c->gexec) {
+        cudaGraph_t graph = nullptr;
+        CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        bool ok = true;
+        try {
+          for (uint64_t k = 0; k < n; ++k) launch_iteration(c, gamma, opts.field_mode, tc);
+        } catch (const CudaError &) {
+          ok = false;
+        }
+        cudaError_t ce = cudaStreamEndCapture(s, &graph);
+        if (!ok || ce != cudaSuccess || cudaGraphInstantiate(&c->gexec, graph, 0) != cudaSuccess) {
+          // Capture not available (e.g. cooperative nodes): plain launches.
+          cudaGetLastError();
+          if (graph) cudaGraphDestroy(graph);
+          c->gexec = nullptr;
+          use_graph = false;
+          for (uint64_t k = 0; k < n; ++k) launch_iteration(c, gamma, opts.field_mode, tc);
+          return;
+        }
+        cudaGraphDestroy(graph);
+        c->g_epoch = c->buf_epoch;
+        c->g_interval = interval;
+        c->g_field = opts.field_mode;
+        c->g_tc = tc;
+        c->g_gamma = gamma;
+      }
+      CK(cudaGraphLaunch(c->gexec, s));
+    } else {
+      for (uint64_t k = 0; k < n; ++k) launch_iteration(c, gamma, opts.field_mode, tc);
+    }
+  }
+
+  void release(Checkpoint *cp) {
+    if (!cp) return;
+    std::vector<float>().swap(cp->xs);
+    std::vector<float>().swap(cp->ys);
+    std::vector<int32_t>().swap(cp->sx);
+    std::vector<int32_t>().swap(cp->sy);
+    if (cp->slot >= 0) {
+      free_slots.push_back(cp->slot);
+      cp->slot = -1;
+    }
+  }
+
+  // Folds finished checkpoints in iteration order; blocking: waits for the
+  // next one if it is still being legalised.  Returns whether any was folded.
+  bool fold(bool blocking) {
+    bool any = false;
+    while (fold_next < cps.size() && final_st == EPLACE_OK) {
+      Checkpoint *cp = cps[fold_next].get();
+      if (cp->chunk >= processed) break;
+      if (gpu_legal) {
+        if (!cp->discard) {
+          LegalSlot &L = *c->lslots[cp->slot];
+          if (blocking) {
+            CK(cudaEventSynchronize(L.done));
+          } else {
+            const cudaError_t q = cudaEventQuery(L.done);
+            if (q == cudaErrorNotReady) break;
+            CK(q);
+          }
+          const LegalOut &o = *L.hout.p;
+          float lms = 0.f;
+          if (cudaEventElapsedTime(&lms, L.start, L.done) == cudaSuccess) cp->secs = 1e-3 * lms;
+          cp->st = o.status == 0 ? EPLACE_OK : EPLACE_ERR_NO_BELS;
+          cp->disp = o.disp;
+          cp->hpwl = (int64_t)o.hpwl;
+        }
+      } else if (!cp->done.load(std::memory_order_acquire)) {
+        if (!blocking) break;
+        while (!cp->done.load(std::memory_order_acquire)) std::this_thread::sleep_for(std::chrono::microseconds(50));
+      }
+      ++fold_next;
+      any = true;
+      if (cp->discard) {
+        release(cp);
+        continue;
+      }
+      if (cp->st != EPLACE_OK) {
+        final_st = cp->st;
+        set_err(c, "logic");
+        break;
+      }
+      const IterLog &L = iterlog[cp->iter];
+      if (res->traj && res->traj_len < res->traj_capacity) {
+        eplace_traj_entry &t = res->traj[res->traj_len++];
+        t.iter = cp->iter;
+        t.hpwl = (double)cp->hpwl;
+        t.displacement = cp->disp;
+        t.step_x = L.step_norm[0];
+        t.step_y = L.step_norm[1];
+        t.density_penalty = L.lam;
+        t.overlap = L.overlap;
+      }
+      if (opts.verbose) {
+        std::fprintf(stderr,
+                     "ElectroPlace iter %d: HPWL=%.0f, disp=%.1f, step=(%.4f,%.4f), density_p=%.3f, overlap=%.4f\n",
+                     cp->iter, (double)cp->hpwl, cp->disp, L.step_norm[0], L.step_norm[1], L.lam, L.overlap);
+      }
+      Checkpoint *drop = cp;
+      if ((double)cp->hpwl < best_metric) {
+        best_metric = (double)cp->hpwl;
+        drop = best;
+        best = cp;
+      }
+      release(drop);
+    }
+    return any;
+  }
+
+  // Launches intervals while allowed, reads finished intervals' outputs and
+  // folds finished legalisations.  block: wait where the loop has to wait
+  // (one interval output per call, as a plain loop would).  Returns whether
+  // anything happened.
+  bool pump(bool block) {
+    if (phase == kDone || phase == kInit) return false;
+    bool progressed = false;
+    try {
+      if (phase == kLoop) progressed |= pump_loop(block);
+      if (phase == kLegal) {
+        if (final_st == EPLACE_OK) {
+          progressed |= fold(false);
+          if (block && fold_next < cps.size()) progressed |= fold(true);
+        }
+        if (final_st != EPLACE_OK || fold_next >= cps.size()) {
+          mark("legalisation_done");
+          phase = kDone;
+          progressed = true;
+        }
+      }
+    } catch (const CudaError &e) {
+      final_st = cuda_fail(c, e);
+      phase = kDone;
+      progressed = true;
+    }
+    return progressed;
+  }
+
+  bool pump_loop(bool block) {
+    const HostProblem &hp = c->hp;
+    cudaStream_t s = c->stream;
     auto &snaps = c->snaps;
     auto &logs = c->logs;
     auto &scs = c->scs;
     auto &evs = c->slot_ev;
-    // The interval graph is reused while nothing it bakes in has changed:
-    // buffers (epoch), interval length, field formula, transform, wl_coeff.
-    bool use_graph = opts.use_graphs != 0 && interval > 1;
-    if (c->gexec && (c->g_epoch != c->buf_epoch || c->g_interval != interval || c->g_field != opts.field_mode ||
-                     c->g_tc != tc || c->g_gamma != gamma)) {
-      cudaGraphExecDestroy(c->gexec);
-      c->gexec = nullptr;
-    }
-    uint64_t launched_iters = 0;
-    auto launch_chunk = [&](const Chunk &ch) {
-      uint64_t n = ch.last - ch.first + 1;
-      launched_iters += n;
-      if (use_graph && n == interval) {
-        if (!c->gexec) {
-          cudaGraph_t graph = nullptr;
-          CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-          bool ok = true;
-          try {
-            for (uint64_t k = 0; k < n; ++k) launch_iteration(c, gamma, opts.field_mode, tc);
-          } catch (const CudaError &) {
-            ok = false;
-          }
-          cudaError_t ce = cudaStreamEndCapture(s, &graph);
-          if (!ok || ce != cudaSuccess || cudaGraphInstantiate(&c->gexec, graph, 0) != cudaSuccess) {
-            // Capture not available (e.g. cooperative nodes): plain launches.
-            cudaGetLastError();
-            if (graph) cudaGraphDestroy(graph);
-            c->gexec = nullptr;
-            use_graph = false;
-            for (uint64_t k = 0; k < n; ++k) launch_iteration(c, gamma, opts.field_mode, tc);
-            return;
-          }
-          cudaGraphDestroy(graph);
-          c->g_epoch = c->buf_epoch;
-          c->g_interval = interval;
-          c->g_field = opts.field_mode;
-          c->g_tc = tc;
-          c->g_gamma = gamma;
-        }
-        CK(cudaGraphLaunch(c->gexec, s));
-      } else {
-        for (uint64_t k = 0; k < n; ++k) launch_iteration(c, gamma, opts.field_mode, tc);
-      }
-    };
-
-    std::deque<std::pair<size_t, int>> pending;  // (chunk index, slot)
-    size_t next_chunk = 0;
-    bool stop = false;
-    size_t converged_chunk = chunks.size();
-    uint64_t iters_done = 0;
-    double last_overlap = 0.0;
-    std::vector<IterLog> iterlog;
-    // Fold legalised checkpoints in iteration order (record_metric,
-    // common.rs:485-495: strict '<' keeps the first best); the positions
-    // and bindings of every checkpoint but the current best are released.
-    Checkpoint *best = nullptr;
-    double best_metric = INFINITY;
-    size_t fold_next = 0;
-    auto fold = [&]() {
-      while (fold_next < cps.size() && final_st == EPLACE_OK) {
-        Checkpoint *cp = cps[fold_next].get();
-        if (!cp->done.load(std::memory_order_acquire)) break;
-        ++fold_next;
-        if (cp->st != EPLACE_OK) {
-          final_st = cp->st;
-          set_err(c, "logic");
+    bool progressed = false;
+    while (!stop && next_chunk < chunks.size() && (int)pending.size() < inflight) {
+      if (gpu_legal && !slot_available()) {
+        if (!pending.empty()) break;  // read the outputs first, then fold
+        if (!fold(block) && !block) break;
+        if (final_st != EPLACE_OK) {
+          stop = true;
           break;
         }
-        const IterLog &L = iterlog[cp->iter];
-        if (res->traj && res->traj_len < res->traj_capacity) {
-          eplace_traj_entry &t = res->traj[res->traj_len++];
-          t.iter = cp->iter;
-          t.hpwl = (double)cp->hpwl;
-          t.displacement = cp->disp;
-          t.step_x = L.step_norm[0];
-          t.step_y = L.step_norm[1];
-          t.density_penalty = L.lam;
-          t.overlap = L.overlap;
-        }
-        if (opts.verbose) {
-          std::fprintf(stderr,
-                       "ElectroPlace iter %d: HPWL=%.0f, disp=%.1f, step=(%.4f,%.4f), density_p=%.3f, overlap=%.4f\n",
-                       cp->iter, (double)cp->hpwl, cp->disp, L.step_norm[0], L.step_norm[1], L.lam, L.overlap);
-        }
-        Checkpoint *drop = cp;
-        if ((double)cp->hpwl < best_metric) {
-          best_metric = (double)cp->hpwl;
-          drop = best;
-          best = cp;
-        }
-        if (drop) {
-          std::vector<float>().swap(drop->xs);
-          std::vector<float>().swap(drop->ys);
-          std::vector<int32_t>().swap(drop->sx);
-          std::vector<int32_t>().swap(drop->sy);
-        }
+        continue;
       }
-    };
-    CK(cudaEventRecord(ev0, s));
-    int slot_rr = 0;
-    while ((!stop && next_chunk < chunks.size()) || !pending.empty()) {
-      while (!stop && next_chunk < chunks.size() && (int)pending.size() < inflight) {
-        const Chunk &ch = chunks[next_chunk];
-        launch_chunk(ch);
-        const int slot = slot_rr;
-        slot_rr = (slot_rr + 1) % inflight;
+      const Chunk &ch = chunks[next_chunk];
+      launch_chunk(ch);
+      const int slot = slot_rr;
+      slot_rr = (slot_rr + 1) % inflight;
+      const uint64_t n = ch.last - ch.first + 1;
+      if (gpu_legal) {
+        // Snapshot on the device and legalise it on the slot's stream.
+        auto cp = std::make_unique<Checkpoint>();
+        cp->iter = (int32_t)ch.last;
+        cp->chunk = next_chunk;
+        cp->slot = acquire_slot();
+        LegalSlot &L = *c->lslots[cp->slot];
+        CK(cudaStreamWaitEvent(s, L.done, 0));  // a reused slot's last legalisation has finished
+        CK(cudaMemcpyAsync(L.pos.p, c->x.p, sizeof(float2) * hp.N, cudaMemcpyDeviceToDevice, s));
+        CK(cudaEventRecord(L.snap, s));
+        CK(cudaStreamWaitEvent(L.stream, L.snap, 0));
+        launch_gpu_legal(c, L);
+        cps.push_back(std::move(cp));
+      } else {
         CK(cudaMemcpyAsync(snaps[slot]->p, c->x.p, sizeof(float2) * hp.N, cudaMemcpyDeviceToHost, s));
-        const uint64_t n = ch.last - ch.first + 1;
-        CK(cudaMemcpyAsync(logs[slot]->p, c->log.p + ch.first, sizeof(IterLog) * n, cudaMemcpyDeviceToHost, s));
-        CK(cudaMemcpyAsync(scs[slot]->p, c->sc.p, sizeof(DevScalars), cudaMemcpyDeviceToHost, s));
-        g_d2h += sizeof(float2) * hp.N + sizeof(IterLog) * n + sizeof(DevScalars);
-        CK(cudaEventRecord(evs[slot], s));
-        pending.push_back({next_chunk, slot});
-        ++next_chunk;
+        g_d2h += sizeof(float2) * hp.N;
       }
-      if (pending.empty()) break;
+      CK(cudaMemcpyAsync(logs[slot]->p, c->log.p + ch.first, sizeof(IterLog) * n, cudaMemcpyDeviceToHost, s));
+      CK(cudaMemcpyAsync(scs[slot]->p, c->sc.p, sizeof(DevScalars), cudaMemcpyDeviceToHost, s));
+      g_d2h += sizeof(IterLog) * n + sizeof(DevScalars);
+      CK(cudaEventRecord(evs[slot], s));
+      pending.push_back({next_chunk, slot});
+      ++next_chunk;
+      progressed = true;
+    }
+    while (!pending.empty()) {
       auto [ci, slot] = pending.front();
+      if (block) {
+        CK(cudaEventSynchronize(evs[slot]));
+      } else {
+        const cudaError_t q = cudaEventQuery(evs[slot]);
+        if (q == cudaErrorNotReady) break;
+        CK(q);
+      }
       pending.pop_front();
-      CK(cudaEventSynchronize(evs[slot]));
-      if (stop) continue;  // ran ahead of convergence: discard
+      progressed = true;
+      processed = ci + 1;
+      if (stop) {  // ran ahead of convergence: discard
+        if (gpu_legal) cps[ci]->discard = true;
+        continue;
+      }
       const Chunk &ch = chunks[ci];
       if (scs[slot]->p->err) {
         set_err(c, "a bounded device wait timed out");
         final_st = EPLACE_ERR_TIMEOUT;
         stop = true;
+        if (gpu_legal) cps[ci]->discard = true;
         continue;
       }
       const uint64_t n = ch.last - ch.first + 1;
@@ -1092,108 +1375,293 @@ eplace_status eplace_run(eplace_ctx *c, const eplace_cfg *cfg, const eplace_opts
       iters_done = ch.last + 1;
       const IterLog &L = logs[slot]->p[n - 1];
       last_overlap = L.overlap;
-      // Legalise this checkpoint on the host pool (mod.rs:176-183).
-      auto cp = std::make_unique<Checkpoint>();
-      cp->iter = (int32_t)ch.last;
-      cp->xs.resize(hp.N);
-      cp->ys.resize(hp.N);
-      for (uint32_t i = 0; i < hp.N; ++i) {
-        cp->xs[i] = snaps[slot]->p[i].x;
-        cp->ys[i] = snaps[slot]->p[i].y;
+      if (!gpu_legal) {
+        // Legalise this checkpoint on the host pool (mod.rs:176-183).
+        auto cp = std::make_unique<Checkpoint>();
+        cp->iter = (int32_t)ch.last;
+        cp->chunk = ci;
+        cp->xs.resize(hp.N);
+        cp->ys.resize(hp.N);
+        for (uint32_t i = 0; i < hp.N; ++i) {
+          cp->xs[i] = snaps[slot]->p[i].x;
+          cp->ys[i] = snaps[slot]->p[i].y;
+        }
+        Checkpoint *raw = cp.get();
+        cps.push_back(std::move(cp));
+        outstanding.fetch_add(1, std::memory_order_acq_rel);
+        eplace_ctx *cc = c;
+        std::atomic<int> *out = &outstanding;
+        pool->submit([raw, cc, out](int tid) {
+          const HostProblem &php = cc->hp;
+          const auto t0 = std::chrono::steady_clock::now();
+          raw->sx.resize(php.N);
+          raw->sy.resize(php.N);
+          raw->st = cc->legal[tid]->run(raw->xs.data(), raw->ys.data(), raw->sx.data(), raw->sy.data(), &raw->disp);
+          if (raw->st == EPLACE_OK) raw->hpwl = hpwl_host(php, raw->sx.data(), raw->sy.data());
+          raw->secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+          raw->done.store(true, std::memory_order_release);
+          out->fetch_sub(1, std::memory_order_acq_rel);
+        });
       }
-      Checkpoint *raw = cp.get();
-      cps.push_back(std::move(cp));
-      pool->submit([raw, &legal, &hp](int tid) {
-        const auto t0 = std::chrono::steady_clock::now();
-        raw->sx.resize(hp.N);
-        raw->sy.resize(hp.N);
-        raw->st = legal[tid]->run(raw->xs.data(), raw->ys.data(), raw->sx.data(), raw->sy.data(), &raw->disp);
-        if (raw->st == EPLACE_OK) raw->hpwl = hpwl_host(hp, raw->sx.data(), raw->sy.data());
-        raw->secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-        raw->done.store(true, std::memory_order_release);
-      });
       // Convergence (mod.rs:190-195).
       if (ch.last >= 20 && L.overlap < 0.1) {
         stop = true;
         converged_chunk = ci;
       }
-      fold();
+      fold(false);
       if (final_st != EPLACE_OK) stop = true;
+      if (block) break;
     }
-    CK(cudaEventRecord(ev1, s));
-    CK(cudaStreamSynchronize(s));
-    mark("device_loop_done");
-    float ms = 0.f;
-    CK(cudaEventElapsedTime(&ms, ev0, ev1));
-    res->gpu_seconds = ms * 1e-3;
-    res->gpu_launches = (uint64_t)kLaunchesPerIter * launched_iters;
-    res->iters = (uint32_t)iters_done;
-    res->converged = converged_chunk < chunks.size() ? 1 : 0;
-    res->overlap = last_overlap;
-    // Wait for the legaliser, then fold the remaining checkpoints.
-    pool->wait_idle();
-    mark("legalisation_done");
-    fold();
-    if (final_st == EPLACE_OK) {
-      if (opts.verbose && res->converged)
-        std::fprintf(stderr, "ElectroPlace converged at iteration %d (overlap %.4f < 0.1)\n",
-                     (int)(iters_done - 1), last_overlap);
-      // Final legalisation of the best snapshot (mod.rs:199).  Its result is
-      // the checkpoint's own binding: legalisation is a pure function of the
-      // positions and the fixed cells.
-      std::vector<int32_t> fsx(hp.N), fsy(hp.N);
-      std::vector<float> bx(hp.N), by(hp.N);
-      if (best) {
-        fsx = best->sx;
-        fsy = best->sy;
-        bx = best->xs;
-        by = best->ys;
-        res->best_iter = best->iter;
-      } else {
-        for (uint32_t i = 0; i < hp.N; ++i) {
-          bx[i] = (float)isx[i];
-          by[i] = (float)isy[i];
+    if (pending.empty() && (stop || next_chunk >= chunks.size())) {
+      // The loop is over: everything before ev1 has already completed.
+      CK(cudaEventRecord(ev1, s));
+      CK(cudaEventSynchronize(ev1));
+      mark("device_loop_done");
+      float ms = 0.f;
+      CK(cudaEventElapsedTime(&ms, ev0, ev1));
+      res->gpu_seconds = ms * 1e-3;
+      res->gpu_launches = (uint64_t)(kLaunchesPerIter + (c->split_step ? 2 : 0)) * launched_iters +
+                          (gpu_legal ? 2 * cps.size() : 0);
+      res->iters = (uint32_t)iters_done;
+      res->converged = converged_chunk < chunks.size() ? 1 : 0;
+      res->overlap = last_overlap;
+      phase = kLegal;
+      progressed = true;
+    }
+    return progressed;
+  }
+
+  // Writes the result (final legalisation = the best checkpoint's binding,
+  // mod.rs:199) and releases what the run holds.  Call once done() (or after
+  // a failed start()).
+  eplace_status finish() {
+    const HostProblem &hp = c->hp;
+    drain();
+    if (final_st == EPLACE_OK && hp.N > 0 && phase == kDone) {
+      try {
+        if (opts.verbose && res->converged)
+          std::fprintf(stderr, "ElectroPlace converged at iteration %d (overlap %.4f < 0.1)\n",
+                       (int)(iters_done - 1), last_overlap);
+        // Legalisation is a pure function of the positions and the fixed
+        // cells, so the final binding is the best checkpoint's own.
+        std::vector<int32_t> fsx(hp.N), fsy(hp.N);
+        std::vector<float> bx(hp.N), by(hp.N);
+        if (best && gpu_legal) {
+          LegalSlot &L = *c->lslots[best->slot];
+          std::vector<int2> sites(hp.N);
+          std::vector<float2> pos(hp.N);
+          CK(cudaMemcpyAsync(sites.data(), L.sites.p, sizeof(int2) * hp.N, cudaMemcpyDeviceToHost, L.stream));
+          CK(cudaMemcpyAsync(pos.data(), L.pos.p, sizeof(float2) * hp.N, cudaMemcpyDeviceToHost, L.stream));
+          g_d2h += (sizeof(int2) + sizeof(float2)) * hp.N;
+          CK(cudaStreamSynchronize(L.stream));
+          for (uint32_t i = 0; i < hp.N; ++i) {
+            fsx[i] = sites[i].x;
+            fsy[i] = sites[i].y;
+            bx[i] = pos[i].x;
+            by[i] = pos[i].y;
+          }
+          res->best_iter = best->iter;
+        } else if (best) {
+          fsx = best->sx;
+          fsy = best->sy;
+          bx = best->xs;
+          by = best->ys;
+          res->best_iter = best->iter;
+        } else {
+          for (uint32_t i = 0; i < hp.N; ++i) {
+            bx[i] = (float)isx[i];
+            by[i] = (float)isy[i];
+          }
+          double d = 0.0;
+          if (!c->lbase) c->lbase.reset(new LegalBase(hp));
+          if (c->legal.empty()) c->legal.emplace_back(new Legalizer(hp, *c->lbase));
+          eplace_status ls = c->legal[0]->run(bx.data(), by.data(), fsx.data(), fsy.data(), &d);
+          if (ls != EPLACE_OK) {
+            final_st = ls;
+            set_err(c, "logic");
+          }
         }
-        double d = 0.0;
-        eplace_status ls = c->legal[0]->run(bx.data(), by.data(), fsx.data(), fsy.data(), &d);
-        if (ls != EPLACE_OK) {
-          final_st = ls;
-          set_err(c, "logic");
+        if (final_st == EPLACE_OK) {
+          for (uint32_t i = 0; i < hp.N; ++i) {
+            res->bel_tile[i] = fsy[i] * hp.W + fsx[i];
+            if (res->bel_index) res->bel_index[i] = 0;
+            if (res->x) res->x[i] = bx[i];
+            if (res->y) res->y[i] = by[i];
+          }
+          res->hpwl = best ? best->hpwl : hpwl_host(hp, fsx.data(), fsy.data());
         }
-      }
-      if (final_st == EPLACE_OK) {
-        for (uint32_t i = 0; i < hp.N; ++i) {
-          res->bel_tile[i] = fsy[i] * hp.W + fsx[i];
-          if (res->bel_index) res->bel_index[i] = 0;
-          if (res->x) res->x[i] = bx[i];
-          if (res->y) res->y[i] = by[i];
-        }
-        res->hpwl = best ? best->hpwl : hpwl_host(hp, fsx.data(), fsy.data());
+      } catch (const CudaError &e) {
+        final_st = cuda_fail(c, e);
       }
     }
+    res->total_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+    if (opts.verbose >= 2) {
+      std::fprintf(stderr, "eplace_run phases (ms from start):");
+      for (auto &m : marks) std::fprintf(stderr, " %s=%.2f", m.first, m.second * 1e3);
+      std::fprintf(stderr, " end=%.2f\n", res->total_seconds * 1e3);
+      double sum = 0.0, mx = 0.0;
+      for (auto &cp : cps) {
+        sum += cp->secs;
+        mx = std::max(mx, cp->secs);
+      }
+      std::fprintf(stderr, "eplace_run legalisations: %zu (%s), mean %.2f ms, max %.2f ms, threads %d\n", cps.size(),
+                   gpu_legal ? "device" : "host", cps.empty() ? 0.0 : 1e3 * sum / cps.size(), 1e3 * mx,
+                   pool ? pool->size() : 0);
+    }
+    res->h2d_bytes = g_h2d - h2d0;
+    res->d2h_bytes = g_d2h - d2h0;
+    return final_st;
+  }
+
+  static constexpr int kMaxLegalSlots = 32;
+  eplace_ctx *c;
+  eplace_cfg cfg;
+  eplace_opts opts;
+  eplace_result *res;
+  Pool *shared_pool;
+  Pool *pool = nullptr;
+  Phase phase = kInit;
+  std::chrono::steady_clock::time_point t_start;
+  uint64_t h2d0 = 0, d2h0 = 0;
+  bool tc = false, gpu_legal = false, use_graph = false;
+  uint64_t max_iters = 0, interval = 1;
+  float gamma = 0.f;
+  std::vector<int32_t> isx, isy;
+  std::vector<std::pair<const char *, double>> marks;
+  std::vector<Chunk> chunks;
+  int inflight = 1;
+  std::vector<int> free_slots;
+  uint64_t launched_iters = 0;
+  std::deque<std::pair<size_t, int>> pending;  // (chunk index, pinned slot)
+  size_t next_chunk = 0, processed = 0;
+  bool stop = false;
+  size_t converged_chunk = 0;
+  uint64_t iters_done = 0;
+  double last_overlap = 0.0;
+  std::vector<IterLog> iterlog;
+  std::vector<std::unique_ptr<Checkpoint>> cps;
+  Checkpoint *best = nullptr;
+  double best_metric = INFINITY;
+  size_t fold_next = 0;
+  int slot_rr = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  eplace_status final_st = EPLACE_OK;
+  std::atomic<int> outstanding{0};
+};
+
+JobState *job_create(eplace_ctx *c, const eplace_cfg &cfg, const eplace_opts &opts, eplace_result *res,
+                     Pool *shared_pool) {
+  return new JobState(c, cfg, opts, res, shared_pool);
+}
+eplace_status job_start(JobState *j) { return j->start(); }
+bool job_pump(JobState *j, bool block) { return j->pump(block); }
+bool job_done(const JobState *j) { return j->done(); }
+eplace_status job_finish(JobState *j) { return j->finish(); }
+void job_destroy(JobState *j) { delete j; }
+void ctx_set_shared(eplace_ctx *c, bool shared) { c->shared_device = shared; }
+uint64_t ctx_device_bytes(const eplace_ctx *c) { return c->device_bytes(); }
+int ctx_bins_x(const eplace_ctx *c) { return c->mat_bx; }
+int ctx_bins_y(const eplace_ctx *c) { return c->mat_by; }
+void set_thread_error(const std::string &m) { set_err(nullptr, m); }
+bool problem_tc_supported(const HostProblem &hp) { return tc_supported(hp); }
+
+uint64_t problem_device_bytes(const HostProblem &hp) {
+  const uint64_t N = hp.N, F = hp.F, NN = hp.NN, P = hp.P;
+  const uint64_t nb = (uint64_t)hp.BX * hp.BY;
+  const uint64_t m = (uint64_t)hp.BX * hp.BX + (uint64_t)hp.BY * hp.BY;
+  return N * 96 + F * 16 + P * 8 + NN * 16 + nb * 64 + m * 48 + (1u << 20);
+}
+
+eplace_ctx *ctx_new(int32_t device, eplace_status *st) {
+  *st = EPLACE_OK;
+  std::unique_ptr<eplace_ctx> c(new eplace_ctx());
+  try {
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+      set_err(nullptr, "no CUDA device");
+      *st = EPLACE_ERR_NO_DEVICE;
+      return nullptr;
+    }
+    if (device < 0 || device >= ndev) {
+      set_err(nullptr, "device index out of range");
+      *st = EPLACE_ERR_INVALID;
+      return nullptr;
+    }
+    c->device = device;
+    CK(cudaSetDevice(device));
+    int major = 0;
+    CK(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device));
+    if (major != 10) {
+      set_err(nullptr, "this library is built for sm_100a (B200) only");
+      *st = EPLACE_ERR_NO_DEVICE;
+      return nullptr;
+    }
+    // The Nesterov loop's stream gets the highest priority: blocks of its
+    // kernels are scheduled ahead of the legaliser's long-running warps.
+    int prio_lo = 0, prio_hi = 0;
+    CK(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
+    CK(cudaStreamCreateWithPriority(&c->stream, cudaStreamNonBlocking, prio_hi));
+    CK(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device));
+    c->sc.alloc(1);
+    c->bar.alloc(4);
+    c->hp_total.alloc(1);
+    ensure_log(c.get(), 8);
+    CK(cudaStreamSynchronize(c->stream));
   } catch (const CudaError &e) {
-    final_st = cuda_fail(c, e);
+    *st = cuda_fail(nullptr, e);
+    return nullptr;
   }
-  // Queued legalisation jobs point into cps: let them finish on every path.
-  if (c->pool) c->pool->wait_idle();
-  if (ev0) cudaEventDestroy(ev0);
-  if (ev1) cudaEventDestroy(ev1);
-  res->total_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
-  if (opts.verbose >= 2) {
-    std::fprintf(stderr, "eplace_run phases (ms from start):");
-    for (auto &m : marks) std::fprintf(stderr, " %s=%.2f", m.first, m.second * 1e3);
-    std::fprintf(stderr, " end=%.2f\n", res->total_seconds * 1e3);
-    double sum = 0.0, mx = 0.0;
-    for (auto &cp : cps) {
-      sum += cp->secs;
-      mx = std::max(mx, cp->secs);
-    }
-    std::fprintf(stderr, "eplace_run legalisations: %zu, mean %.2f ms, max %.2f ms, threads %d\n", cps.size(),
-                 cps.empty() ? 0.0 : 1e3 * sum / cps.size(), 1e3 * mx, nthreads);
+  return c.release();
+}
+
+eplace_status ctx_load_problem(eplace_ctx *c, HostProblem &&hp) {
+  try {
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(c->stream));
+    for (auto &l : c->lslots)
+      if (l && l->stream) CK(cudaStreamSynchronize(l->stream));
+    load_into(c, std::move(hp));
+    CK(cudaStreamSynchronize(c->stream));
+  } catch (const CudaError &e) {
+    return cuda_fail(c, e);
   }
-  res->h2d_bytes = g_h2d - h2d0;
-  res->d2h_bytes = g_d2h - d2h0;
-  return final_st;
+  return EPLACE_OK;
+}
+
+}  // namespace eplace
+
+uint64_t eplace_ctx::device_bytes() const {
+  uint64_t b = 0;
+  auto add = [&b](const auto &buf) { b += (uint64_t)buf.cap * sizeof(*buf.p); };
+  add(net_off); add(pin_cell); add(has_driver); add(wa_tasks); add(wa_off); add(wa_pins);
+  add(half); add(area); add(pw); add(look); add(x); add(xp); add(g); add(gprev); add(tmp_wl); add(tmp_den);
+  add(acc); add(dens); add(rho); add(T); add(Exh); add(Eyh); add(U); add(V); add(Ex); add(Ey); add(phi);
+  add(mB1); add(mL2); add(mB3); add(mL4); add(mB5); add(mL6); add(mB3g); add(mL6g);
+  add(wx); add(gx2); add(wy); add(gy2); add(ops); add(mom); add(part); add(part2); add(part_b);
+  add(sc); add(log); add(bar); add(loc); add(hp_total);
+  add(rho_h); add(rho_l); add(Tt_h); add(Tt_l); add(Exh_h); add(Exh_l); add(Eyh_h); add(Eyh_l);
+  add(Ut_h); add(Ut_l); add(Vt_h); add(Vt_l); add(B1t_h); add(B1t_l); add(L2_h); add(L2_l);
+  add(B3t_h); add(B3t_l); add(B5t_h); add(B5t_l); add(L4_h); add(L4_l); add(L6_h); add(L6_l);
+  add(B3gt_h); add(B3gt_l); add(L6g_h); add(L6g_l); add(lg_order); add(lg_msize); add(lg_free0);
+  for (const auto &l : lslots) {
+    add(l->pos); add(l->sites); add(l->loc); add(l->cost); add(l->work); add(l->out);
+  }
+  return b;
+}
+
+extern "C" {
+
+eplace_status eplace_run(eplace_ctx *c, const eplace_cfg *cfg, const eplace_opts *opts_in,
+                         eplace_result *res) {
+  if (!c || !cfg || !res) return EPLACE_ERR_INVALID;
+  eplace_opts opts;
+  eplace_opts_default(&opts);
+  if (opts_in) opts = *opts_in;
+  JobState j(c, *cfg, opts, res, nullptr);
+  eplace_status st = job_start(&j);
+  if (st != EPLACE_OK) return st;
+  while (!j.done()) j.pump(true);
+  return j.finish();
 }
 
 eplace_status eplace_place(const eplace_netlist *nl, const eplace_chip *chip, const eplace_cfg *cfg,
@@ -1203,9 +1671,19 @@ eplace_status eplace_place(const eplace_netlist *nl, const eplace_chip *chip, co
   eplace_ctx *c = nullptr;
   eplace_status st = eplace_ctx_create(nl, chip, device, &c);
   if (st != EPLACE_OK) return st;
+  const auto t1 = std::chrono::steady_clock::now();
   st = eplace_run(c, cfg, opts, res);
   if (st != EPLACE_OK) g_thread_error = c->err;
+  const auto t2 = std::chrono::steady_clock::now();
   eplace_ctx_destroy(c);
+  if (opts && opts->verbose >= 2) {
+    const auto t3 = std::chrono::steady_clock::now();
+    auto ms = [](std::chrono::steady_clock::time_point a, std::chrono::steady_clock::time_point b) {
+      return std::chrono::duration<double>(b - a).count() * 1e3;
+    };
+    std::fprintf(stderr, "eplace_place: create %.2f ms, run %.2f ms, destroy %.2f ms\n", ms(t0, t1), ms(t1, t2),
+                 ms(t2, t3));
+  }
   if (res) {
     res->h2d_bytes = g_h2d - h2d0;
     res->d2h_bytes = g_d2h - d2h0;
@@ -1528,6 +2006,49 @@ eplace_status eplace_legalize(eplace_ctx *c, const float *x, const float *y, int
   eplace_status st = L.run(x, y, sx, sy, disp);
   if (st != EPLACE_OK) set_err(c, "logic");
   return st;
+}
+
+eplace_status eplace_stage_legalize(eplace_ctx *c, const float *x, const float *y, int32_t *sx, int32_t *sy,
+                                    double *disp, int64_t *hpwl) {
+  if (!c || (c->hp.N && (!x || !y || !sx || !sy))) return EPLACE_ERR_INVALID;
+  const HostProblem &hp = c->hp;
+  if (!legalize_supported(hp.W, hp.H)) {
+    set_err(c, "the device legaliser supports chips up to 4096 sites wide");
+    return EPLACE_ERR_INVALID;
+  }
+  try {
+    CK(cudaSetDevice(c->device));
+    if (hp.N == 0) {
+      if (disp) *disp = 0.0;
+      if (hpwl) *hpwl = hpwl_host(hp, nullptr, nullptr);
+      return EPLACE_OK;
+    }
+    setup_gpu_legal(c);
+    LegalSlot *L = c->lslots.empty() ? new_legal_slot(c) : c->lslots[0].get();
+    prepare_slot(c, *L);
+    std::vector<float2> p = pack2(x, y, hp.N);
+    CK(cudaMemcpyAsync(L->pos.p, p.data(), sizeof(float2) * hp.N, cudaMemcpyHostToDevice, L->stream));
+    g_h2d += sizeof(float2) * hp.N;
+    launch_gpu_legal(c, *L);
+    std::vector<int2> s(hp.N);
+    CK(cudaMemcpyAsync(s.data(), L->sites.p, sizeof(int2) * hp.N, cudaMemcpyDeviceToHost, L->stream));
+    g_d2h += sizeof(int2) * hp.N;
+    CK(cudaStreamSynchronize(L->stream));
+    const LegalOut &o = *L->hout.p;
+    if (o.status != 0) {
+      set_err(c, "logic");
+      return EPLACE_ERR_NO_BELS;
+    }
+    for (uint32_t i = 0; i < hp.N; ++i) {
+      sx[i] = s[i].x;
+      sy[i] = s[i].y;
+    }
+    if (disp) *disp = o.disp;
+    if (hpwl) *hpwl = (int64_t)o.hpwl;
+  } catch (const CudaError &e) {
+    return cuda_fail(c, e);
+  }
+  return EPLACE_OK;
 }
 
 eplace_status eplace_legalize_host(const eplace_netlist *nl, const eplace_chip *chip, const float *x, const float *y,

@@ -2,8 +2,13 @@
 // of libeplace.so.  Nothing here crosses the C ABI.
 #pragma once
 
+#include <condition_variable>
 #include <cstdint>
+#include <deque>
+#include <functional>
+#include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/eplace.h"
@@ -74,5 +79,63 @@ int64_t hpwl_host(const HostProblem &hp, const int32_t *site_x, const int32_t *s
 eplace_status synth(const eplace_synth_spec &spec, eplace_synth_info *info, uint8_t *cw,
                     uint8_t *ch, int32_t *fx, int32_t *fy, uint32_t *net_off,
                     uint32_t *pin_cell);
+
+// FIFO worker pool of the host legaliser; one pool may serve many placement
+// jobs (the job engine shares one across its contexts).
+class Pool {
+ public:
+  explicit Pool(int n) {
+    for (int i = 0; i < n; ++i) th_.emplace_back([this, i] { loop(i); });
+  }
+  ~Pool() {
+    {
+      std::lock_guard<std::mutex> g(m_);
+      stop_ = true;
+    }
+    cv_.notify_all();
+    for (auto &t : th_) t.join();
+  }
+  void submit(std::function<void(int)> f) {
+    {
+      std::lock_guard<std::mutex> g(m_);
+      q_.push_back(std::move(f));
+    }
+    cv_.notify_one();
+  }
+  int size() const { return (int)th_.size(); }
+  // Blocks until the queue is empty and no job is running.
+  void wait_idle() {
+    std::unique_lock<std::mutex> g(m_);
+    idle_cv_.wait(g, [this] { return q_.empty() && active_ == 0; });
+  }
+
+ private:
+  void loop(int id) {
+    for (;;) {
+      std::function<void(int)> f;
+      {
+        std::unique_lock<std::mutex> g(m_);
+        cv_.wait(g, [this] { return stop_ || !q_.empty(); });
+        if (stop_ && q_.empty()) return;
+        f = std::move(q_.front());
+        q_.pop_front();
+        ++active_;
+      }
+      f(id);
+      {
+        std::lock_guard<std::mutex> g(m_);
+        --active_;
+      }
+      idle_cv_.notify_all();
+    }
+  }
+  std::vector<std::thread> th_;
+  std::deque<std::function<void(int)>> q_;
+  std::mutex m_;
+  std::condition_variable cv_, idle_cv_;
+  int active_ = 0;
+  bool stop_ = false;
+};
+
 
 }  // namespace eplace

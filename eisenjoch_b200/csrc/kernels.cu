@@ -560,35 +560,45 @@ __global__ void __launch_bounds__(kStepBlock) k_step(const StepArgs a) {
     for (uint32_t i = tid0; i < a.N; i += gstride) a.tmp_den[i] = gather_cell(a, i, a.look[i]);
     return;
   }
-  // Phase A: gather, read + clear the WA accumulator, combine.
+  // Modes: 0 = whole step in one cooperative launch (grid barriers between
+  // phases); 2, 3, 4 = phase A, the penalty-initialisation pass and phase C
+  // as three ordinary launches of the same grid (kernel boundaries replace
+  // the barriers, so no block ever waits for another).
+  const bool coop = a.mode == 0;
   double v[4] = {0.0, 0.0, 0.0, 0.0};
-  for (uint32_t i = tid0; i < a.N; i += gstride) {
-    const float2 p = a.look[i];
-    const float2 gd = gather_cell(a, i, p);
-    const float2 gw = make_float2((float)from_fix(a.acc[2 * i]), (float)from_fix(a.acc[2 * i + 1]));
-    a.acc[2 * i] = 0ull;
-    a.acc[2 * i + 1] = 0ull;
-    if (was_init) {
-      const float2 g = combine(a, i, gw, gd, lam);
-      a.g[i] = g;
-      const float2 x = a.x[i], xp = a.xp[i], gp = a.gprev[i];
-      const double dx = (double)x.x - xp.x, dy = (double)x.y - xp.y;
-      v[0] += dx * dx;
-      v[1] += dx * ((double)g.x - gp.x);
-      v[2] += dy * dy;
-      v[3] += dy * ((double)g.y - gp.y);
-    } else {
-      a.tmp_wl[i] = gw;
-      a.tmp_den[i] = gd;
-      v[0] += (double)gw.x * gw.x + (double)gw.y * gw.y;
-      v[1] += (double)gd.x * gd.x + (double)gd.y * gd.y;
+  if (a.mode == 0 || a.mode == 2) {
+    // Phase A: gather, read + clear the WA accumulator, combine.
+    for (uint32_t i = tid0; i < a.N; i += gstride) {
+      const float2 p = a.look[i];
+      const float2 gd = gather_cell(a, i, p);
+      const float2 gw = make_float2((float)from_fix(a.acc[2 * i]), (float)from_fix(a.acc[2 * i + 1]));
+      a.acc[2 * i] = 0ull;
+      a.acc[2 * i + 1] = 0ull;
+      if (was_init) {
+        const float2 g = combine(a, i, gw, gd, lam);
+        a.g[i] = g;
+        const float2 x = a.x[i], xp = a.xp[i], gp = a.gprev[i];
+        const double dx = (double)x.x - xp.x, dy = (double)x.y - xp.y;
+        v[0] += dx * dx;
+        v[1] += dx * ((double)g.x - gp.x);
+        v[2] += dy * dy;
+        v[3] += dy * ((double)g.y - gp.y);
+      } else {
+        a.tmp_wl[i] = gw;
+        a.tmp_den[i] = gd;
+        v[0] += (double)gw.x * gw.x + (double)gw.y * gw.y;
+        v[1] += (double)gd.x * gd.x + (double)gd.y * gd.y;
+      }
     }
+    block_sum<4>(v, sm);
+    if (threadIdx.x == 0)
+      for (int k = 0; k < 4; ++k) a.part[4 * blockIdx.x + k] = v[k];
+    if (a.mode == 2) return;
+    grid_barrier(a.bar, a.sc);
   }
-  block_sum<4>(v, sm);
-  if (threadIdx.x == 0)
-    for (int k = 0; k < 4; ++k) a.part[4 * blockIdx.x + k] = v[k];
-  grid_barrier(a.bar, a.sc);
 
+  // Pass-2 partials: part[] again after a barrier (cooperative), else part_b[].
+  double *part2nd = coop ? a.part : a.part_b;
   if (!was_init) {
     // First penalty: 0.1 * |g_wl| / |g_den| when |g_den| > 1e-30 (mod.rs:132-138).
     double nr[2];
@@ -599,29 +609,34 @@ __global__ void __launch_bounds__(kStepBlock) k_step(const StepArgs a) {
       lam = 0.1 * wl / dn;
       lam_init = true;
     }
-    grid_barrier(a.bar, a.sc);  // everyone has read part[] before it is reused
-    for (int k = 0; k < 4; ++k) v[k] = 0.0;
-    for (uint32_t i = tid0; i < a.N; i += gstride) {
-      const float2 g = combine(a, i, a.tmp_wl[i], a.tmp_den[i], lam);
-      a.g[i] = g;
-      const float2 x = a.x[i], xp = a.xp[i], gp = a.gprev[i];
-      const double dx = (double)x.x - xp.x, dy = (double)x.y - xp.y;
-      v[0] += dx * dx;
-      v[1] += dx * ((double)g.x - gp.x);
-      v[2] += dy * dy;
-      v[3] += dy * ((double)g.y - gp.y);
+    if (a.mode == 0 || a.mode == 3) {
+      if (coop) grid_barrier(a.bar, a.sc);  // everyone has read part[] before it is reused
+      for (int k = 0; k < 4; ++k) v[k] = 0.0;
+      for (uint32_t i = tid0; i < a.N; i += gstride) {
+        const float2 g = combine(a, i, a.tmp_wl[i], a.tmp_den[i], lam);
+        a.g[i] = g;
+        const float2 x = a.x[i], xp = a.xp[i], gp = a.gprev[i];
+        const double dx = (double)x.x - xp.x, dy = (double)x.y - xp.y;
+        v[0] += dx * dx;
+        v[1] += dx * ((double)g.x - gp.x);
+        v[2] += dy * dy;
+        v[3] += dy * ((double)g.y - gp.y);
+      }
+      block_sum<4>(v, sm);
+      if (threadIdx.x == 0)
+        for (int k = 0; k < 4; ++k) part2nd[4 * blockIdx.x + k] = v[k];
+      if (a.mode == 3) return;
+      grid_barrier(a.bar, a.sc);
     }
-    block_sum<4>(v, sm);
-    if (threadIdx.x == 0)
-      for (int k = 0; k < 4; ++k) a.part[4 * blockIdx.x + k] = v[k];
-    grid_barrier(a.bar, a.sc);
+  } else if (a.mode == 3) {
+    return;
   }
 
   // Barzilai-Borwein per axis after the first iteration (mod.rs:158-166,
   // nesterov.rs:199-218): |dx.dx / dx.dg| clamped to [1e-4, 1], kept when
   // |dx.dg| < 1e-30.
   double t[4];
-  sum_partials<4>(a.part, 4, gridDim.x, t, sm);
+  sum_partials<4>(was_init ? a.part : part2nd, 4, gridDim.x, t, sm);
   double alpha[2] = {a.sc->step[0], a.sc->step[1]};
   if (it > 0) {
     for (int ax = 0; ax < 2; ++ax) {
@@ -746,6 +761,16 @@ int step_max_grid(int device) {
 cudaError_t launch_step(const StepArgs &a, int grid, cudaStream_t s) {
   void *args[] = {const_cast<StepArgs *>(&a)};
   return cudaLaunchCooperativeKernel((const void *)k_step, dim3(grid), dim3(kStepBlock), args, 0, s);
+}
+cudaError_t launch_step_split(const StepArgs &a, int grid, cudaStream_t s) {
+  for (int mode = 2; mode <= 4; ++mode) {
+    StepArgs b = a;
+    b.mode = mode;
+    k_step<<<grid, kStepBlock, 0, s>>>(b);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 cudaError_t launch_hpwl(const HpwlArgs &a, int grid, cudaStream_t s) {

@@ -101,9 +101,11 @@ struct StepArgs {
   IterLog *log;
   double *part;             // [4 * grid]
   double *part2;            // [2 * grid] step-norm partials
+  double *part_b;           // [4 * grid] pass-2 partials of the split form
   unsigned *bar;            // grid barrier {count, generation}
   unsigned *ticket;
-  int mode;                 // 0: full step; 1: gather only (tmp_den <- density gradient)
+  int mode;                 // 0: full step (cooperative); 1: gather only (tmp_den <- density
+                            // gradient); 2/3/4: phase A / penalty-init pass / phase C
 };
 
 struct HpwlArgs {
@@ -124,6 +126,9 @@ cudaError_t launch_sgemm(const GemmOp *ops_dev, int nb, int M, int N, int K, cud
 cudaError_t launch_sgemm_spectral(const GemmOp *ops_dev, int M, int N, int K,
                                   const SpectralArgs &sp, cudaStream_t s);
 cudaError_t launch_step(const StepArgs &a, int grid, cudaStream_t s);
+// The same step as three ordinary launches (modes 2, 3, 4): no grid barrier,
+// safe beside long-running kernels of other streams.
+cudaError_t launch_step_split(const StepArgs &a, int grid, cudaStream_t s);
 int step_max_grid(int device);
 cudaError_t launch_hpwl(const HpwlArgs &a, int grid, cudaStream_t s);
 

@@ -59,6 +59,7 @@ class RunOptions:
     verbose: int = 0
     max_inflight: int = 3
     field_mode: int = _abi.EPLACE_FIELD_REFERENCE
+    legal_mode: int = _abi.EPLACE_LEGAL_HOST
 
     def to_c(self):
         o = _abi.Opts()
@@ -69,6 +70,7 @@ class RunOptions:
         o.verbose = int(self.verbose)
         o.max_inflight = int(self.max_inflight)
         o.field_mode = int(self.field_mode)
+        o.legal_mode = int(self.legal_mode)
         return o
 
 
@@ -306,6 +308,41 @@ def workload(name):
     return nl, chip, ElectroPlaceCfg(**w["cfg"])
 
 
+def mixed_job_spec(seed, num_cells):
+    """One job of the mixed-size streams (same generator as the single
+    instances): nets = 1.1 x cells, 5% macros, clusters of 64 with locality
+    0.6, pads = cells / 100 (at least 40), bin grid = next power of two >=
+    sqrt(cells) clamped to [64, 512], two sites per bin edge."""
+    b = 64
+    while b * b < num_cells and b < 512:
+        b *= 2
+    return SynthSpec(seed=seed, num_cells=int(num_cells), num_nets=int(round(1.1 * num_cells)),
+                     num_pads=max(40, int(num_cells) // 100), width=2 * b, height=2 * b, bins_x=b, bins_y=b,
+                     cluster_size=64, macro_fraction=0.05)
+
+
+def mixed_job_specs(count, seed0, nmin, nmax, rng_seed):
+    """count jobs with cell counts log-uniform in [nmin, nmax] (numpy
+    default_rng(rng_seed)); job i has generator seed seed0 + i."""
+    rng = np.random.default_rng(rng_seed)
+    cells = np.exp(rng.uniform(np.log(nmin), np.log(nmax), count)).astype(np.int64)
+    return [mixed_job_spec(seed0 + i, int(n)) for i, n in enumerate(cells)]
+
+
+def batched_specs(count=64):
+    """Batched form: instances of 2k..200k cells, instance i seed 1000 + i."""
+    return mixed_job_specs(count, 1000, 2000, 200000, rng_seed=1000)
+
+
+def served_stream(count, rate):
+    """Served form: jobs of 1k..300k cells, job j seed 100000 + j, Poisson
+    arrivals (seed 7) at `rate` jobs/s.  Returns (specs, arrival times in s,
+    the first at 0)."""
+    specs = mixed_job_specs(count, 100000, 1000, 300000, rng_seed=100000)
+    gaps = np.random.default_rng(7).exponential(1.0 / rate, count)
+    return specs, np.cumsum(gaps) - gaps[0]
+
+
 # ---------------------------------------------------------------------------
 # Results
 # ---------------------------------------------------------------------------
@@ -398,6 +435,13 @@ class PlacementContext:
         h = ctypes.c_void_p()
         check(self._lib.eplace_ctx_create(ctypes.byref(self._nl_c), ctypes.byref(self._chip_c), device, ctypes.byref(h)))
         self.handle = h
+
+    def load(self, netlist: Netlist, chip: Chip):
+        """Re-targets this context at another netlist (eplace_ctx_load):
+        device buffers are kept and only grow."""
+        nl_c, chip_c = netlist.to_c(), chip.to_c()
+        self._check(self._lib.eplace_ctx_load(self.handle, ctypes.byref(nl_c), ctypes.byref(chip_c)))
+        self.netlist, self.chip, self._nl_c, self._chip_c = netlist, chip, nl_c, chip_c
 
     def close(self):
         if self.handle:
@@ -504,6 +548,19 @@ class PlacementContext:
                                               _abi.ptr(sy, ctypes.c_int32), ctypes.byref(d)))
         return sx, sy, d.value
 
+    def legalize_device(self, x, y):
+        """The same legalisation on the GPU plus the device HPWL of the
+        binding: (site_x, site_y, displacement, hpwl)."""
+        n = self.netlist.num_cells
+        x, y = _abi.f32(x), _abi.f32(y)
+        sx, sy = np.zeros(n, np.int32), np.zeros(n, np.int32)
+        d, h = ctypes.c_double(), ctypes.c_int64()
+        F = ctypes.c_float
+        self._check(self._lib.eplace_stage_legalize(self.handle, _abi.ptr(x, F), _abi.ptr(y, F),
+                                                    _abi.ptr(sx, ctypes.c_int32), _abi.ptr(sy, ctypes.c_int32),
+                                                    ctypes.byref(d), ctypes.byref(h)))
+        return sx, sy, d.value, int(h.value)
+
     STAGES = ("wa_grad", "density_scatter", "density_final", "dct_gemm1", "dct_gemm2_spectral",
               "dct_gemm3", "dct_gemm4", "gather_step")
 
@@ -563,6 +620,88 @@ def initial_placement_host(netlist: Netlist, chip: Chip, seed: int):
 # ---------------------------------------------------------------------------
 # Reference entry points
 # ---------------------------------------------------------------------------
+# ---------------------------------------------------------------------------
+# Job engine (eplace_server_*): many jobs on one GPU, continuously batched
+# ---------------------------------------------------------------------------
+@dataclass
+class JobInfo:
+    queued_seconds: float
+    run_seconds: float
+    latency_seconds: float
+    footprint_bytes: int
+
+
+class JobServer:
+    """Placement jobs admitted by device footprint and run concurrently on
+    one GPU (include/eplace.h, job engine).  submit() copies the inputs and
+    returns at once; wait() returns the PlacementResult, equal to
+    place_electro's on the same inputs."""
+
+    def __init__(self, device: int = 0, max_jobs: int = 16, hbm_budget: int = 0, legal_threads: int = 0,
+                 opts: Optional[RunOptions] = None):
+        self.handle = None
+        self._lib = _abi.lib()
+        c = _abi.ServerCfg()
+        self._lib.eplace_server_cfg_default(ctypes.byref(c))
+        c.device, c.max_jobs, c.hbm_budget, c.legal_threads = device, max_jobs, hbm_budget, legal_threads
+        c.opts = (opts or RunOptions()).to_c()
+        h = ctypes.c_void_p()
+        check(self._lib.eplace_server_create(ctypes.byref(c), ctypes.byref(h)))
+        self.handle = h
+        self._meta = {}
+
+    def submit(self, netlist: Netlist, chip: Chip, cfg: Optional[ElectroPlaceCfg] = None) -> int:
+        cfg = cfg or ElectroPlaceCfg()
+        nl_c, chip_c, cc = netlist.to_c(), chip.to_c(), cfg.to_c()
+        jid = ctypes.c_uint64()
+        check(self._lib.eplace_server_submit(self.handle, ctypes.byref(nl_c), ctypes.byref(chip_c), ctypes.byref(cc),
+                                             ctypes.byref(jid)))
+        self._meta[jid.value] = (netlist.num_cells, chip.width, _traj_cap(cfg))
+        return jid.value
+
+    def wait(self, job_id: int, timeout_ms: int = -1):
+        """(PlacementResult, JobInfo), or None while the job is still running
+        (timeout_ms >= 0).  Raises the job's PlacerError / EplaceError."""
+        n, width, cap = self._meta[job_id]
+        buf = _ResultBuffers(n, width, cap)
+        info = _abi.JobInfo()
+        st = self._lib.eplace_server_wait(self.handle, job_id, timeout_ms, ctypes.byref(buf.c), ctypes.byref(info))
+        if st == _abi.EPLACE_PENDING:
+            return None
+        del self._meta[job_id]
+        check(st)
+        return buf.result(), JobInfo(info.queued_seconds, info.run_seconds, info.latency_seconds,
+                                     int(info.footprint_bytes))
+
+    def stats(self):
+        s = _abi.ServerStats()
+        check(self._lib.eplace_server_stats_get(self.handle, ctypes.byref(s)))
+        return {k: int(getattr(s, k)) for k, _ in _abi.ServerStats._fields_}
+
+    def close(self):
+        if self.handle:
+            self._lib.eplace_server_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def footprint(netlist: Netlist, chip: Chip) -> int:
+    """Admission estimate of a job's device bytes (eplace_footprint)."""
+    nl_c, chip_c = netlist.to_c(), chip.to_c()
+    return int(_abi.lib().eplace_footprint(ctypes.byref(nl_c), ctypes.byref(chip_c)))
+
+
 def place_electro(netlist: Netlist, chip: Chip, cfg: Optional[ElectroPlaceCfg] = None,
                   opts: Optional[RunOptions] = None, device: int = 0) -> PlacementResult:
     """place_electro (electro_place/mod.rs:65-204) through the C ABI's

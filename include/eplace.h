@@ -40,7 +40,8 @@ typedef enum {
   EPLACE_ERR_OOM = 5,               /* device/host allocation or admission refused */
   EPLACE_ERR_CUDA = 6,              /* CUDA runtime error (message has details) */
   EPLACE_ERR_TIMEOUT = 7,           /* a bounded device wait gave up */
-  EPLACE_ERR_NO_DEVICE = 8          /* no usable sm_100 device */
+  EPLACE_ERR_NO_DEVICE = 8,         /* no usable sm_100 device */
+  EPLACE_PENDING = 9                /* job engine: the job has not finished yet */
 } eplace_status;
 
 /* ElectroPlaceCfg (crates/nextpnr/src/placer/electro_place/config.rs:5-40):
@@ -82,6 +83,18 @@ typedef enum {
   EPLACE_FIELD_POTENTIAL_GRADIENT = 1
 } eplace_field_mode;
 
+/* Where the periodic legalisations run.  Both give the same bindings, the
+ * same displacement and the same HPWL (the reference's greedy choice and
+ * tie-break, electro_place/mod.rs:206-255).  EPLACE_LEGAL_HOST: host
+ * threads, snapshots copied to pinned memory.  EPLACE_LEGAL_GPU: one warp
+ * per checkpoint on the device, concurrent with the Nesterov loop, HPWL on
+ * the device; only the best checkpoint's binding is copied back.  Chips
+ * wider than 4096 sites fall back to EPLACE_LEGAL_HOST. */
+typedef enum {
+  EPLACE_LEGAL_HOST = 0,
+  EPLACE_LEGAL_GPU = 1
+} eplace_legal_mode;
+
 typedef struct {
   int32_t dct_mode;            /* eplace_dct_mode; default EPLACE_DCT_FP32_SIMT */
   int32_t legal_threads;       /* host legaliser threads; 0 = hardware concurrency */
@@ -89,7 +102,8 @@ typedef struct {
   int32_t verbose;             /* 1 = print the reference's per-legalisation trajectory line */
   int32_t max_inflight;        /* intervals launched ahead of the host; default 3 */
   int32_t field_mode;          /* eplace_field_mode; default EPLACE_FIELD_REFERENCE */
-  int32_t reserved[2];
+  int32_t legal_mode;          /* eplace_legal_mode; default EPLACE_LEGAL_HOST */
+  int32_t reserved[1];
 } eplace_opts;
 
 void eplace_opts_default(eplace_opts *opts);
@@ -160,6 +174,13 @@ typedef struct eplace_ctx eplace_ctx;
 eplace_status eplace_ctx_create(const eplace_netlist *nl, const eplace_chip *chip,
                                 int32_t device, eplace_ctx **out);
 void eplace_ctx_destroy(eplace_ctx *ctx);
+
+/* Re-targets an existing context at another netlist / chip (the next job),
+ * keeping its device buffers: they only grow, nothing is freed, and the DCT
+ * matrices are rebuilt only when the bin grid changes.  Equivalent to
+ * destroy + create, without the allocations.  No reference counterpart
+ * (the reference rebuilds its Context per design). */
+eplace_status eplace_ctx_load(eplace_ctx *ctx, const eplace_netlist *nl, const eplace_chip *chip);
 
 /* place_electro (electro_place/mod.rs:65-204) on the uploaded netlist.
  * opts may be NULL (defaults). */
@@ -235,9 +256,19 @@ eplace_status eplace_profile_stages(eplace_ctx *ctx, const eplace_cfg *cfg, cons
                                     uint32_t reps, double *stage_ms);
 
 /* Greedy legalisation of continuous positions (electro_place/mod.rs:206-255),
- * host ring search with the reference's tie-break. */
+ * host row search with the reference's tie-break. */
 eplace_status eplace_legalize(eplace_ctx *ctx, const float *x, const float *y,
                               int32_t *site_x, int32_t *site_y, double *displacement);
+
+/* The same legalisation on the GPU (one warp, free-site bitmap in shared
+ * memory; results identical to eplace_legalize), followed by the device
+ * HPWL of the binding.  Replaces legalize_electro (electro_place/mod.rs:
+ * 206-255) + total_hpwl (metrics/wirelength.rs:10-51).  Returns
+ * EPLACE_ERR_NO_BELS when a cell finds no free site; EPLACE_ERR_INVALID for
+ * chips wider than 4096 sites. */
+eplace_status eplace_stage_legalize(eplace_ctx *ctx, const float *x, const float *y,
+                                    int32_t *site_x, int32_t *site_y, double *displacement,
+                                    int64_t *hpwl);
 
 /* The same legaliser and the host HPWL without a context (no device needed):
  * host code of the path that callers may run on CPU-only machines. */
@@ -271,6 +302,61 @@ eplace_status eplace_density_noalloc(const float *pos_xy, const float *half_wh,
                                      uint32_t num_cells, int32_t width, int32_t height,
                                      int32_t bins_x, int32_t bins_y, double *density,
                                      double *overlap, void *stream);
+
+/* ---------------------------------------------------------------------- */
+/* Job engine: many placement jobs on one GPU, continuously batched.       */
+/* No reference counterpart (the reference places one design per call).   */
+/* Jobs are admitted while fewer than max_jobs run and their estimated     */
+/* device footprint fits hbm_budget (a job larger than the budget still    */
+/* runs, alone).  Admitted jobs run concurrently: each on a context of its */
+/* own (device buffers kept and reused across jobs), its intervals as CUDA */
+/* graphs on its own stream, the legalisations on one shared host pool.    */
+/* A job's result is the same as eplace_run's on the same input.           */
+/* One internal thread drives the device; the calls are thread-safe.       */
+/* ---------------------------------------------------------------------- */
+typedef struct eplace_server eplace_server;
+
+typedef struct {
+  int32_t device;
+  int32_t max_jobs;            /* jobs on the device at once; 0 = 16 */
+  uint64_t hbm_budget;         /* device bytes jobs may hold; 0 = half the free memory */
+  int32_t legal_threads;       /* shared host legaliser threads; 0 = hardware concurrency */
+  int32_t reserved;
+  eplace_opts opts;            /* run options of every job (a job whose bin grid the tensor-core
+                                  transform does not support runs the FP32 transform) */
+} eplace_server_cfg;
+
+typedef struct {
+  double queued_seconds;       /* submit -> admitted */
+  double run_seconds;          /* admitted -> finished */
+  double latency_seconds;      /* submit -> finished */
+  uint64_t footprint_bytes;    /* admission estimate */
+} eplace_job_info;
+
+typedef struct {
+  uint64_t submitted, finished, running, queued;
+  uint64_t contexts;           /* contexts created (each reused across jobs) */
+  uint64_t device_bytes;       /* device memory the contexts hold */
+} eplace_server_stats;
+
+void eplace_server_cfg_default(eplace_server_cfg *cfg);
+eplace_status eplace_server_create(const eplace_server_cfg *cfg, eplace_server **out);
+/* Finishes the running jobs, drops queued ones, frees everything.  Call it
+ * after the last eplace_server_wait has returned. */
+void eplace_server_destroy(eplace_server *srv);
+/* Copies and validates the job's inputs (the caller may free them on
+ * return) and queues it.  EPLACE_ERR_INVALID for a malformed netlist. */
+eplace_status eplace_server_submit(eplace_server *srv, const eplace_netlist *nl, const eplace_chip *chip,
+                                   const eplace_cfg *cfg, uint64_t *job_id);
+/* Waits up to timeout_ms (< 0: forever, 0: poll) for the job.  Finished:
+ * fills res (buffers as for eplace_run) and info (may be NULL), forgets the
+ * job and returns its status (the message via eplace_last_error(NULL, ..)).
+ * Not finished: EPLACE_PENDING. */
+eplace_status eplace_server_wait(eplace_server *srv, uint64_t job_id, int32_t timeout_ms, eplace_result *res,
+                                 eplace_job_info *info);
+eplace_status eplace_server_stats_get(eplace_server *srv, eplace_server_stats *out);
+/* The admission estimate of a job's device bytes (0 for an invalid netlist). */
+uint64_t eplace_footprint(const eplace_netlist *nl, const eplace_chip *chip);
 
 /* ---------------------------------------------------------------------- */
 /* Synthetic netlist generator (seeded, deterministic), no reference      */

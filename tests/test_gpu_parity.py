@@ -330,3 +330,28 @@ def test_place_cells_keeps_others():
     others = np.setdiff1d(np.arange(300), target)
     assert np.array_equal(tiles[others], first.bel_tile[others])
     assert len(np.unique(tiles)) == 300
+
+
+def test_ctx_load_equals_fresh_context():
+    """A context re-targeted at another netlist (eplace_ctx_load, buffers
+    kept) gives exactly the result of a fresh context, for a smaller and a
+    larger design and a different bin grid."""
+    specs = [E.SynthSpec(seed=21, num_cells=3000, num_nets=3300, num_pads=200, width=96, height=96),
+             E.SynthSpec(seed=22, num_cells=6000, num_nets=6600, num_pads=300, width=128, height=128,
+                         bins_x=64, bins_y=64, macro_fraction=0.03),
+             E.SynthSpec(seed=23, num_cells=1500, num_nets=1650, num_pads=100, width=64, height=64)]
+    cfg = E.ElectroPlaceCfg(max_iters=60)
+    opts = E.RunOptions(field_mode=1)
+    first = E.synth_netlist(specs[0])
+    ctx = E.PlacementContext(*first)
+    try:
+        for spec in specs:
+            nl, chip = E.synth_netlist(spec)
+            ctx.load(nl, chip)
+            a = ctx.run(cfg, opts)
+            b = E.place_electro(nl, chip, cfg, opts)
+            assert a.hpwl == b.hpwl and a.iters == b.iters and a.best_iter == b.best_iter
+            assert np.array_equal(a.bel_tile, b.bel_tile)
+            assert a.trajectory == b.trajectory
+    finally:
+        ctx.close()

@@ -155,3 +155,42 @@ def test_lock_others_flattening():
         return (int(n.fixed_x[f]), int(n.fixed_y[f]))
     for p in range(nl.num_pins):
         assert loc(nl, nl.pin_cell[p]) == loc(sub, sub.pin_cell[p])
+
+
+def test_footprint_estimate_grows_with_the_job():
+    """The engine's admission estimate (eplace_footprint) is host-only: it
+    validates the netlist and grows with cells, pins and bins."""
+    small = E.synth_netlist(E.SynthSpec(seed=3, num_cells=1000, num_nets=1100, num_pads=50, width=64, height=64))
+    big = E.synth_netlist(E.SynthSpec(seed=3, num_cells=8000, num_nets=8800, num_pads=200, width=128, height=128))
+    fs, fb = E.footprint(*small), E.footprint(*big)
+    assert 0 < fs < fb
+    nl, chip = small
+    assert fb - fs > 7000 * 96  # per-cell state at least
+    bad = E.Netlist(num_cells=2, net_offsets=np.array([0, 2], np.uint32), pin_cell=np.array([0, 9], np.uint32))
+    assert E.footprint(bad, chip) == 0
+
+
+def test_mixed_job_streams_are_seeded_and_feasible():
+    """The batched / served job generators: deterministic, cell counts in
+    range, bins a power of two in [64, 512], total footprint of every job
+    below 70% of its sites."""
+    a, b = E.batched_specs(64), E.batched_specs(64)
+    assert a == b and len(a) == 64
+    assert all(2000 <= s.num_cells <= 200000 for s in a)
+    assert all(s.bins_x in (64, 128, 256, 512) and s.width == 2 * s.bins_x for s in a)
+    specs, arr = E.served_stream(50, 40.0)
+    assert arr[0] == 0 and np.all(np.diff(arr) >= 0)
+    assert all(1000 <= s.num_cells <= 300000 for s in specs)
+    for sp in a[:8] + specs[:4]:
+        nl, chip = E.synth_netlist(sp)
+        area = (nl.cell_w.astype(int) * nl.cell_h.astype(int)).sum()
+        assert area < 0.7 * chip.width * chip.height
+
+
+def test_engine_without_gpu_reports_no_device():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(E.EplaceError) as ei:
+        E.JobServer()
+    assert ei.value.status == E._abi.EPLACE_ERR_NO_DEVICE
