@@ -58,6 +58,13 @@ def parse():
     ap.add_argument("--field-mode", default="potential_gradient", choices=["reference", "potential_gradient"],
                     help="reference: the reference's field formula (default, parity); potential_gradient: the "
                          "opt-in extension that spreads cells")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched (64 mixed-size jobs) arm")
+    ap.add_argument("--no-served", action="store_true", help="skip the served (Poisson stream) arm")
+    ap.add_argument("--batched-jobs", type=int, default=64)
+    ap.add_argument("--served-jobs", type=int, default=120,
+                    help="jobs of the served stream (a subsample of the 2,000-job stream, same distribution)")
+    ap.add_argument("--served-rate", type=float, default=60.0, help="offered rate of the served stream, jobs/s")
+    ap.add_argument("--max-jobs", type=int, default=16, help="jobs the engine keeps on the GPU at once")
     return ap.parse_args()
 
 
@@ -210,6 +217,136 @@ def ncu_traffic(kernel, workload):
             if kv.get("stage") == kernel and kv.get("workload") == workload:
                 return float(kv["dram_bytes_per_launch"])
     return None
+
+
+# ---------------------------------------------------------------------------
+# Batched and served forms: the job engine against the plain single-instance
+# form on the same jobs.
+# ---------------------------------------------------------------------------
+def _mixed_jobs(E, specs, rank):
+    return [E.synth_netlist(replica_spec(sp, rank)) for sp in specs]
+
+
+def _plain(E, jobs, cfg, opts, reuse, arrivals=None):
+    """One job at a time through the single-instance API: a fresh context
+    per job (reuse=False), or one context re-loaded per job (reuse=True).
+    With arrivals, a job starts at max(its arrival, the previous job's end).
+    Returns (seconds, results, latencies)."""
+    ctx = None
+    res, lat = [], []
+    t0 = time.perf_counter()
+    for k, (nl, chip) in enumerate(jobs):
+        if arrivals is not None:
+            wait = arrivals[k] - (time.perf_counter() - t0)
+            if wait > 0:
+                time.sleep(wait)
+        if reuse:
+            if ctx is None:
+                ctx = E.PlacementContext(nl, chip)
+            else:
+                ctx.load(nl, chip)
+            res.append(ctx.run(cfg, opts))
+        else:
+            with E.PlacementContext(nl, chip) as c:
+                res.append(c.run(cfg, opts))
+        if arrivals is not None:
+            lat.append(time.perf_counter() - t0 - arrivals[k])
+    dt = time.perf_counter() - t0
+    if ctx is not None:
+        ctx.close()
+    return dt, res, lat
+
+
+def _engine(E, srv, jobs, cfg, arrivals=None):
+    """All jobs through the engine (submitted at their arrival times when
+    given).  Returns (seconds from the first submit to the last result,
+    results, latencies)."""
+    t0 = time.perf_counter()
+    ids = []
+    for k, (nl, chip) in enumerate(jobs):
+        if arrivals is not None:
+            wait = arrivals[k] - (time.perf_counter() - t0)
+            if wait > 0:
+                time.sleep(wait)
+        ids.append(srv.submit(nl, chip, cfg))
+    out = [srv.wait(i) for i in ids]
+    dt = time.perf_counter() - t0
+    return dt, [r for r, _ in out], [info.latency_seconds for _, info in out]
+
+
+def _agree(a, b):
+    """Largest relative HPWL difference, jobs within 0.5%, converged counts."""
+    rel = [abs(x.hpwl - y.hpwl) / max(1, y.hpwl) for x, y in zip(a, b)]
+    return {"max_rel_hpwl_diff": max(rel), "within_0.5pct": int(sum(r <= 0.005 for r in rel)),
+            "converged": int(sum(x.converged for x in a)), "converged_plain": int(sum(y.converged for y in b)),
+            "max_overflow": max(x.overlap for x in a)}
+
+
+def batched_arm(args, dist, E, cfg):
+    """64 instances, 2k..200k cells (log-uniform), mixed precision (BF16x3
+    tensor-core transform where the bin grid allows it) through the engine,
+    against the plain FP32 form one job at a time on the same jobs."""
+    jobs = _mixed_jobs(E, E.batched_specs(args.batched_jobs), dist.rank)
+    eng_opts = E.RunOptions(field_mode=1, dct_mode=1)
+    plain_opts = E.RunOptions(field_mode=1, dct_mode=0)
+    with E.JobServer(device=dist.local, max_jobs=args.max_jobs, opts=eng_opts) as srv:
+        _engine(E, srv, jobs[: args.max_jobs], cfg)  # warm-up: creates the contexts
+        dist.barrier()
+        t_eng, r_eng, _ = _engine(E, srv, jobs, cfg)
+        stats = srv.stats()
+    dist.barrier()
+    _plain(E, jobs[:2], cfg, plain_opts, reuse=True)  # warm-up
+    t_reuse, r_reuse, _ = _plain(E, jobs, cfg, plain_opts, reuse=True)
+    t_fresh, _, _ = _plain(E, jobs, cfg, plain_opts, reuse=False)
+    n = dist.sum(len(jobs))
+    t_eng, t_reuse, t_fresh = dist.max(t_eng), dist.max(t_reuse), dist.max(t_fresh)
+    cells = [nl.num_cells for nl, _ in jobs]
+    return {
+        "workload": "batched_%d_jobs_2k_200k" % len(jobs), "jobs": n,
+        "cells_total": int(sum(cells)), "cells_min": int(min(cells)), "cells_max": int(max(cells)),
+        "engine": {"jobs_per_s": n / t_eng, "seconds": t_eng, "max_jobs": args.max_jobs,
+                   "dct": "bf16x3 tcgen05 (fp32 where bins < 128)", "contexts": stats["contexts"],
+                   "device_bytes": stats["device_bytes"]},
+        "plain_fp32_reused_ctx": {"jobs_per_s": n / t_reuse, "seconds": t_reuse},
+        "plain_fp32_fresh_ctx": {"jobs_per_s": n / t_fresh, "seconds": t_fresh},
+        "speedup_vs_plain_reused_ctx": t_reuse / t_eng,
+        "speedup_vs_plain_fresh_ctx": t_fresh / t_eng,
+        "results_vs_plain": _agree(r_eng, r_reuse),
+        "time_to_overflow_s_mean": float(np.mean([r.total_seconds for r in r_eng])),
+    }
+
+
+def served_arm(args, dist, E, cfg):
+    """A Poisson stream (fixed offered rate) of 1k..300k-cell jobs: the
+    engine (continuous batching) against the plain form, which serves the
+    same stream one job at a time in arrival order."""
+    specs, arrivals = E.served_stream(args.served_jobs, args.served_rate)
+    jobs = _mixed_jobs(E, specs, dist.rank)
+    eng_opts = E.RunOptions(field_mode=1, dct_mode=1)
+    plain_opts = E.RunOptions(field_mode=1, dct_mode=0)
+    with E.JobServer(device=dist.local, max_jobs=args.max_jobs, opts=eng_opts) as srv:
+        _engine(E, srv, jobs[: args.max_jobs], cfg)  # warm-up
+        dist.barrier()
+        t_eng, r_eng, lat_eng = _engine(E, srv, jobs, cfg, arrivals)
+    dist.barrier()
+    t_pl, r_pl, lat_pl = _plain(E, jobs, cfg, plain_opts, reuse=True, arrivals=arrivals)
+    n = dist.sum(len(jobs))
+    t_eng, t_pl = dist.max(t_eng), dist.max(t_pl)
+
+    def pct(v, q):
+        return float(np.percentile(v, q))
+
+    return {
+        "workload": "served_poisson_%d_jobs_1k_300k" % len(jobs), "jobs": n,
+        "offered_rate_jobs_per_s": args.served_rate * dist.world,
+        "sample": "first %d jobs of the 2,000-job stream (seeds 100000+j, arrivals seed 7)" % len(jobs),
+        "engine": {"jobs_per_s": n / t_eng, "p50_latency_s": pct(lat_eng, 50), "p99_latency_s": pct(lat_eng, 99),
+                   "max_jobs": args.max_jobs, "dct": "bf16x3 tcgen05 (fp32 where bins < 128)"},
+        "plain_fp32": {"jobs_per_s": n / t_pl, "p50_latency_s": pct(lat_pl, 50), "p99_latency_s": pct(lat_pl, 99)},
+        "throughput_vs_plain": t_pl / t_eng,
+        "p99_latency_vs_plain": pct(lat_pl, 99) / pct(lat_eng, 99),
+        "results_vs_plain": _agree(r_eng, r_pl),
+    }
 
 
 # ---------------------------------------------------------------------------
@@ -390,6 +527,10 @@ def ours(args, dist):
     e2e_value = jobs / e2e_s
     ctx.close()
 
+    mixed_cfg = E.ElectroPlaceCfg(max_iters=500)
+    batched = None if args.no_batched else batched_arm(args, dist, E, mixed_cfg)
+    served = None if args.no_served else served_arm(args, dist, E, mixed_cfg)
+
     if dist.rank != 0:
         return
 
@@ -469,6 +610,8 @@ def ours(args, dist):
         "cpu_baseline": cpu,
         "gpu_launches": int(launches),
         "clocks": ck,
+        "batched": batched,
+        "served": served,
     }
     print(json.dumps(line), flush=True)
 

@@ -1572,6 +1572,45 @@ uint64_t problem_device_bytes(const HostProblem &hp) {
   return N * 96 + F * 16 + P * 8 + NN * 16 + nb * 64 + m * 48 + (1u << 20);
 }
 
+namespace {
+std::mutex g_kept_mu;
+std::vector<eplace_ctx *> *g_kept = nullptr;  // never freed: lives until the process exits
+constexpr size_t kMaxKept = 4;
+}  // namespace
+
+// A kept context of `device`, preferring one whose DCT matrices match the
+// bin grid; nullptr if none is kept.
+eplace_ctx *take_kept_context(int32_t device, int bx, int by) {
+  std::lock_guard<std::mutex> g(g_kept_mu);
+  if (!g_kept) return nullptr;
+  size_t pick = g_kept->size();
+  for (size_t k = 0; k < g_kept->size(); ++k) {
+    eplace_ctx *c = (*g_kept)[k];
+    if (c->device != device) continue;
+    if (pick == g_kept->size()) pick = k;
+    if (c->mat_bx == bx && c->mat_by == by) {
+      pick = k;
+      break;
+    }
+  }
+  if (pick == g_kept->size()) return nullptr;
+  eplace_ctx *c = (*g_kept)[pick];
+  g_kept->erase(g_kept->begin() + pick);
+  return c;
+}
+
+void keep_context(eplace_ctx *c) {
+  {
+    std::lock_guard<std::mutex> g(g_kept_mu);
+    if (!g_kept) g_kept = new std::vector<eplace_ctx *>();
+    if (g_kept->size() < kMaxKept) {
+      g_kept->push_back(c);
+      return;
+    }
+  }
+  eplace_ctx_destroy(c);
+}
+
 eplace_ctx *ctx_new(int32_t device, eplace_status *st) {
   *st = EPLACE_OK;
   std::unique_ptr<eplace_ctx> c(new eplace_ctx());
@@ -1668,21 +1707,40 @@ eplace_status eplace_place(const eplace_netlist *nl, const eplace_chip *chip, co
                            const eplace_opts *opts, int32_t device, eplace_result *res) {
   const uint64_t h2d0 = g_h2d, d2h0 = g_d2h;
   const auto t0 = std::chrono::steady_clock::now();
-  eplace_ctx *c = nullptr;
-  eplace_status st = eplace_ctx_create(nl, chip, device, &c);
-  if (st != EPLACE_OK) return st;
+  // The one-shot call keeps its context between calls (one per device and
+  // concurrent caller): the next call re-loads it with its own netlist
+  // (eplace_ctx_load semantics), so a stream of one-shot placements
+  // allocates, builds DCT matrices and frees only when a design outgrows
+  // the kept buffers or the bin grid changes.  Kept contexts live until the
+  // process exits.
+  std::string msg;
+  HostProblem hp;
+  eplace_status st = load_problem(nl, chip, hp, msg);
+  if (st != EPLACE_OK) {
+    set_err(nullptr, msg);
+    return st;
+  }
+  eplace_ctx *c = take_kept_context(device, hp.BX, hp.BY);
+  if (!c) {
+    c = ctx_new(device, &st);
+    if (!c) return st;
+  }
+  st = ctx_load_problem(c, std::move(hp));
+  if (st != EPLACE_OK) {
+    g_thread_error = c->err;
+    eplace_ctx_destroy(c);
+    return st;
+  }
   const auto t1 = std::chrono::steady_clock::now();
   st = eplace_run(c, cfg, opts, res);
   if (st != EPLACE_OK) g_thread_error = c->err;
   const auto t2 = std::chrono::steady_clock::now();
-  eplace_ctx_destroy(c);
+  keep_context(c);
   if (opts && opts->verbose >= 2) {
-    const auto t3 = std::chrono::steady_clock::now();
     auto ms = [](std::chrono::steady_clock::time_point a, std::chrono::steady_clock::time_point b) {
       return std::chrono::duration<double>(b - a).count() * 1e3;
     };
-    std::fprintf(stderr, "eplace_place: create %.2f ms, run %.2f ms, destroy %.2f ms\n", ms(t0, t1), ms(t1, t2),
-                 ms(t2, t3));
+    std::fprintf(stderr, "eplace_place: load %.2f ms, run %.2f ms\n", ms(t0, t1), ms(t1, t2));
   }
   if (res) {
     res->h2d_bytes = g_h2d - h2d0;

@@ -36,6 +36,10 @@ int ctx_bins_x(const eplace_ctx *c);
 int ctx_bins_y(const eplace_ctx *c);
 // An empty context on `device` (stream, scalars); nullptr + *st on failure.
 eplace_ctx *ctx_new(int32_t device, eplace_status *st);
+// The one-shot entry point's kept contexts: take one of `device` (matching
+// bin grid preferred), or give one back (destroyed beyond a small limit).
+eplace_ctx *take_kept_context(int32_t device, int bx, int by);
+void keep_context(eplace_ctx *c);
 // Loads a validated problem into a context (buffers reused, only grow).
 eplace_status ctx_load_problem(eplace_ctx *c, HostProblem &&hp);
 // Whether the tensor-core transform supports the problem's bin grid.

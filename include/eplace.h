@@ -187,7 +187,10 @@ eplace_status eplace_ctx_load(eplace_ctx *ctx, const eplace_netlist *nl, const e
 eplace_status eplace_run(eplace_ctx *ctx, const eplace_cfg *cfg, const eplace_opts *opts,
                          eplace_result *res);
 
-/* One-shot convenience: create, run, destroy (the host-buffer path). */
+/* One-shot convenience: load, run, return the result (the host-buffer
+ * path).  The call keeps its context for the next one-shot call on the same
+ * device (up to four are kept, until the process exits); the next call
+ * re-loads it (eplace_ctx_load), so repeated calls do not re-allocate. */
 eplace_status eplace_place(const eplace_netlist *nl, const eplace_chip *chip,
                            const eplace_cfg *cfg, const eplace_opts *opts,
                            int32_t device, eplace_result *res);

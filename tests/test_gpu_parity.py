@@ -349,7 +349,10 @@ def test_ctx_load_equals_fresh_context():
             nl, chip = E.synth_netlist(spec)
             ctx.load(nl, chip)
             a = ctx.run(cfg, opts)
-            b = E.place_electro(nl, chip, cfg, opts)
+            with E.PlacementContext(nl, chip) as fresh:
+                b = fresh.run(cfg, opts)
+            c = E.place_electro(nl, chip, cfg, opts)  # one-shot: a kept context, re-loaded
+            assert c.hpwl == b.hpwl and np.array_equal(c.bel_tile, b.bel_tile) and c.trajectory == b.trajectory
             assert a.hpwl == b.hpwl and a.iters == b.iters and a.best_iter == b.best_iter
             assert np.array_equal(a.bel_tile, b.bel_tile)
             assert a.trajectory == b.trajectory
