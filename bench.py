@@ -306,7 +306,8 @@ def batched_arm(args, dist, E, cfg):
         "cells_total": int(sum(cells)), "cells_min": int(min(cells)), "cells_max": int(max(cells)),
         "engine": {"jobs_per_s": n / t_eng, "seconds": t_eng, "max_jobs": args.max_jobs,
                    "dct": "bf16x3 tcgen05 (fp32 where bins < 128)", "contexts": stats["contexts"],
-                   "device_bytes": stats["device_bytes"]},
+                   "device_bytes": stats["device_bytes"],
+                   "scheduler_s": {k: round(stats[k + "_seconds"], 3) for k in ("admit", "pump", "idle")}},
         "plain_fp32_reused_ctx": {"jobs_per_s": n / t_reuse, "seconds": t_reuse},
         "plain_fp32_fresh_ctx": {"jobs_per_s": n / t_fresh, "seconds": t_fresh},
         "speedup_vs_plain_reused_ctx": t_reuse / t_eng,

@@ -186,6 +186,9 @@ class ServerStats(ctypes.Structure):
         ("queued", ctypes.c_uint64),
         ("contexts", ctypes.c_uint64),
         ("device_bytes", ctypes.c_uint64),
+        ("admit_seconds", ctypes.c_double),
+        ("pump_seconds", ctypes.c_double),
+        ("idle_seconds", ctypes.c_double),
     ]
 
 

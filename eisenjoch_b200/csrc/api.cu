@@ -22,6 +22,7 @@
 #include <cstring>
 #include <deque>
 #include <functional>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -296,13 +297,18 @@ std::vector<WaTask> build_wa_tasks(const std::vector<uint32_t> &off) {
   return t;
 }
 
-// DCT matrices as GEMM operands (rustdct conventions, density.rs:211-275).
-void build_matrices(eplace_ctx *c) {
-  const int W = c->hp.BX, H = c->hp.BY;
+// Host copies of the FP32 DCT matrices of one bin grid (rustdct conventions,
+// density.rs:211-275).  They depend on the bin grid only, so each is computed
+// once per process and kept; uploading a kept set costs only the copy.
+struct HostMats {
+  std::vector<float> B1, B3, B5, L2, L4, L6, B3g, L6g, wx, gx2, wy, gy2;
+};
+
+void compute_host_mats(int W, int H, HostMats &m) {
   const double pi = 3.14159265358979323846;
-  std::vector<float> B1((size_t)W * W), B3((size_t)W * W), B5((size_t)W * W);
-  std::vector<float> L2((size_t)H * H), L4((size_t)H * H), L6((size_t)H * H);
-  std::vector<float> B3g((size_t)W * W), L6g((size_t)H * H);
+  auto &B1 = m.B1, &B3 = m.B3, &B5 = m.B5, &L2 = m.L2, &L4 = m.L4, &L6 = m.L6, &B3g = m.B3g, &L6g = m.L6g;
+  for (auto *v : {&B1, &B3, &B5, &B3g}) v->assign((size_t)W * W, 0.f);
+  for (auto *v : {&L2, &L4, &L6, &L6g}) v->assign((size_t)H * H, 0.f);
   // GEMM1  T = rho * B1,     B1[x][kx] = cos(pi kx (x + 1/2) / W)        (row DCT-II)
   // GEMM3a U = Ex^ * B3,     B3[kx][x] = sin(pi (kx+1)(x + 1/2) / W), kx = W-1 halved (row DST-III)
   // GEMM3b V = Ey^ * B5,     B5[kx][x] = cos(pi kx (x + 1/2) / W),    kx = 0 halved   (row DCT-III)
@@ -325,7 +331,11 @@ void build_matrices(eplace_ctx *c) {
       // potential-gradient field: L6g[y][ky] = -sin(pi ky (y + 1/2) / H)
       L6g[(size_t)a * H + b] = (float)(-std::sin(pi * b * (a + 0.5) / H));
     }
-  std::vector<float> wx(W), gx2(W), wy(H), gy2(H);
+  auto &wx = m.wx, &gx2 = m.gx2, &wy = m.wy, &gy2 = m.gy2;
+  wx.assign(W, 0.f);
+  gx2.assign(W, 0.f);
+  wy.assign(H, 0.f);
+  gy2.assign(H, 0.f);
   for (int k = 0; k < W; ++k) {
     double w = pi * k / W;
     wx[k] = (float)w;
@@ -336,6 +346,26 @@ void build_matrices(eplace_ctx *c) {
     wy[k] = (float)w;
     gy2[k] = (float)(2.0 * (1.0 - std::cos(w)));
   }
+}
+
+const HostMats &host_mats(int W, int H) {
+  static std::mutex mu;
+  static auto *cache = new std::map<std::pair<int, int>, std::unique_ptr<HostMats>>();  // kept for the process
+  std::lock_guard<std::mutex> g(mu);
+  auto &slot = (*cache)[{W, H}];
+  if (!slot) {
+    slot.reset(new HostMats());
+    compute_host_mats(W, H, *slot);
+  }
+  return *slot;
+}
+
+// DCT matrices as GEMM operands, uploaded from the kept host copies.
+void build_matrices(eplace_ctx *c) {
+  const int W = c->hp.BX, H = c->hp.BY;
+  const HostMats &hm = host_mats(W, H);
+  const auto &B1 = hm.B1, &B3 = hm.B3, &B5 = hm.B5, &L2 = hm.L2, &L4 = hm.L4, &L6 = hm.L6, &B3g = hm.B3g,
+             &L6g = hm.L6g, &wx = hm.wx, &gx2 = hm.gx2, &wy = hm.wy, &gy2 = hm.gy2;
   cudaStream_t s = c->stream;
   c->mB1.ensure(B1.size()); c->mB1.upload(B1.data(), B1.size(), s);
   c->mB3.ensure(B3.size()); c->mB3.upload(B3.data(), B3.size(), s);
@@ -429,28 +459,26 @@ CUtensorMap make_map(const __nv_bfloat16 *base, int rows, int k, int box_rows) {
   return m;
 }
 
-void upload_split(DBuf<__nv_bfloat16> &hi, DBuf<__nv_bfloat16> &lo, const std::vector<double> &v, cudaStream_t s) {
-  std::vector<__nv_bfloat16> h(v.size()), l(v.size());
+bool tc_supported(const HostProblem &hp) { return hp.BY % 128 == 0 && hp.BX % kTcBN == 0 && hp.BX % 64 == 0; }
+
+// Host copies of the tensor-core operands (BF16 hi/lo planes of the eight
+// transposed DCT matrices) of one bin grid, computed once per process.
+struct HostTcMats {
+  std::vector<__nv_bfloat16> hi[8], lo[8];  // B1t, B3t, B5t, B3gt, L2, L4, L6, L6g
+};
+
+void split_planes(const std::vector<double> &v, std::vector<__nv_bfloat16> &h, std::vector<__nv_bfloat16> &l) {
+  h.resize(v.size());
+  l.resize(v.size());
   for (size_t i = 0; i < v.size(); ++i) {
     const float f = (float)v[i];
     h[i] = __float2bfloat16_rn(f);
     l[i] = __float2bfloat16_rn(f - __bfloat162float(h[i]));
   }
-  hi.ensure(v.size());
-  lo.ensure(v.size());
-  hi.upload(h.data(), h.size(), s);
-  lo.upload(l.data(), l.size(), s);
 }
 
-bool tc_supported(const HostProblem &hp) { return hp.BY % 128 == 0 && hp.BX % kTcBN == 0 && hp.BX % 64 == 0; }
-
-// Builds the hi/lo DCT matrices, the operand buffers and the tensor maps of
-// the four GEMM launches (two field formulas for the inverse transforms).
-void setup_tc(eplace_ctx *c) {
-  if (c->tc_ready) return;
-  const int W = c->hp.BX, H = c->hp.BY;
+void compute_host_tc(int W, int H, HostTcMats &m) {
   const double pi = 3.14159265358979323846;
-  cudaStream_t s = c->stream;
   std::vector<double> B1t((size_t)W * W), B3t((size_t)W * W), B5t((size_t)W * W), B3gt((size_t)W * W);
   std::vector<double> L2((size_t)H * H), L4((size_t)H * H), L6((size_t)H * H), L6g((size_t)H * H);
   for (int a = 0; a < W; ++a)      // row a of B^T = output column a
@@ -467,14 +495,41 @@ void setup_tc(eplace_ctx *c) {
       L6[(size_t)a * H + b] = std::sin(pi * (b + 1) * (a + 0.5) / H) * (b == H - 1 ? 0.5 : 1.0);   // y=a, ky=b
       L6g[(size_t)a * H + b] = -std::sin(pi * b * (a + 0.5) / H);                                   // y=a, ky=b
     }
-  upload_split(c->B1t_h, c->B1t_l, B1t, s);
-  upload_split(c->B3t_h, c->B3t_l, B3t, s);
-  upload_split(c->B5t_h, c->B5t_l, B5t, s);
-  upload_split(c->B3gt_h, c->B3gt_l, B3gt, s);
-  upload_split(c->L2_h, c->L2_l, L2, s);
-  upload_split(c->L4_h, c->L4_l, L4, s);
-  upload_split(c->L6_h, c->L6_l, L6, s);
-  upload_split(c->L6g_h, c->L6g_l, L6g, s);
+  const std::vector<double> *src[8] = {&B1t, &B3t, &B5t, &B3gt, &L2, &L4, &L6, &L6g};
+  for (int k = 0; k < 8; ++k) split_planes(*src[k], m.hi[k], m.lo[k]);
+}
+
+const HostTcMats &host_tc(int W, int H) {
+  static std::mutex mu;
+  static auto *cache = new std::map<std::pair<int, int>, std::unique_ptr<HostTcMats>>();  // kept for the process
+  std::lock_guard<std::mutex> g(mu);
+  auto &slot = (*cache)[{W, H}];
+  if (!slot) {
+    slot.reset(new HostTcMats());
+    compute_host_tc(W, H, *slot);
+  }
+  return *slot;
+}
+
+void upload_planes(DBuf<__nv_bfloat16> &hi, DBuf<__nv_bfloat16> &lo, const std::vector<__nv_bfloat16> &h,
+                   const std::vector<__nv_bfloat16> &l, cudaStream_t s) {
+  hi.ensure(h.size());
+  lo.ensure(l.size());
+  hi.upload(h.data(), h.size(), s);
+  lo.upload(l.data(), l.size(), s);
+}
+
+// Uploads the kept hi/lo DCT matrices and builds the operand buffers and the
+// tensor maps of the four GEMM launches (two field formulas for the inverse
+// transforms).
+void setup_tc(eplace_ctx *c) {
+  if (c->tc_ready) return;
+  const int W = c->hp.BX, H = c->hp.BY;
+  cudaStream_t s = c->stream;
+  const HostTcMats &hm = host_tc(W, H);
+  DBuf<__nv_bfloat16> *dh[8] = {&c->B1t_h, &c->B3t_h, &c->B5t_h, &c->B3gt_h, &c->L2_h, &c->L4_h, &c->L6_h, &c->L6g_h};
+  DBuf<__nv_bfloat16> *dl[8] = {&c->B1t_l, &c->B3t_l, &c->B5t_l, &c->B3gt_l, &c->L2_l, &c->L4_l, &c->L6_l, &c->L6g_l};
+  for (int k = 0; k < 8; ++k) upload_planes(*dh[k], *dl[k], hm.hi[k], hm.lo[k], s);
   const size_t nb = (size_t)W * H;
   for (auto *b : {&c->rho_h, &c->rho_l, &c->Tt_h, &c->Tt_l, &c->Exh_h, &c->Exh_l, &c->Eyh_h, &c->Eyh_l, &c->Ut_h,
                   &c->Ut_l, &c->Vt_h, &c->Vt_l})

@@ -77,6 +77,7 @@ struct eplace_server {
   std::unordered_map<uint64_t, std::unique_ptr<JobRec>> jobs;
   uint64_t submitted = 0, finished = 0, running_n = 0, contexts = 0;
   uint64_t device_bytes = 0;  // held by all contexts, refreshed after each job
+  double t_admit = 0.0, t_pump = 0.0, t_idle = 0.0;  // scheduler time split (under m)
   // scheduler-thread state
   std::vector<Running> running;
   std::vector<eplace_ctx *> idle;
@@ -97,7 +98,9 @@ struct eplace_server {
           continue;
         }
       }
+      const auto a0 = Clock::now();
       admit();
+      const auto a1 = Clock::now();
       bool progressed = false;
       for (size_t k = 0; k < running.size();) {
         Running &r = running[k];
@@ -110,7 +113,13 @@ struct eplace_server {
           ++k;
         }
       }
+      const auto a2 = Clock::now();
       if (!progressed) std::this_thread::sleep_for(std::chrono::microseconds(20));
+      const auto a3 = Clock::now();
+      std::lock_guard<std::mutex> g(m);
+      t_admit += secs(a0, a1);
+      t_pump += secs(a1, a2);
+      t_idle += secs(a2, a3);
     }
   }
 
@@ -390,6 +399,9 @@ eplace_status eplace_server_stats_get(eplace_server *s, eplace_server_stats *out
   out->queued = s->queue.size();
   out->contexts = s->contexts;
   out->device_bytes = s->device_bytes;
+  out->admit_seconds = s->t_admit;
+  out->pump_seconds = s->t_pump;
+  out->idle_seconds = s->t_idle;
   return EPLACE_OK;
 }
 

@@ -676,7 +676,7 @@ class JobServer:
     def stats(self):
         s = _abi.ServerStats()
         check(self._lib.eplace_server_stats_get(self.handle, ctypes.byref(s)))
-        return {k: int(getattr(s, k)) for k, _ in _abi.ServerStats._fields_}
+        return {k: (float if t is ctypes.c_double else int)(getattr(s, k)) for k, t in _abi.ServerStats._fields_}
 
     def close(self):
         if self.handle:

@@ -340,6 +340,9 @@ typedef struct {
   uint64_t submitted, finished, running, queued;
   uint64_t contexts;           /* contexts created (each reused across jobs) */
   uint64_t device_bytes;       /* device memory the contexts hold */
+  double admit_seconds;        /* scheduler time spent admitting (load + start) */
+  double pump_seconds;         /* scheduler time spent advancing and completing jobs */
+  double idle_seconds;         /* scheduler time with nothing to do */
 } eplace_server_stats;
 
 void eplace_server_cfg_default(eplace_server_cfg *cfg);
