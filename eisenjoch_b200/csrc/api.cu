@@ -39,8 +39,9 @@ namespace eplace {
 namespace {
 
 thread_local std::string g_thread_error;
-// Host<->device bytes copied by the current call (reported in eplace_result).
-thread_local uint64_t g_h2d = 0, g_d2h = 0;
+// Host<->device bytes copied by the library (eplace_result reports each
+// call's share; calls running at the same time share the counters).
+std::atomic<uint64_t> g_h2d{0}, g_d2h{0};
 
 struct CudaError {
   cudaError_t e;

@@ -62,12 +62,23 @@ struct Running {
   JobState *job;
 };
 
+// A job a loader thread has loaded and started (or failed to).
+struct Ready {
+  JobRec *rec;
+  eplace_ctx *ctx;
+  JobState *job;  // nullptr when the load failed
+  eplace_status st;
+};
+
 }  // namespace
 
 struct eplace_server {
   eplace_server_cfg cfg{};
   uint64_t budget = 0;
-  std::unique_ptr<Pool> pool;
+  std::unique_ptr<Pool> pool;     // host legaliser, shared by all jobs
+  std::unique_ptr<Pool> loaders;  // admission work: context load + job start
+  std::vector<Ready> ready;       // loaded jobs waiting for the scheduler (under m)
+  int loading = 0;                // jobs handed to the loaders (scheduler thread)
   std::thread sched;
   std::mutex m;
   std::condition_variable cv_work, cv_done;
@@ -92,13 +103,14 @@ struct eplace_server {
     for (;;) {
       {
         std::unique_lock<std::mutex> g(m);
-        if (stop && running.empty()) break;
-        if (running.empty() && queue.empty()) {
+        if (stop && running.empty() && loading == 0) break;
+        if (running.empty() && queue.empty() && loading == 0) {
           cv_work.wait(g, [&] { return stop || !queue.empty(); });
           continue;
         }
       }
       const auto a0 = Clock::now();
+      take_ready();
       admit();
       const auto a1 = Clock::now();
       bool progressed = false;
@@ -152,9 +164,9 @@ struct eplace_server {
       JobRec *r = nullptr;
       {
         std::lock_guard<std::mutex> g(m);
-        if (stop || queue.empty() || (int)running.size() >= cfg.max_jobs) return;
+        if (stop || queue.empty() || (int)running.size() + loading >= cfg.max_jobs) return;
         JobRec *front = queue.front();
-        if (!running.empty() && used + front->footprint > budget) return;
+        if ((!running.empty() || loading > 0) && used + front->footprint > budget) return;
         queue.pop_front();
         r = front;
         ++running_n;
@@ -172,32 +184,61 @@ struct eplace_server {
         fail(r, st);
         continue;
       }
-      st = ctx_load_problem(c, std::move(r->hp));
-      if (st != EPLACE_OK) {
-        char buf[512];
-        eplace_last_error(c, buf, sizeof buf);
-        r->err = buf;
-        idle.push_back(c);
-        fail(r, st);
-        continue;
+      // The host work of admission (CSR copies, initial placement, uploads)
+      // runs on a loader thread while this thread keeps the others going.
+      ++loading;
+      const bool shared = cfg.max_jobs > 1;
+      Pool *lp = pool.get();
+      loaders->submit([this, r, c, jo, shared, lp](int) {
+        Ready rd{r, c, nullptr, EPLACE_OK};
+        rd.st = ctx_load_problem(c, std::move(r->hp));
+        if (rd.st != EPLACE_OK) {
+          char buf[512];
+          eplace_last_error(c, buf, sizeof buf);
+          r->err = buf;
+        } else {
+          ctx_set_shared(c, shared);
+          r->bel_tile.assign(r->n, 0);
+          r->bel_index.assign(r->n, 0);
+          r->x.assign(r->n, 0.f);
+          r->y.assign(r->n, 0.f);
+          r->traj.assign(r->cfg.max_iters / std::max<uint64_t>(1, r->cfg.legalize_interval) + 2,
+                         eplace_traj_entry{});
+          r->res = eplace_result{};
+          r->res.bel_tile = r->bel_tile.data();
+          r->res.bel_index = r->bel_index.data();
+          r->res.x = r->x.data();
+          r->res.y = r->y.data();
+          r->res.traj = r->traj.data();
+          r->res.traj_capacity = (uint32_t)r->traj.size();
+          rd.job = job_create(c, r->cfg, jo, &r->res, lp);
+          const eplace_status st2 = job_start(rd.job);
+          if (st2 != EPLACE_OK) r->st = st2;  // the job is done(); complete() records it
+        }
+        {
+          std::lock_guard<std::mutex> g(m);
+          ready.push_back(rd);
+        }
+        cv_work.notify_one();
+      });
+    }
+  }
+
+  // Moves the loaders' finished admissions into the running set.
+  void take_ready() {
+    std::vector<Ready> got;
+    {
+      std::lock_guard<std::mutex> g(m);
+      got.swap(ready);
+    }
+    for (const Ready &rd : got) {
+      --loading;
+      if (!rd.job) {
+        idle.push_back(rd.ctx);
+        fail(rd.rec, rd.st);
+      } else {
+        running.push_back({rd.rec, rd.ctx, rd.job});
       }
-      ctx_set_shared(c, cfg.max_jobs > 1);
-      r->bel_tile.assign(r->n, 0);
-      r->bel_index.assign(r->n, 0);
-      r->x.assign(r->n, 0.f);
-      r->y.assign(r->n, 0.f);
-      r->traj.assign(r->cfg.max_iters / std::max<uint64_t>(1, r->cfg.legalize_interval) + 2, eplace_traj_entry{});
-      r->res = eplace_result{};
-      r->res.bel_tile = r->bel_tile.data();
-      r->res.bel_index = r->bel_index.data();
-      r->res.x = r->x.data();
-      r->res.y = r->y.data();
-      r->res.traj = r->traj.data();
-      r->res.traj_capacity = (uint32_t)r->traj.size();
-      JobState *j = job_create(c, r->cfg, jo, &r->res, pool.get());
-      running.push_back({r, c, j});
-      st = job_start(j);
-      if (st != EPLACE_OK) r->st = st;  // the job is done(); complete() records it
     }
   }
 
@@ -283,6 +324,7 @@ eplace_status eplace_server_create(const eplace_server_cfg *cfg, eplace_server *
   }
   const int nt = s->cfg.legal_threads > 0 ? s->cfg.legal_threads : (int)std::max(1u, std::thread::hardware_concurrency());
   s->pool.reset(new Pool(std::min(nt, 64)));
+  s->loaders.reset(new Pool(4));
   eplace_server *raw = s.get();
   s->sched = std::thread([raw] { raw->loop(); });
   *out = s.release();
