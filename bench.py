@@ -61,9 +61,10 @@ def parse():
     ap.add_argument("--no-batched", action="store_true", help="skip the batched (64 mixed-size jobs) arm")
     ap.add_argument("--no-served", action="store_true", help="skip the served (Poisson stream) arm")
     ap.add_argument("--batched-jobs", type=int, default=64)
-    ap.add_argument("--served-jobs", type=int, default=120,
+    ap.add_argument("--served-jobs", type=int, default=200,
                     help="jobs of the served stream (a subsample of the 2,000-job stream, same distribution)")
-    ap.add_argument("--served-rate", type=float, default=60.0, help="offered rate of the served stream, jobs/s")
+    ap.add_argument("--served-rate", type=float, default=100.0,
+                    help="offered rate of the served stream, jobs/s (above the plain form's capacity)")
     ap.add_argument("--max-jobs", type=int, default=16, help="jobs the engine keeps on the GPU at once")
     return ap.parse_args()
 
