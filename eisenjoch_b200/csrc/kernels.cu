@@ -147,6 +147,62 @@ __device__ __forceinline__ float seg_sum(float v, int lane, int end, int head, i
   return __shfl_sync(kFull, v, head);
 }
 
+// A net of 33 .. 32*K pins on one warp with its pins held in registers
+// (lane l holds pins l, l + 32, ...): one gather of pin ids and positions
+// instead of one per pass.  Per-lane sums run in the same order as the
+// three-pass loop below, so the results are the same.
+template <int K>
+__device__ void wa_big_net_reg(const WaArgs &a, int pb, int pe, int lane) {
+  const float kg = a.gamma * kLog2e;
+  uint32_t cc[K];
+  float px[K], py[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const int q = pb + lane + 32 * k;
+    cc[k] = (q < pe) ? a.pin_cell[q] : 0xffffffffu;
+  }
+  float mx = -INFINITY, mn = INFINITY, my = -INFINITY, ny = INFINITY;
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const float2 p = (cc[k] != 0xffffffffu) ? a.pos[cc[k]] : make_float2(0.f, 0.f);
+    px[k] = p.x;
+    py[k] = p.y;
+    if (cc[k] != 0xffffffffu) {
+      mx = fmaxf(mx, p.x);
+      mn = fminf(mn, p.x);
+      my = fmaxf(my, p.y);
+      ny = fminf(ny, p.y);
+    }
+  }
+  mx = warp_allreduce(mx, OpMax());
+  mn = warp_allreduce(mn, OpMin());
+  my = warp_allreduce(my, OpMax());
+  ny = warp_allreduce(ny, OpMin());
+  float s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    if (cc[k] == 0xffffffffu) continue;
+    const float ux = px[k] - mx, vx = px[k] - mn, uy = py[k] - my, vy = py[k] - ny;
+    const float epx = ex2(kg * ux), emx = ex2(-kg * vx);
+    const float epy = ex2(kg * uy), emy = ex2(-kg * vy);
+    s[0] += epx; s[1] += ux * epx; s[2] += emx; s[3] += vx * emx;
+    s[4] += epy; s[5] += uy * epy; s[6] += emy; s[7] += vy * emy;
+  }
+#pragma unroll
+  for (int k = 0; k < 8; ++k) s[k] = warp_allreduce(s[k], OpAdd());
+  const float ipx = 1.0f / s[0], imx = 1.0f / s[2], ipy = 1.0f / s[4], imy = 1.0f / s[6];
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const uint32_t c = cc[k];
+    if (c >= a.N) continue;  // fixed cells and padding lanes
+    const float ux = px[k] - mx, vx = px[k] - mn, uy = py[k] - my, vy = py[k] - ny;
+    const float gx = wa_pin_grad(ux, vx, ex2(kg * ux), ex2(-kg * vx), ipx, s[1], imx, s[3], a.gamma);
+    const float gy = wa_pin_grad(uy, vy, ex2(kg * uy), ex2(-kg * vy), ipy, s[5], imy, s[7], a.gamma);
+    atomicAdd(&a.acc[2 * c], to_fix(gx));
+    atomicAdd(&a.acc[2 * c + 1], to_fix(gy));
+  }
+}
+
 __device__ void wa_big_net(const WaArgs &a, int pb, int pe, int lane) {
   const float kg = a.gamma * kLog2e;
   float mx = -INFINITY, mn = INFINITY, my = -INFINITY, ny = INFINITY;
@@ -197,7 +253,8 @@ __global__ void __launch_bounds__(kWaBlock) k_wa(const WaArgs a) {
     const WaTask tk = a.tasks[t];
     const int pb = tk.x, npin = tk.y - tk.x;
     if (npin > 32) {
-      wa_big_net(a, pb, tk.y, lane);
+      if (npin <= 32 * 7) wa_big_net_reg<7>(a, pb, tk.y, lane);
+      else wa_big_net(a, pb, tk.y, lane);
       continue;
     }
     // Segment heads: bit j set where a net starts at lane j.
