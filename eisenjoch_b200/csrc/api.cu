@@ -54,6 +54,41 @@ struct CudaError {
     if (e_ != cudaSuccess) throw CudaError{e_, std::string(#call)};        \
   } while (0)
 
+// Device allocations of a context are stream-ordered (cudaMallocFromPoolAsync
+// on the context's stream, from one memory pool per device that keeps what
+// it has mapped).  A plain cudaMalloc / cudaFree is a device-wide implicit
+// synchronisation point: while the job engine runs many contexts, one job's
+// (re)load would otherwise stall every other job's stream.  The stream comes
+// from the AllocOn guard of the calling thread; without one, plain
+// cudaMalloc (context creation).
+thread_local cudaStream_t t_alloc_stream = nullptr;
+struct AllocOn {
+  cudaStream_t prev;
+  explicit AllocOn(cudaStream_t s) : prev(t_alloc_stream) { t_alloc_stream = s; }
+  ~AllocOn() { t_alloc_stream = prev; }
+};
+
+cudaMemPool_t device_pool() {
+  static std::mutex mu;
+  static std::vector<cudaMemPool_t> pools;
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> g(mu);
+  if ((int)pools.size() <= dev) pools.resize(dev + 1, nullptr);
+  if (!pools[dev]) {
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t mp = nullptr;
+    CK(cudaMemPoolCreate(&mp, &props));
+    uint64_t keep = ~0ull;  // never trim: freed blocks serve the next loads
+    CK(cudaMemPoolSetAttribute(mp, cudaMemPoolAttrReleaseThreshold, &keep));
+    pools[dev] = mp;  // lives until the process exits
+  }
+  return pools[dev];
+}
+
 template <typename T>
 struct DBuf {
   T *p = nullptr;
@@ -63,11 +98,21 @@ struct DBuf {
   DBuf(const DBuf &) = delete;
   DBuf &operator=(const DBuf &) = delete;
   ~DBuf() { if (p) cudaFree(p); }
-  void alloc(size_t count) {
-    if (p) cudaFree(p);
+  void release() {
+    if (!p) return;
+    if (t_alloc_stream) cudaFreeAsync(p, t_alloc_stream);
+    else cudaFree(p);
     p = nullptr;
+  }
+  void alloc(size_t count) {
+    release();
     n = cap = 0;
-    if (count) CK(cudaMalloc(&p, sizeof(T) * count));
+    if (count) {
+      if (t_alloc_stream)
+        CK(cudaMallocFromPoolAsync((void **)&p, sizeof(T) * count, device_pool(), t_alloc_stream));
+      else
+        CK(cudaMalloc(&p, sizeof(T) * count));
+    }
     n = cap = count;
   }
   // Room for count elements; reallocates only when the capacity is short.
@@ -100,6 +145,75 @@ struct PinBuf {
     p = nullptr;
     n = count;
     if (count) CK(cudaMallocHost(&p, sizeof(T) * count));
+  }
+};
+
+// Pinned host blocks for checkpoint snapshots, from power-of-two size
+// classes carved out of 32 MiB chunks that are never returned: page-locked
+// allocation and release are device-wide implicit synchronisation points,
+// which the job engine must not hit while other jobs run.  Process-wide.
+class PinArena {
+ public:
+  static PinArena &get() {
+    static PinArena *a = new PinArena();  // never destroyed (pinned memory lives until exit)
+    return *a;
+  }
+  // A block of at least `bytes`; *cls receives its class for put().
+  void *take(size_t bytes, int *cls) {
+    int k = kMinClass;
+    while (((size_t)1 << k) < bytes) ++k;
+    *cls = k;
+    std::lock_guard<std::mutex> g(mu_);
+    if (k > kMaxClass) {  // beyond the chunk size: a block of its own
+      void *p = nullptr;
+      CK(cudaMallocHost(&p, (size_t)1 << k));
+      return p;
+    }
+    auto &fl = free_[k - kMinClass];
+    if (fl.empty()) {
+      char *chunk = nullptr;
+      CK(cudaMallocHost((void **)&chunk, kChunk));
+      for (size_t off = 0; off + ((size_t)1 << k) <= kChunk; off += (size_t)1 << k) fl.push_back(chunk + off);
+    }
+    void *p = fl.back();
+    fl.pop_back();
+    return p;
+  }
+  void put(void *p, int cls) {
+    if (!p) return;
+    std::lock_guard<std::mutex> g(mu_);
+    if (cls > kMaxClass) {
+      cudaFreeHost(p);
+      return;
+    }
+    free_[cls - kMinClass].push_back(p);
+  }
+
+ private:
+  static constexpr int kMinClass = 16, kMaxClass = 25;  // 64 KiB .. 32 MiB
+  static constexpr size_t kChunk = (size_t)1 << kMaxClass;
+  std::mutex mu_;
+  std::vector<void *> free_[kMaxClass - kMinClass + 1];
+};
+
+// A checkpoint's positions in pinned memory (the interval's device-to-host
+// copy lands here) and the host legaliser's binding of them.  Kept by the
+// context and reused across checkpoints and runs.
+struct HostSnap {
+  float2 *pos = nullptr;
+  size_t cap = 0;  // positions
+  int cls = 0;     // PinArena class of pos
+  std::vector<int32_t> sx, sy;
+  HostSnap() = default;
+  HostSnap(const HostSnap &) = delete;
+  HostSnap &operator=(const HostSnap &) = delete;
+  ~HostSnap() { PinArena::get().put(pos, cls); }
+  void reserve(size_t n) {
+    if (n <= cap && pos) return;
+    PinArena::get().put(pos, cls);
+    pos = nullptr;
+    pos = (float2 *)PinArena::get().take(sizeof(float2) * std::max<size_t>(n, 1), &cls);
+    cap = ((size_t)1 << cls) / sizeof(float2);
   }
 };
 
@@ -182,12 +296,14 @@ struct eplace_ctx {
   std::unique_ptr<LegalBase> lbase;
   std::vector<std::unique_ptr<Legalizer>> legal;
   std::unique_ptr<Pool> pool;
-  std::vector<std::unique_ptr<PinBuf<float2>>> snaps;
+  std::vector<std::unique_ptr<HostSnap>> hsnaps;  // all of them
+  std::vector<HostSnap *> hsnap_free;             // not held by a run
   std::vector<std::unique_ptr<PinBuf<IterLog>>> logs;
   std::vector<std::unique_ptr<PinBuf<DevScalars>>> scs;
   std::vector<cudaEvent_t> slot_ev;
   size_t slot_log_cap = 0;
   cudaGraphExec_t gexec = nullptr;
+  bool g_valid = false;  // gexec matches the current buffers and settings
   uint64_t g_epoch = 0, g_interval = 0;
   int g_field = -1;
   bool g_tc = false;
@@ -363,6 +479,7 @@ const HostMats &host_mats(int W, int H) {
 
 // DCT matrices as GEMM operands, uploaded from the kept host copies.
 void build_matrices(eplace_ctx *c) {
+  AllocOn on_stream(c->stream);
   const int W = c->hp.BX, H = c->hp.BY;
   const HostMats &hm = host_mats(W, H);
   const auto &B1 = hm.B1, &B3 = hm.B3, &B5 = hm.B5, &L2 = hm.L2, &L4 = hm.L4, &L6 = hm.L6, &B3g = hm.B3g,
@@ -401,6 +518,7 @@ void build_matrices(eplace_ctx *c) {
 }
 
 void ensure_log(eplace_ctx *c, size_t iters) {
+  AllocOn on_stream(c->stream);
   if (c->log_cap >= iters + 2) return;
   c->log_cap = std::max<size_t>(iters + 2, 1024);
   c->log.alloc(c->log_cap);
@@ -524,6 +642,7 @@ void upload_planes(DBuf<__nv_bfloat16> &hi, DBuf<__nv_bfloat16> &lo, const std::
 // tensor maps of the four GEMM launches (two field formulas for the inverse
 // transforms).
 void setup_tc(eplace_ctx *c) {
+  AllocOn on_stream(c->stream);
   if (c->tc_ready) return;
   const int W = c->hp.BX, H = c->hp.BY;
   cudaStream_t s = c->stream;
@@ -692,6 +811,7 @@ void launch_iteration(eplace_ctx *c, float gamma, int field_mode, bool tc) {
 constexpr int kLaunchesPerIter = 8;  // with the cooperative step; +2 with the split step
 
 void upload_momentum(eplace_ctx *c, uint64_t iters) {
+  AllocOn on_stream(c->stream);
   // FISTA sequence a_0 = 1, a_{k+1} = (1 + sqrt(1 + 4 a_k^2)) / 2; the
   // look-ahead and the step of iteration k both use m_k = (a_k - 1) / a_{k+1}
   // (nesterov.rs:41-64, :75-82; m_0 = 0).
@@ -712,6 +832,7 @@ void upload_momentum(eplace_ctx *c, uint64_t iters) {
 // Uploads what every device legalisation reads: the cell order (macros
 // first), the macros' footprints and the free map with the fixed cells.
 void setup_gpu_legal(eplace_ctx *c) {
+  AllocOn on_stream(c->stream);
   if (c->lg_ready) return;
   const HostProblem &hp = c->hp;
   if (!c->lbase) c->lbase.reset(new LegalBase(hp));
@@ -735,6 +856,7 @@ void setup_gpu_legal(eplace_ctx *c) {
 // Sizes slot L for the current problem (capacity reuse) and writes the
 // fixed cells' pin locations after a (re)load.
 void prepare_slot(eplace_ctx *c, LegalSlot &L) {
+  AllocOn on_stream(L.stream);  // synchronised below
   const HostProblem &hp = c->hp;
   if (L.gen == c->load_gen) return;
   const size_t N1 = std::max<size_t>(hp.N, 1);
@@ -758,6 +880,7 @@ LegalSlot *new_legal_slot(eplace_ctx *c) {
   int prio_lo = 0, prio_hi = 0;
   CK(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
   CK(cudaStreamCreateWithPriority(&L->stream, cudaStreamNonBlocking, prio_lo));
+  AllocOn on_stream(L->stream);  // prepare_slot synchronises it
   CK(cudaEventCreateWithFlags(&L->snap, cudaEventDisableTiming));
   CK(cudaEventCreate(&L->start));
   CK(cudaEventCreate(&L->done));
@@ -804,6 +927,7 @@ void launch_gpu_legal(eplace_ctx *c, LegalSlot &L) {
 // matrices and the tensor-core operands are rebuilt only when the bin grid
 // changes; every captured graph is invalidated.
 void load_into(eplace_ctx *c, HostProblem &&hp_in) {
+  AllocOn on_stream(c->stream);
   const bool same_bins = c->mat_bx == hp_in.BX && c->mat_by == hp_in.BY;
   c->hp = std::move(hp_in);
   const HostProblem &hp = c->hp;
@@ -814,8 +938,7 @@ void load_into(eplace_ctx *c, HostProblem &&hp_in) {
   c->lg_ready = false;
   ++c->load_gen;
   if (c->gexec) {
-    cudaGraphExecDestroy(c->gexec);
-    c->gexec = nullptr;
+    c->g_valid = false;  // updated in place by the next capture
   }
   ++c->buf_epoch;
   c->net_off.ensure(hp.net_off.size());
@@ -1022,8 +1145,7 @@ struct Checkpoint {
   int32_t iter = -1;
   size_t chunk = 0;
   // host legaliser: the snapshot and its binding
-  std::vector<float> xs, ys;
-  std::vector<int32_t> sx, sy;
+  HostSnap *hs = nullptr;
   // device legaliser: the slot holding positions and binding
   int slot = -1;
   bool discard = false;  // its interval ran past convergence
@@ -1063,6 +1185,7 @@ struct JobState {
   }
   ~JobState() {
     drain();
+    for (auto &cp : cps) release(cp.get());
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
   }
@@ -1157,20 +1280,16 @@ struct JobState {
         chunks.push_back({k, last});
         k = last + 1;
       }
-      // Pinned ring of interval outputs (log, scalars, and the positions when
-      // the host legalises).
+      // Pinned ring of interval outputs (log and scalars); the positions of
+      // a checkpoint the host legalises go to a HostSnap of their own.
       inflight = std::max(1, std::min(opts.max_inflight, 8));
-      if ((int)c->snaps.size() < inflight || c->slot_log_cap < interval + 1 ||
-          (!c->snaps.empty() && c->snaps[0]->n < hp.N)) {
-        c->snaps.clear();
+      if ((int)c->logs.size() < inflight || c->slot_log_cap < interval + 1) {
         c->logs.clear();
         c->scs.clear();
         for (auto e : c->slot_ev) cudaEventDestroy(e);
         c->slot_ev.clear();
         c->slot_log_cap = std::max<uint64_t>(interval + 1, 16);
         for (int i = 0; i < inflight; ++i) {
-          c->snaps.emplace_back(new PinBuf<float2>());
-          c->snaps.back()->alloc(hp.N);
           c->logs.emplace_back(new PinBuf<IterLog>());
           c->logs.back()->alloc(c->slot_log_cap);
           c->scs.emplace_back(new PinBuf<DevScalars>());
@@ -1180,15 +1299,23 @@ struct JobState {
           c->slot_ev.push_back(e);
         }
       }
+      if (!gpu_legal) {
+        // Snapshots for the intervals in flight and a few legalisations:
+        // pinned allocations here rather than while the loop runs.
+        std::vector<HostSnap *> pre;
+        for (int i = 0; i < inflight + 2; ++i) pre.push_back(take_snap());
+        for (HostSnap *h : pre) give_snap(h);
+      }
       for (int i = (int)c->lslots.size() - 1; i >= 0; --i) free_slots.push_back(i);
       // The interval graph is reused while nothing it bakes in has changed:
       // buffers (epoch), interval length, field formula, transform, wl_coeff.
+      // A new one is captured, instantiated and uploaded here, so that the
+      // thread pumping the loop only launches it.
       use_graph = opts.use_graphs != 0 && interval > 1;
       if (c->gexec && (c->g_epoch != c->buf_epoch || c->g_interval != interval || c->g_field != opts.field_mode ||
-                       c->g_tc != tc || c->g_gamma != gamma)) {
-        cudaGraphExecDestroy(c->gexec);
-        c->gexec = nullptr;
-      }
+                       c->g_tc != tc || c->g_gamma != gamma))
+        c->g_valid = false;
+      if (use_graph && interval < max_iters) ensure_graph();
       converged_chunk = chunks.size();
       CK(cudaEventRecord(ev0, s));
       phase = kLoop;
@@ -1211,49 +1338,98 @@ struct JobState {
     return k;
   }
 
+  // Captures the graph of one interval (`interval` iterations) unless the
+  // context holds a current one; on failure (capture not available, e.g.
+  // cooperative nodes) the run falls back to plain launches.
+  void ensure_graph() {
+    if (c->gexec && c->g_valid) return;
+    cudaStream_t s = c->stream;
+    cudaGraph_t graph = nullptr;
+    CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    bool ok = true;
+    try {
+      for (uint64_t k = 0; k < interval; ++k) launch_iteration(c, gamma, opts.field_mode, tc);
+    } catch (const CudaError &) {
+      ok = false;
+    }
+    cudaError_t ce = cudaStreamEndCapture(s, &graph);
+    ok = ok && ce == cudaSuccess;
+    // A stale executable graph of the same shape (same kernels, new
+    // pointers and sizes) is updated in place, which is cheaper than a new
+    // instantiation.
+    if (ok && c->gexec) {
+      cudaGraphExecUpdateResultInfo info{};
+      if (cudaGraphExecUpdate(c->gexec, graph, &info) != cudaSuccess) {
+        cudaGetLastError();
+        cudaGraphExecDestroy(c->gexec);
+        c->gexec = nullptr;
+      }
+    }
+    if (ok && !c->gexec && cudaGraphInstantiate(&c->gexec, graph, 0) != cudaSuccess) {
+      c->gexec = nullptr;
+      ok = false;
+    }
+    if (!ok) {
+      cudaGetLastError();
+      if (graph) cudaGraphDestroy(graph);
+      if (c->gexec) cudaGraphExecDestroy(c->gexec);
+      c->gexec = nullptr;
+      c->g_valid = false;
+      use_graph = false;
+      return;
+    }
+    cudaGraphDestroy(graph);
+    c->g_valid = true;
+    CK(cudaGraphUpload(c->gexec, s));
+    c->g_epoch = c->buf_epoch;
+    c->g_interval = interval;
+    c->g_field = opts.field_mode;
+    c->g_tc = tc;
+    c->g_gamma = gamma;
+  }
+
   void launch_chunk(const Chunk &ch) {
     cudaStream_t s = c->stream;
     const uint64_t n = ch.last - ch.first + 1;
     launched_iters += n;
+    if (use_graph && n == interval) ensure_graph();
     if (use_graph && n == interval) {
-      if (!c->gexec) {
-        cudaGraph_t graph = nullptr;
-        CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-        bool ok = true;
-        try {
-          for (uint64_t k = 0; k < n; ++k) launch_iteration(c, gamma, opts.field_mode, tc);
-        } catch (const CudaError &) {
-          ok = false;
-        }
-        cudaError_t ce = cudaStreamEndCapture(s, &graph);
-        if (!ok || ce != cudaSuccess || cudaGraphInstantiate(&c->gexec, graph, 0) != cudaSuccess) {
-          // Capture not available (e.g. cooperative nodes): plain launches.
-          cudaGetLastError();
-          if (graph) cudaGraphDestroy(graph);
-          c->gexec = nullptr;
-          use_graph = false;
-          for (uint64_t k = 0; k < n; ++k) launch_iteration(c, gamma, opts.field_mode, tc);
-          return;
-        }
-        cudaGraphDestroy(graph);
-        c->g_epoch = c->buf_epoch;
-        c->g_interval = interval;
-        c->g_field = opts.field_mode;
-        c->g_tc = tc;
-        c->g_gamma = gamma;
-      }
       CK(cudaGraphLaunch(c->gexec, s));
     } else {
       for (uint64_t k = 0; k < n; ++k) launch_iteration(c, gamma, opts.field_mode, tc);
     }
   }
 
+  // A pinned snapshot buffer of at least N positions from the context's
+  // free list (allocated when none fits).
+  HostSnap *take_snap() {
+    const size_t N = c->hp.N;
+    auto &fl = c->hsnap_free;
+    for (size_t k = 0; k < fl.size(); ++k)
+      if (fl[k]->pos && fl[k]->cap >= N) {
+        HostSnap *h = fl[k];
+        fl.erase(fl.begin() + k);
+        return h;
+      }
+    HostSnap *h;
+    if (!fl.empty()) {
+      h = fl.back();
+      fl.pop_back();
+    } else {
+      c->hsnaps.emplace_back(new HostSnap());
+      h = c->hsnaps.back().get();
+    }
+    h->reserve(N);
+    return h;
+  }
+  void give_snap(HostSnap *h) {
+    if (h) c->hsnap_free.push_back(h);
+  }
+
   void release(Checkpoint *cp) {
     if (!cp) return;
-    std::vector<float>().swap(cp->xs);
-    std::vector<float>().swap(cp->ys);
-    std::vector<int32_t>().swap(cp->sx);
-    std::vector<int32_t>().swap(cp->sy);
+    give_snap(cp->hs);
+    cp->hs = nullptr;
     if (cp->slot >= 0) {
       free_slots.push_back(cp->slot);
       cp->slot = -1;
@@ -1357,7 +1533,6 @@ struct JobState {
   bool pump_loop(bool block) {
     const HostProblem &hp = c->hp;
     cudaStream_t s = c->stream;
-    auto &snaps = c->snaps;
     auto &logs = c->logs;
     auto &scs = c->scs;
     auto &evs = c->slot_ev;
@@ -1377,6 +1552,7 @@ struct JobState {
       const int slot = slot_rr;
       slot_rr = (slot_rr + 1) % inflight;
       const uint64_t n = ch.last - ch.first + 1;
+      HostSnap *hs = nullptr;
       if (gpu_legal) {
         // Snapshot on the device and legalise it on the slot's stream.
         auto cp = std::make_unique<Checkpoint>();
@@ -1391,19 +1567,22 @@ struct JobState {
         launch_gpu_legal(c, L);
         cps.push_back(std::move(cp));
       } else {
-        CK(cudaMemcpyAsync(snaps[slot]->p, c->x.p, sizeof(float2) * hp.N, cudaMemcpyDeviceToHost, s));
+        hs = take_snap();
+        CK(cudaMemcpyAsync(hs->pos, c->x.p, sizeof(float2) * hp.N, cudaMemcpyDeviceToHost, s));
         g_d2h += sizeof(float2) * hp.N;
       }
       CK(cudaMemcpyAsync(logs[slot]->p, c->log.p + ch.first, sizeof(IterLog) * n, cudaMemcpyDeviceToHost, s));
       CK(cudaMemcpyAsync(scs[slot]->p, c->sc.p, sizeof(DevScalars), cudaMemcpyDeviceToHost, s));
       g_d2h += sizeof(IterLog) * n + sizeof(DevScalars);
       CK(cudaEventRecord(evs[slot], s));
-      pending.push_back({next_chunk, slot});
+      pending.push_back({next_chunk, slot, hs});
       ++next_chunk;
       progressed = true;
     }
     while (!pending.empty()) {
-      auto [ci, slot] = pending.front();
+      const size_t ci = pending.front().chunk;
+      const int slot = pending.front().slot;
+      HostSnap *hs = pending.front().hs;
       if (block) {
         CK(cudaEventSynchronize(evs[slot]));
       } else {
@@ -1416,6 +1595,7 @@ struct JobState {
       processed = ci + 1;
       if (stop) {  // ran ahead of convergence: discard
         if (gpu_legal) cps[ci]->discard = true;
+        give_snap(hs);
         continue;
       }
       const Chunk &ch = chunks[ci];
@@ -1424,6 +1604,7 @@ struct JobState {
         final_st = EPLACE_ERR_TIMEOUT;
         stop = true;
         if (gpu_legal) cps[ci]->discard = true;
+        give_snap(hs);
         continue;
       }
       const uint64_t n = ch.last - ch.first + 1;
@@ -1436,12 +1617,7 @@ struct JobState {
         auto cp = std::make_unique<Checkpoint>();
         cp->iter = (int32_t)ch.last;
         cp->chunk = ci;
-        cp->xs.resize(hp.N);
-        cp->ys.resize(hp.N);
-        for (uint32_t i = 0; i < hp.N; ++i) {
-          cp->xs[i] = snaps[slot]->p[i].x;
-          cp->ys[i] = snaps[slot]->p[i].y;
-        }
+        cp->hs = hs;  // the legaliser reads the pinned snapshot in place
         Checkpoint *raw = cp.get();
         cps.push_back(std::move(cp));
         outstanding.fetch_add(1, std::memory_order_acq_rel);
@@ -1450,10 +1626,11 @@ struct JobState {
         pool->submit([raw, cc, out](int tid) {
           const HostProblem &php = cc->hp;
           const auto t0 = std::chrono::steady_clock::now();
-          raw->sx.resize(php.N);
-          raw->sy.resize(php.N);
-          raw->st = cc->legal[tid]->run(raw->xs.data(), raw->ys.data(), raw->sx.data(), raw->sy.data(), &raw->disp);
-          if (raw->st == EPLACE_OK) raw->hpwl = hpwl_host(php, raw->sx.data(), raw->sy.data());
+          HostSnap &h = *raw->hs;
+          h.sx.resize(php.N);
+          h.sy.resize(php.N);
+          raw->st = cc->legal[tid]->run(&h.pos[0].x, &h.pos[0].y, 2, h.sx.data(), h.sy.data(), &raw->disp);
+          if (raw->st == EPLACE_OK) raw->hpwl = hpwl_host(php, h.sx.data(), h.sy.data());
           raw->secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
           raw->done.store(true, std::memory_order_release);
           out->fetch_sub(1, std::memory_order_acq_rel);
@@ -1518,10 +1695,13 @@ struct JobState {
           }
           res->best_iter = best->iter;
         } else if (best) {
-          fsx = best->sx;
-          fsy = best->sy;
-          bx = best->xs;
-          by = best->ys;
+          const HostSnap &h = *best->hs;
+          std::copy(h.sx.begin(), h.sx.begin() + hp.N, fsx.begin());
+          std::copy(h.sy.begin(), h.sy.begin() + hp.N, fsy.begin());
+          for (uint32_t i = 0; i < hp.N; ++i) {
+            bx[i] = h.pos[i].x;
+            by[i] = h.pos[i].y;
+          }
           res->best_iter = best->iter;
         } else {
           for (uint32_t i = 0; i < hp.N; ++i) {
@@ -1588,7 +1768,12 @@ struct JobState {
   int inflight = 1;
   std::vector<int> free_slots;
   uint64_t launched_iters = 0;
-  std::deque<std::pair<size_t, int>> pending;  // (chunk index, pinned slot)
+  struct Pending {
+    size_t chunk;
+    int slot;      // pinned log / scalars slot
+    HostSnap *hs;  // the positions, when the host legalises
+  };
+  std::deque<Pending> pending;
   size_t next_chunk = 0, processed = 0;
   bool stop = false;
   size_t converged_chunk = 0;
@@ -1870,6 +2055,7 @@ eplace_status eplace_profile_stages(eplace_ctx *c, const eplace_cfg *cfg, const 
 // Stage entry points (host buffers in/out, one kernel family each).
 // ---------------------------------------------------------------------------
 static void upload_look(eplace_ctx *c, const float *x, const float *y) {
+  AllocOn on_stream(c->stream);
   std::vector<float2> p(c->hp.N);
   for (uint32_t i = 0; i < c->hp.N; ++i) p[i] = make_float2(x[i], y[i]);
   if (c->hp.N) CK(cudaMemcpyAsync(c->look.p, p.data(), sizeof(float2) * c->hp.N, cudaMemcpyHostToDevice, c->stream));

@@ -55,6 +55,7 @@ struct LegalBase {
   explicit LegalBase(const HostProblem &hp);
   int32_t W = 0, H = 0, WR = 0;       // WR: 64-bit words per row
   std::vector<uint64_t> free0;        // per-row bitmaps, bit set = free
+  std::vector<uint64_t> sum0;         // per row (WR <= 64): bit w set = word w has a free site
   std::vector<uint32_t> order;
 };
 
@@ -62,14 +63,18 @@ struct LegalBase {
 // choice and tie-break.  One instance per thread (owns its working map).
 struct Legalizer {
   Legalizer(const HostProblem &hp, const LegalBase &base);
-  // Returns EPLACE_OK or EPLACE_ERR_NO_BELS.
-  eplace_status run(const float *x, const float *y, int32_t *site_x, int32_t *site_y,
+  // Returns EPLACE_OK or EPLACE_ERR_NO_BELS.  Cell i's target is
+  // (x[i * stride], y[i * stride]): stride 2 reads interleaved (x, y) pairs.
+  eplace_status run(const float *x, const float *y, size_t stride, int32_t *site_x, int32_t *site_y,
                     double *displacement);
+  eplace_status run(const float *x, const float *y, int32_t *site_x, int32_t *site_y, double *displacement) {
+    return run(x, y, 1, site_x, site_y, displacement);
+  }
 
  private:
   const HostProblem &hp_;
   const LegalBase &base_;
-  std::vector<uint64_t> free_;
+  std::vector<uint64_t> free_, sum_;
 };
 
 // total_hpwl (metrics/wirelength.rs:10-51) on the host.

@@ -164,8 +164,9 @@ void pin_weights(const HostProblem &hp, std::vector<double> &w) {
 //    answer, and among tied ones the lowest tile wins, as in the scan.
 //  * otherwise rows are visited outward from the target; in one row the
 //    best free site is the nearest free bit left of or right of floor(x)
-//    (64-bit free maps), and a row whose dy^2 already exceeds the best cost
-//    cannot win or tie.
+//    (64-bit free maps; a per-row summary word, one bit per map word,
+//    jumps over full words in one step on rows up to 4096 sites), and a
+//    row whose dy^2 already exceeds the best cost cannot win or tie.
 // Macros (w*h > 1, an extension) go first onto fully free blocks, cost
 // measured at the block centre.
 // ---------------------------------------------------------------------------
@@ -178,6 +179,12 @@ LegalBase::LegalBase(const HostProblem &hp) : W(hp.W), H(hp.H) {
   }
   for (uint32_t f = 0; f < hp.F; ++f)
     if (hp.f_logic[f]) free0[(size_t)hp.fy[f] * WR + (hp.fx[f] >> 6)] &= ~(1ull << (hp.fx[f] & 63));
+  if (WR <= 64) {
+    sum0.assign(H, 0);
+    for (int32_t y = 0; y < H; ++y)
+      for (int32_t w = 0; w < WR; ++w)
+        if (free0[(size_t)y * WR + w]) sum0[y] |= 1ull << w;
+  }
   order.reserve(hp.N);
   for (uint32_t i = 0; i < hp.N; ++i)
     if (hp.cw[i] * hp.ch[i] > 1) order.push_back(i);
@@ -187,34 +194,51 @@ LegalBase::LegalBase(const HostProblem &hp) : W(hp.W), H(hp.H) {
 
 Legalizer::Legalizer(const HostProblem &hp, const LegalBase &base) : hp_(hp), base_(base) {
   free_.resize(base.free0.size());
+  sum_.resize(base.sum0.size());
 }
 
 namespace {
-// highest free x <= pos in the row, or -1
-inline int32_t free_at_or_left(const uint64_t *row, int32_t pos) {
+// highest free x <= pos in the row, or -1.  sum (when given) has bit w set
+// for each word w of the row with a free site, so a full stretch of words
+// is skipped in one step.
+inline int32_t free_at_or_left(const uint64_t *row, const uint64_t *sum, int32_t pos) {
   if (pos < 0) return -1;
   int32_t w = pos >> 6;
   uint64_t m = row[w] & (((pos & 63) == 63) ? ~0ull : ((2ull << (pos & 63)) - 1));
+  if (m) return (w << 6) + 63 - __builtin_clzll(m);
+  if (sum) {
+    const uint64_t s = *sum & ((1ull << w) - 1);
+    if (!s) return -1;
+    const int32_t w2 = 63 - __builtin_clzll(s);
+    return (w2 << 6) + 63 - __builtin_clzll(row[w2]);
+  }
   while (true) {
-    if (m) return (w << 6) + 63 - __builtin_clzll(m);
     if (--w < 0) return -1;
     m = row[w];
+    if (m) return (w << 6) + 63 - __builtin_clzll(m);
   }
 }
 // lowest free x >= pos in the row, or -1
-inline int32_t free_at_or_right(const uint64_t *row, int32_t pos, int32_t W, int32_t words) {
+inline int32_t free_at_or_right(const uint64_t *row, const uint64_t *sum, int32_t pos, int32_t W, int32_t words) {
   if (pos >= W) return -1;
   if (pos < 0) pos = 0;
   int32_t w = pos >> 6;
   uint64_t m = row[w] & (~0ull << (pos & 63));
-  while (true) {
-    if (m) {
-      int32_t x = (w << 6) + __builtin_ctzll(m);
-      return x < W ? x : -1;
+  if (!m) {
+    if (sum) {
+      const uint64_t s = (w >= 63) ? 0ull : (*sum & (~0ull << (w + 1)));
+      if (!s) return -1;
+      w = __builtin_ctzll(s);
+      m = row[w];
+    } else {
+      do {
+        if (++w >= words) return -1;
+        m = row[w];
+      } while (!m);
     }
-    if (++w >= words) return -1;
-    m = row[w];
   }
+  const int32_t x = (w << 6) + __builtin_ctzll(m);
+  return x < W ? x : -1;
 }
 inline bool is_free(const uint64_t *fm, int32_t WR, int32_t x, int32_t y) {
   return (fm[(size_t)y * WR + (x >> 6)] >> (x & 63)) & 1;
@@ -240,14 +264,16 @@ inline int nearest_ints(double t, int32_t n, int32_t (&out)[2]) {
 }
 }  // namespace
 
-eplace_status Legalizer::run(const float *x, const float *y, int32_t *site_x, int32_t *site_y,
+eplace_status Legalizer::run(const float *x, const float *y, size_t stride, int32_t *site_x, int32_t *site_y,
                              double *displacement) {
   const int32_t W = hp_.W, H = hp_.H, WR = base_.WR;
   std::copy(base_.free0.begin(), base_.free0.end(), free_.begin());
+  std::copy(base_.sum0.begin(), base_.sum0.end(), sum_.begin());
   uint64_t *fm = free_.data();
+  uint64_t *sm = sum_.empty() ? nullptr : sum_.data();
   double total = 0.0;
   for (uint32_t i : base_.order) {
-    const double tx = (double)x[i], ty = (double)y[i];
+    const double tx = (double)x[i * stride], ty = (double)y[i * stride];
     const int w = hp_.cw[i], h = hp_.ch[i];
     double best = INFINITY;
     int64_t best_t = -1;
@@ -270,10 +296,11 @@ eplace_status Legalizer::run(const float *x, const float *y, int32_t *site_x, in
         const int32_t fx0 = (int32_t)std::floor(tx);
         auto scan_row = [&](int32_t row) {
           const uint64_t *r = fm + (size_t)row * WR;
+          const uint64_t *rs = sm ? sm + row : nullptr;
           const double dy = (double)row - ty;
           const double dy2 = dy * dy;
-          const int32_t l = free_at_or_left(r, std::min(fx0, W - 1));
-          const int32_t rr = free_at_or_right(r, fx0 + 1, W, WR);
+          const int32_t l = free_at_or_left(r, rs, std::min(fx0, W - 1));
+          const int32_t rr = free_at_or_right(r, rs, fx0 + 1, W, WR);
           if (l >= 0) {
             const double dx = (double)l - tx, cost = dx * dx + dy2;
             const int64_t t = (int64_t)row * W + l;
@@ -409,7 +436,9 @@ eplace_status Legalizer::run(const float *x, const float *y, int32_t *site_x, in
     for (int dy = 0; dy < h; ++dy)
       for (int dx = 0; dx < w; ++dx) {
         const int32_t xx = bx + dx;
-        fm[(size_t)(by + dy) * WR + (xx >> 6)] &= ~(1ull << (xx & 63));
+        uint64_t &word = fm[(size_t)(by + dy) * WR + (xx >> 6)];
+        word &= ~(1ull << (xx & 63));
+        if (sm && !word) sm[by + dy] &= ~(1ull << (xx >> 6));
       }
     site_x[i] = bx;
     site_y[i] = by;
