@@ -64,7 +64,10 @@ def parse():
     ap.add_argument("--served-jobs", type=int, default=200,
                     help="jobs of the served stream (a subsample of the 2,000-job stream, same distribution)")
     ap.add_argument("--served-rate", type=float, default=100.0,
-                    help="offered rate of the served stream, jobs/s (above the plain form's capacity)")
+                    help="offered rate of the served stream, jobs/s (above the plain form's capacity, "
+                         "within the engine's)")
+    ap.add_argument("--served-rate-saturated", type=float, default=200.0,
+                    help="second offered rate, above both forms' capacity (0: skip)")
     ap.add_argument("--max-jobs", type=int, default=16, help="jobs the engine keeps on the GPU at once")
     return ap.parse_args()
 
@@ -318,11 +321,11 @@ def batched_arm(args, dist, E, cfg):
     }
 
 
-def served_arm(args, dist, E, cfg):
+def served_arm(args, dist, E, cfg, rate):
     """A Poisson stream (fixed offered rate) of 1k..300k-cell jobs: the
     engine (continuous batching) against the plain form, which serves the
     same stream one job at a time in arrival order."""
-    specs, arrivals = E.served_stream(args.served_jobs, args.served_rate)
+    specs, arrivals = E.served_stream(args.served_jobs, rate)
     jobs = _mixed_jobs(E, specs, dist.rank)
     eng_opts = E.RunOptions(field_mode=1, dct_mode=1)
     plain_opts = E.RunOptions(field_mode=1, dct_mode=0)
@@ -340,7 +343,7 @@ def served_arm(args, dist, E, cfg):
 
     return {
         "workload": "served_poisson_%d_jobs_1k_300k" % len(jobs), "jobs": n,
-        "offered_rate_jobs_per_s": args.served_rate * dist.world,
+        "offered_rate_jobs_per_s": rate * dist.world,
         "sample": "first %d jobs of the 2,000-job stream (seeds 100000+j, arrivals seed 7)" % len(jobs),
         "engine": {"jobs_per_s": n / t_eng, "p50_latency_s": pct(lat_eng, 50), "p99_latency_s": pct(lat_eng, 99),
                    "max_jobs": args.max_jobs, "dct": "bf16x3 tcgen05 (fp32 where bins < 128)"},
@@ -531,7 +534,10 @@ def ours(args, dist):
 
     mixed_cfg = E.ElectroPlaceCfg(max_iters=500)
     batched = None if args.no_batched else batched_arm(args, dist, E, mixed_cfg)
-    served = None if args.no_served else served_arm(args, dist, E, mixed_cfg)
+    served = None if args.no_served else served_arm(args, dist, E, mixed_cfg, args.served_rate)
+    served_sat = None
+    if not args.no_served and args.served_rate_saturated > 0:
+        served_sat = served_arm(args, dist, E, mixed_cfg, args.served_rate_saturated)
 
     if dist.rank != 0:
         return
@@ -614,6 +620,7 @@ def ours(args, dist):
         "clocks": ck,
         "batched": batched,
         "served": served,
+        "served_saturated": served_sat,
     }
     print(json.dumps(line), flush=True)
 

@@ -267,7 +267,6 @@ struct eplace_ctx {
   // problem on device
   DBuf<uint32_t> net_off, pin_cell;
   DBuf<uint8_t> has_driver;
-  DBuf<WaTask> wa_tasks;
   DBuf<uint32_t> wa_off, wa_pins;  // CSR copy, nets ordered by pin count
   DBuf<float2> half;
   DBuf<float> area, pw;
@@ -334,7 +333,8 @@ struct eplace_ctx {
   bool shared_device = false;  // set by the job engine: other jobs' kernels run beside this one
   int mat_bx = -1, mat_by = -1;  // bin grid the DCT matrices were built for
   uint64_t load_gen = 0;         // bumped by every (re)load of a problem
-  int n_wa_tasks = 0;
+  WaClass wa_cls[kWaClasses] = {};  // degree classes of the sorted CSR
+  int wa_warps = 0;
 
   // Device memory this context holds (allocated capacities).
   uint64_t device_bytes() const;
@@ -365,10 +365,8 @@ eplace_status cuda_fail(eplace_ctx *c, const CudaError &e) {
   return EPLACE_ERR_CUDA;
 }
 
-// Packs whole nets into warp tasks of at most 32 pins (and 32 nets); a net
-// with more than 32 pins gets a task of its own.
 // The WA kernel works on a copy of the CSR with the nets ordered by pin
-// count (stable), so each warp task holds nets of similar size.  Net order
+// count (stable), so nets of one degree class are contiguous.  Net order
 // does not change the result: the gradient accumulates in fixed point.
 void degree_sorted_csr(const HostProblem &hp, std::vector<uint32_t> &off, std::vector<uint32_t> &pins) {
   std::vector<uint32_t> order(hp.NN);
@@ -386,32 +384,21 @@ void degree_sorted_csr(const HostProblem &hp, std::vector<uint32_t> &off, std::v
   }
 }
 
-// Packs whole nets into warp tasks of at most 32 pins (and 32 nets); a net
-// with more than 32 pins gets a task of its own.
-std::vector<WaTask> build_wa_tasks(const std::vector<uint32_t> &off) {
-  std::vector<WaTask> t;
+// Splits the degree-sorted nets into the WA kernel's degree classes and
+// numbers the warps (32 / group width nets per warp).  Returns the warps.
+int build_wa_classes(const std::vector<uint32_t> &off, WaClass (&cls)[kWaClasses]) {
   const uint32_t NN = (uint32_t)off.size() - 1;
   uint32_t n = 0;
-  while (n < NN) {
-    const uint32_t b = off[n];
-    const uint32_t d = off[n + 1] - b;
-    if (d > 32) {
-      t.push_back(make_int4((int)b, (int)(b + d), (int)n, 1));
-      ++n;
-      continue;
-    }
-    uint32_t m = n, e = b;
-    while (m < NN && m - n < 32) {
-      const uint32_t dd = off[m + 1] - off[m];
-      if (dd > 32 || (off[m + 1] - b) > 32) break;
-      e = off[m + 1];
-      ++m;
-    }
-    if (e > b) t.push_back(make_int4((int)b, (int)e, (int)n, (int)(m - n)));
-    if (m == n) ++m;  // a run of empty nets
-    n = m;
+  while (n < NN && off[n + 1] - off[n] < 2) ++n;  // no gradient below two pins
+  int warps = 0;
+  for (int j = 0; j < kWaClasses; ++j) {
+    const uint32_t first = n;
+    while (n < NN && off[n + 1] - off[n] <= (uint32_t)kWaDegHi[j]) ++n;
+    const int per_warp = 32 / kWaGroup[j];
+    cls[j] = WaClass{(int)first, (int)(n - first), warps};
+    warps += (int)((n - first + per_warp - 1) / per_warp);
   }
-  return t;
+  return warps;
 }
 
 // Host copies of the FP32 DCT matrices of one bin grid (rustdct conventions,
@@ -535,8 +522,16 @@ int grid_for(int n, int block, int cap) {
 
 // --- kernel sequence of one iteration ------------------------------------
 void launch_wa_stage(eplace_ctx *c, float gamma) {
-  WaArgs a{c->wa_tasks.p, c->n_wa_tasks, c->wa_off.p, c->wa_pins.p, c->look.p, c->acc.p, c->hp.N, gamma};
-  CK(launch_wa(a, grid_for(c->n_wa_tasks * 32, kWaBlock, c->num_sms * 16), c->stream));
+  WaArgs a{};
+  std::copy(c->wa_cls, c->wa_cls + kWaClasses, a.cls);
+  a.nwarps = c->wa_warps;
+  a.net_off = c->wa_off.p;
+  a.pin_cell = c->wa_pins.p;
+  a.pos = c->look.p;
+  a.acc = c->acc.p;
+  a.N = c->hp.N;
+  a.gamma = gamma;
+  CK(launch_wa(a, grid_for(c->wa_warps * 32, kWaBlock, c->num_sms * 16), c->stream));
 }
 
 void launch_scatter_stage(eplace_ctx *c) {
@@ -954,10 +949,7 @@ void load_into(eplace_ctx *c, HostProblem &&hp_in) {
     c->wa_off.upload(soff.data(), soff.size(), s);
     c->wa_pins.ensure(std::max<size_t>(spins.size(), 1));
     c->wa_pins.upload(spins.data(), spins.size(), s);
-    std::vector<WaTask> tasks = build_wa_tasks(soff);
-    c->wa_tasks.ensure(std::max<size_t>(tasks.size(), 1));
-    c->wa_tasks.upload(tasks.data(), tasks.size(), s);
-    c->n_wa_tasks = (int)tasks.size();
+    c->wa_warps = build_wa_classes(soff, c->wa_cls);
   }
   const size_t N1 = std::max<size_t>(hp.N, 1);
   std::vector<float2> half(hp.N);
@@ -1913,7 +1905,7 @@ eplace_status ctx_load_problem(eplace_ctx *c, HostProblem &&hp) {
 uint64_t eplace_ctx::device_bytes() const {
   uint64_t b = 0;
   auto add = [&b](const auto &buf) { b += (uint64_t)buf.cap * sizeof(*buf.p); };
-  add(net_off); add(pin_cell); add(has_driver); add(wa_tasks); add(wa_off); add(wa_pins);
+  add(net_off); add(pin_cell); add(has_driver); add(wa_off); add(wa_pins);
   add(half); add(area); add(pw); add(look); add(x); add(xp); add(g); add(gprev); add(tmp_wl); add(tmp_den);
   add(acc); add(dens); add(rho); add(T); add(Exh); add(Eyh); add(U); add(V); add(Ex); add(Ey); add(phi);
   add(mB1); add(mL2); add(mB3); add(mL4); add(mB5); add(mL6); add(mB3g); add(mL6g);

@@ -1,8 +1,9 @@
 // kernels.cu -- sm_100a kernels of the ElectroPlace iteration.
 //
 //   k_wa            WA wirelength gradient (placer/common.rs:205-291,
-//                   solver/wa.rs:51-101): net-segmented warp reductions over
-//                   the CSR pin array, deterministic fixed-point scatter.
+//                   solver/wa.rs:51-101): nets grouped by degree class, a
+//                   fixed lane-group width per class (one thread per net up
+//                   to a warp per net), deterministic fixed-point scatter.
 //   k_scatter       cell -> bin overlap areas (electro_place/density.rs:54-76),
 //                   fixed-point atomics (order independent, bit-reproducible).
 //   k_density_final FP64 sum / overflow (density.rs:79-86), FP32 charge map
@@ -147,23 +148,45 @@ __device__ __forceinline__ float seg_sum(float v, int lane, int end, int head, i
   return __shfl_sync(kFull, v, head);
 }
 
-// A net of 33 .. 32*K pins on one warp with its pins held in registers
-// (lane l holds pins l, l + 32, ...): one gather of pin ids and positions
-// instead of one per pass.  Per-lane sums run in the same order as the
-// three-pass loop below, so the results are the same.
-template <int K>
-__device__ void wa_big_net_reg(const WaArgs &a, int pb, int pe, int lane) {
+// Reduction over the g lanes of an aligned lane group (g a power of two,
+// the same on all lanes of the warp); every lane takes part.  Each xor step
+// adds a pair in both orders, and FP32 addition commutes, so all lanes of a
+// group get the same bits.
+template <typename Op>
+__device__ __forceinline__ float group_allreduce(float v, int g, Op op) {
+  for (int o = g >> 1; o > 0; o >>= 1) v = op(v, __shfl_xor_sync(kFull, v, o));
+  return v;
+}
+
+// Nets of one degree class: g lanes per net (32 / g nets per warp), lane l
+// of a group holding pins l, l + g, ..., l + (np - 1) g of its net in
+// registers (pin ids and positions gathered once; np <= P, uniform over the
+// warp).  Max/min and the eight exponential sums are reduced over the group;
+// the exponentials are kept for the gradient when P <= 4 and recomputed
+// otherwise (register budget).  Nets with fewer than two pins contribute
+// nothing (wa.rs:58).
+template <int P>
+__device__ __forceinline__ void wa_group(const WaArgs &a, const WaClass &cl, int g, int np, int wi, int lane) {
+  constexpr bool kKeep = P <= 4;
   const float kg = a.gamma * kLog2e;
-  uint32_t cc[K];
-  float px[K], py[K];
+  const int gl = lane & (g - 1);
+  const int idx = wi * (32 / g) + lane / g;
+  const bool valid = idx < cl.nets;
+  uint32_t pb = 0, pe = 0;
+  if (valid) {
+    pb = a.net_off[cl.first_net + idx];
+    pe = a.net_off[cl.first_net + idx + 1];
+  }
+  uint32_t cc[P];
+  float px[P], py[P];
 #pragma unroll
-  for (int k = 0; k < K; ++k) {
-    const int q = pb + lane + 32 * k;
-    cc[k] = (q < pe) ? a.pin_cell[q] : 0xffffffffu;
+  for (int k = 0; k < P; ++k) {
+    const uint32_t q = pb + gl + g * k;
+    cc[k] = (k < np && q < pe) ? a.pin_cell[q] : 0xffffffffu;
   }
   float mx = -INFINITY, mn = INFINITY, my = -INFINITY, ny = INFINITY;
 #pragma unroll
-  for (int k = 0; k < K; ++k) {
+  for (int k = 0; k < P; ++k) {
     const float2 p = (cc[k] != 0xffffffffu) ? a.pos[cc[k]] : make_float2(0.f, 0.f);
     px[k] = p.x;
     py[k] = p.y;
@@ -174,35 +197,56 @@ __device__ void wa_big_net_reg(const WaArgs &a, int pb, int pe, int lane) {
       ny = fminf(ny, p.y);
     }
   }
-  mx = warp_allreduce(mx, OpMax());
-  mn = warp_allreduce(mn, OpMin());
-  my = warp_allreduce(my, OpMax());
-  ny = warp_allreduce(ny, OpMin());
+  mx = group_allreduce(mx, g, OpMax());
+  mn = group_allreduce(mn, g, OpMin());
+  my = group_allreduce(my, g, OpMax());
+  ny = group_allreduce(ny, g, OpMin());
+  float e[kKeep ? P : 1][4];
   float s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll
-  for (int k = 0; k < K; ++k) {
+  for (int k = 0; k < P; ++k) {
     if (cc[k] == 0xffffffffu) continue;
     const float ux = px[k] - mx, vx = px[k] - mn, uy = py[k] - my, vy = py[k] - ny;
     const float epx = ex2(kg * ux), emx = ex2(-kg * vx);
     const float epy = ex2(kg * uy), emy = ex2(-kg * vy);
+    if (kKeep) {
+      e[kKeep ? k : 0][0] = epx;
+      e[kKeep ? k : 0][1] = emx;
+      e[kKeep ? k : 0][2] = epy;
+      e[kKeep ? k : 0][3] = emy;
+    }
     s[0] += epx; s[1] += ux * epx; s[2] += emx; s[3] += vx * emx;
     s[4] += epy; s[5] += uy * epy; s[6] += emy; s[7] += vy * emy;
   }
 #pragma unroll
-  for (int k = 0; k < 8; ++k) s[k] = warp_allreduce(s[k], OpAdd());
+  for (int k = 0; k < 8; ++k) s[k] = group_allreduce(s[k], g, OpAdd());
+  if (pe - pb < 2) return;  // also the lanes of an empty slot (pb == pe)
   const float ipx = 1.0f / s[0], imx = 1.0f / s[2], ipy = 1.0f / s[4], imy = 1.0f / s[6];
 #pragma unroll
-  for (int k = 0; k < K; ++k) {
+  for (int k = 0; k < P; ++k) {
     const uint32_t c = cc[k];
-    if (c >= a.N) continue;  // fixed cells and padding lanes
+    if (c >= a.N) continue;  // fixed cells and empty slots
     const float ux = px[k] - mx, vx = px[k] - mn, uy = py[k] - my, vy = py[k] - ny;
-    const float gx = wa_pin_grad(ux, vx, ex2(kg * ux), ex2(-kg * vx), ipx, s[1], imx, s[3], a.gamma);
-    const float gy = wa_pin_grad(uy, vy, ex2(kg * uy), ex2(-kg * vy), ipy, s[5], imy, s[7], a.gamma);
+    float epx, emx, epy, emy;
+    if (kKeep) {
+      epx = e[kKeep ? k : 0][0];
+      emx = e[kKeep ? k : 0][1];
+      epy = e[kKeep ? k : 0][2];
+      emy = e[kKeep ? k : 0][3];
+    } else {
+      epx = ex2(kg * ux);
+      emx = ex2(-kg * vx);
+      epy = ex2(kg * uy);
+      emy = ex2(-kg * vy);
+    }
+    const float gx = wa_pin_grad(ux, vx, epx, emx, ipx, s[1], imx, s[3], a.gamma);
+    const float gy = wa_pin_grad(uy, vy, epy, emy, ipy, s[5], imy, s[7], a.gamma);
     atomicAdd(&a.acc[2 * c], to_fix(gx));
     atomicAdd(&a.acc[2 * c + 1], to_fix(gy));
   }
 }
 
+// A net of more than 224 pins on one warp, three passes over its pins.
 __device__ void wa_big_net(const WaArgs &a, int pb, int pe, int lane) {
   const float kg = a.gamma * kLog2e;
   float mx = -INFINITY, mn = INFINITY, my = -INFINITY, ny = INFINITY;
@@ -241,69 +285,34 @@ __device__ void wa_big_net(const WaArgs &a, int pb, int pe, int lane) {
   }
 }
 
-// Warp tasks come from nets ordered by degree, so the nets of one task have
-// similar pin counts and the segmented sums need only ceil(log2(longest
-// net)) shuffle rounds (one for a task of 2-pin nets).
+// Nets are ordered by degree and split into degree classes (WaClass): each
+// warp takes 32 / G nets of one class, so the reductions run over a fixed
+// group width with no per-lane segment logic.  Warps are visited from the
+// heaviest class down.
 __global__ void __launch_bounds__(kWaBlock) k_wa(const WaArgs a) {
   const int lane = threadIdx.x & 31;
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nw = (gridDim.x * blockDim.x) >> 5;
-  const float kg = a.gamma * kLog2e;
-  for (int t = gw; t < a.ntasks; t += nw) {
-    const WaTask tk = a.tasks[t];
-    const int pb = tk.x, npin = tk.y - tk.x;
-    if (npin > 32) {
-      if (npin <= 32 * 7) wa_big_net_reg<7>(a, pb, tk.y, lane);
-      else wa_big_net(a, pb, tk.y, lane);
-      continue;
-    }
-    // Segment heads: bit j set where a net starts at lane j.
-    uint32_t bits = 0;
-    if (lane < tk.w) {
-      const uint32_t off = a.net_off[tk.z + lane] - (uint32_t)pb;
-      if (off < (uint32_t)npin) bits = 1u << off;
-    }
-    bits = __reduce_or_sync(kFull, bits);
-    const bool valid = lane < npin;
-    int head, end;
-    if (valid) {
-      const uint32_t le = kFull >> (31 - lane);
-      head = 31 - __clz(bits & le);
-      const uint32_t above = bits & ~le;
-      end = above ? (__ffs(above) - 1) : npin;
-    } else {  // idle lanes form segments of their own
-      head = lane;
-      end = lane + 1;
-    }
-    const int len = end - head;
-    const unsigned mask = (len == 32) ? kFull : (((1u << len) - 1u) << head);
-    const int maxlen = (int)__reduce_max_sync(kFull, (unsigned)len);
-    const int steps = 32 - __clz(maxlen - 1);  // ceil(log2(maxlen)), 0 for 1
-    uint32_t c = 0xffffffffu;
-    float2 p = make_float2(0.f, 0.f);
-    if (valid) {
-      c = a.pin_cell[pb + lane];
-      p = a.pos[c];
-    }
-    const float mx = seg_max(p.x, mask), mn = seg_min(p.x, mask);
-    const float my = seg_max(p.y, mask), ny = seg_min(p.y, mask);
-    const float ux = p.x - mx, vx = p.x - mn, uy = p.y - my, vy = p.y - ny;
-    const float epx = ex2(kg * ux), emx = ex2(-kg * vx);
-    const float epy = ex2(kg * uy), emy = ex2(-kg * vy);
-    const float Spx = seg_sum(epx, lane, end, head, steps);
-    const float Apx = seg_sum(ux * epx, lane, end, head, steps);
-    const float Smx = seg_sum(emx, lane, end, head, steps);
-    const float Amx = seg_sum(vx * emx, lane, end, head, steps);
-    const float Spy = seg_sum(epy, lane, end, head, steps);
-    const float Apy = seg_sum(uy * epy, lane, end, head, steps);
-    const float Smy = seg_sum(emy, lane, end, head, steps);
-    const float Amy = seg_sum(vy * emy, lane, end, head, steps);
-    // Nets with fewer than two pins are skipped, as in the reference.
-    if (valid && c < a.N && len >= 2) {
-      const float gx = wa_pin_grad(ux, vx, epx, emx, 1.0f / Spx, Apx, 1.0f / Smx, Amx, a.gamma);
-      const float gy = wa_pin_grad(uy, vy, epy, emy, 1.0f / Spy, Apy, 1.0f / Smy, Amy, a.gamma);
-      atomicAdd(&a.acc[2 * c], to_fix(gx));
-      atomicAdd(&a.acc[2 * c + 1], to_fix(gy));
+  for (int t = gw; t < a.nwarps; t += nw) {
+    const int w = a.nwarps - 1 - t;
+    int j = 0;
+#pragma unroll
+    for (int k = 1; k < kWaClasses; ++k) j += (w >= a.cls[k].first_warp) ? 1 : 0;
+    const WaClass &cl = a.cls[j];
+    const int wi = w - cl.first_warp;
+    switch (j) {
+      case 0: case 1: case 2: case 3: case 4: {  // up to 32 pins: 1..8 lanes per net, <= 4 pins per lane
+        const int g = j <= 1 ? 1 : (1 << (j - 1));   // kWaGroup
+        wa_group<4>(a, cl, g, j == 0 ? 2 : 4, wi, lane);
+        break;
+      }
+      case 5: case 6: case 7:  // 33..224 pins: a warp per net, <= 7 pins per lane
+        wa_group<7>(a, cl, 32, j == 5 ? 2 : (j == 6 ? 4 : 7), wi, lane);
+        break;
+      default: {
+        const uint32_t n = cl.first_net + wi;
+        wa_big_net(a, a.net_off[n], a.net_off[n + 1], lane);
+      }
     }
   }
 }
@@ -779,7 +788,7 @@ __global__ void __launch_bounds__(kHpwlBlock) k_hpwl(const HpwlArgs a) {
 }  // namespace
 
 cudaError_t launch_wa(const WaArgs &a, int grid, cudaStream_t s) {
-  if (a.ntasks == 0) return cudaSuccess;
+  if (a.nwarps == 0) return cudaSuccess;
   k_wa<<<grid, kWaBlock, 0, s>>>(a);
   return cudaGetLastError();
 }

@@ -29,14 +29,24 @@ struct IterLog {
   double alpha[2];      // step sizes used by the FISTA step
 };
 
-// Warp task of the WA kernel: a run of whole nets with <= 32 pins in total
-// (x = first pin, y = end pin, z = first net, w = net count <= 32), or one
-// net with more than 32 pins (w = 1).
-using WaTask = int4;
+// Degree classes of the WA kernel over the degree-sorted nets: class j holds
+// the nets of degree (kWaDegHi[j-1], kWaDegHi[j]] (class 0 from degree 2;
+// nets of fewer pins have no gradient) and runs kWaGroup[j] lanes per net,
+// kWaPins[j] pins per lane; the last class (more than 224 pins) runs a warp
+// per net over its pins in three passes.
+constexpr int kWaClasses = 9;
+constexpr int kWaDegHi[kWaClasses] = {2, 4, 8, 16, 32, 64, 128, 224, 0x7fffffff};
+constexpr int kWaGroup[kWaClasses] = {1, 1, 2, 4, 8, 32, 32, 32, 32};
+
+struct WaClass {
+  int first_net;   // index into the degree-sorted CSR
+  int nets;
+  int first_warp;  // warps of the classes before this one
+};
 
 struct WaArgs {
-  const WaTask *tasks;
-  int ntasks;
+  WaClass cls[kWaClasses];
+  int nwarps;
   const uint32_t *net_off;
   const uint32_t *pin_cell;
   const float2 *pos;        // [N + F]: look-ahead positions, then fixed cells
