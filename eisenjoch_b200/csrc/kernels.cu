@@ -402,48 +402,67 @@ __global__ void __launch_bounds__(kFinalBlock) k_density_final(const FinalArgs a
 }
 
 // ---------------------------------------------------------------------------
-// FP32 SIMT GEMM: 64x64 CTA tile, BK = 16, 256 threads with 4x4 outputs,
-// double-buffered shared memory.  Bounds are checked on every load and
-// store, so any M, N, K works; multiples of 64 / 16 take the float4 path.
+// FP32 SIMT GEMM: TM x TN CTA tile (64 x 64 with 256 threads, or 32 x 32 with
+// 64 threads when the large tile leaves SMs idle), BK = 16, 4 x 4 outputs per
+// thread, double-buffered shared memory.  Bounds are checked on every load
+// and store, so any M, N, K works; multiples of 4 take the float4 path.
+// Every output sums k = 0 .. K-1 in order whatever the tile, so both tile
+// sizes give the same bits.
 // ---------------------------------------------------------------------------
-constexpr int GT = 64, GK = 16;
+constexpr int GK = 16;
 
-template <bool SPECTRAL>
-__global__ void __launch_bounds__(256) k_sgemm(const GemmOp *ops, int M, int N, int K,
-                                               SpectralArgs sp) {
+template <bool SPECTRAL, int TM, int TN>
+__global__ void __launch_bounds__((TM / 4) * (TN / 4)) k_sgemm(const GemmOp *ops, int M, int N, int K,
+                                                               SpectralArgs sp) {
+  constexpr int T = (TM / 4) * (TN / 4);
+  constexpr int LA = TM * GK / (4 * T), LB = GK * TN / (4 * T);  // float4 loads per thread
   const GemmOp op = ops[blockIdx.z];
-  __shared__ __align__(16) float As[2][GK][GT + 4];
-  __shared__ __align__(16) float Bs[2][GK][GT + 4];
-  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
-  const int bm = blockIdx.y * GT, bn = blockIdx.x * GT;
+  __shared__ __align__(16) float As[2][GK][TM + 4];
+  __shared__ __align__(16) float Bs[2][GK][TN + 4];
+  const int tid = threadIdx.x, tx = tid % (TN / 4), ty = tid / (TN / 4);
+  const int bm = blockIdx.y * TM, bn = blockIdx.x * TN;
   const bool vec = ((K & 3) == 0) && ((N & 3) == 0);
-  // A tile: 64 rows x 16 k; thread -> row tid/4, k (tid%4)*4..+3
-  const int ar = tid >> 2, ak = (tid & 3) * 4;
-  // B tile: 16 k x 64 cols; thread -> k tid/16, col (tid%16)*4..+3
-  const int bk = tid >> 4, bc = (tid & 15) * 4;
-  float ra[4], rb[4];
+  float ra[LA][4], rb[LB][4];
   auto load = [&](int k0) {
-    const int gr = bm + ar, gk = k0 + ak;
-    if (vec && gr < M && gk + 3 < K) {
-      float4 t = *reinterpret_cast<const float4 *>(op.A + (size_t)gr * K + gk);
-      ra[0] = t.x; ra[1] = t.y; ra[2] = t.z; ra[3] = t.w;
-    } else {
 #pragma unroll
-      for (int j = 0; j < 4; ++j) ra[j] = (gr < M && gk + j < K) ? op.A[(size_t)gr * K + gk + j] : 0.0f;
+    for (int l = 0; l < LA; ++l) {
+      const int f = tid + l * T;
+      const int gr = bm + f / (GK / 4), gk = k0 + (f % (GK / 4)) * 4;
+      if (vec && gr < M && gk + 3 < K) {
+        const float4 t = *reinterpret_cast<const float4 *>(op.A + (size_t)gr * K + gk);
+        ra[l][0] = t.x; ra[l][1] = t.y; ra[l][2] = t.z; ra[l][3] = t.w;
+      } else {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) ra[l][j] = (gr < M && gk + j < K) ? op.A[(size_t)gr * K + gk + j] : 0.0f;
+      }
     }
-    const int gk2 = k0 + bk, gc = bn + bc;
-    if (vec && gk2 < K && gc + 3 < N) {
-      float4 t = *reinterpret_cast<const float4 *>(op.B + (size_t)gk2 * N + gc);
-      rb[0] = t.x; rb[1] = t.y; rb[2] = t.z; rb[3] = t.w;
-    } else {
 #pragma unroll
-      for (int j = 0; j < 4; ++j) rb[j] = (gk2 < K && gc + j < N) ? op.B[(size_t)gk2 * N + gc + j] : 0.0f;
+    for (int l = 0; l < LB; ++l) {
+      const int f = tid + l * T;
+      const int gk = k0 + f / (TN / 4), gc = bn + (f % (TN / 4)) * 4;
+      if (vec && gk < K && gc + 3 < N) {
+        const float4 t = *reinterpret_cast<const float4 *>(op.B + (size_t)gk * N + gc);
+        rb[l][0] = t.x; rb[l][1] = t.y; rb[l][2] = t.z; rb[l][3] = t.w;
+      } else {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) rb[l][j] = (gk < K && gc + j < N) ? op.B[(size_t)gk * N + gc + j] : 0.0f;
+      }
     }
   };
   auto store = [&](int buf) {
 #pragma unroll
-    for (int j = 0; j < 4; ++j) As[buf][ak + j][ar] = ra[j];
-    *reinterpret_cast<float4 *>(&Bs[buf][bk][bc]) = make_float4(rb[0], rb[1], rb[2], rb[3]);
+    for (int l = 0; l < LA; ++l) {
+      const int f = tid + l * T;
+      const int r = f / (GK / 4), k = (f % (GK / 4)) * 4;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) As[buf][k + j][r] = ra[l][j];
+    }
+#pragma unroll
+    for (int l = 0; l < LB; ++l) {
+      const int f = tid + l * T;
+      const int k = f / (TN / 4), c = (f % (TN / 4)) * 4;
+      *reinterpret_cast<float4 *>(&Bs[buf][k][c]) = make_float4(rb[l][0], rb[l][1], rb[l][2], rb[l][3]);
+    }
   };
   float acc[4][4];
 #pragma unroll
@@ -502,6 +521,27 @@ __global__ void __launch_bounds__(256) k_sgemm(const GemmOp *ops, int M, int N, 
       }
     }
   }
+}
+
+// SMs of the current device (cached per device).
+int device_sms() {
+  static int sms[64] = {0};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+  if (!sms[dev]) {
+    int v = 0;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) v = 148;
+    sms[dev] = v;
+  }
+  return sms[dev];
+}
+
+// The small tile when the 64 x 64 grid would leave more than half the SMs
+// without a CTA (measured: 64 CTAs of 512^3 gain from the small tile, 128
+// CTAs do not).
+bool sgemm_small_tile(int M, int N, int nb) {
+  const long ctas = (long)((N + 63) / 64) * ((M + 63) / 64) * nb;
+  return 2L * ctas < device_sms();
 }
 
 // ---------------------------------------------------------------------------
@@ -607,7 +647,67 @@ __device__ __forceinline__ float2 combine(const StepArgs &a, uint32_t i, float2 
                      (float)(((double)gw.y + lam * (double)gd.y) * ipc));
 }
 
-__global__ void __launch_bounds__(kStepBlock) k_step(const StepArgs a) {
+// Phase A of the step for one cell, split into its loads and the rest so
+// that a thread can have the loads of two cells in flight.
+struct CellA {
+  float2 gd, gw;     // density field gather, WA gradient
+  float2 x, xp, gp;  // for the Barzilai-Borwein dots (after the first penalty)
+};
+
+__device__ __forceinline__ CellA load_a(const StepArgs &a, uint32_t i, bool was_init) {
+  CellA c;
+  c.gd = gather_cell(a, i, a.look[i]);
+  c.gw = make_float2((float)from_fix(a.acc[2 * i]), (float)from_fix(a.acc[2 * i + 1]));
+  if (was_init) {
+    c.x = a.x[i];
+    c.xp = a.xp[i];
+    c.gp = a.gprev[i];
+  }
+  return c;
+}
+
+__device__ __forceinline__ void finish_a(const StepArgs &a, uint32_t i, const CellA &c, bool was_init, double lam,
+                                         double (&v)[4]) {
+  a.acc[2 * i] = 0ull;
+  a.acc[2 * i + 1] = 0ull;
+  if (was_init) {
+    const float2 g = combine(a, i, c.gw, c.gd, lam);
+    a.g[i] = g;
+    const double dx = (double)c.x.x - c.xp.x, dy = (double)c.x.y - c.xp.y;
+    v[0] += dx * dx;
+    v[1] += dx * ((double)g.x - c.gp.x);
+    v[2] += dy * dy;
+    v[3] += dy * ((double)g.y - c.gp.y);
+  } else {
+    a.tmp_wl[i] = c.gw;
+    a.tmp_den[i] = c.gd;
+    v[0] += (double)c.gw.x * c.gw.x + (double)c.gw.y * c.gw.y;
+    v[1] += (double)c.gd.x * c.gd.x + (double)c.gd.y * c.gd.y;
+  }
+}
+
+// FISTA step (nesterov.rs:41-64), clamp (:67-72), next look-ahead (:95-101)
+// clamped to the chip (common.rs:410-415), for one cell.
+__device__ __forceinline__ void fista_cell(const StepArgs &a, uint32_t i, float2 x, float2 xp, float2 g, double m,
+                                           double mn, const double (&alpha)[2], double (&nrm)[2]) {
+  const double yx = (double)x.x + m * ((double)x.x - xp.x);
+  const double yy = (double)x.y + m * ((double)x.y - xp.y);
+  const double nx = yx - alpha[0] * g.x, ny = yy - alpha[1] * g.y;
+  nrm[0] += (nx - x.x) * (nx - x.x);
+  nrm[1] += (ny - x.y) * (ny - x.y);
+  const float cx = fminf(fmaxf((float)nx, 0.0f), a.maxx);
+  const float cy = fminf(fmaxf((float)ny, 0.0f), a.maxy);
+  const float px = fminf(fmaxf(x.x, 0.0f), a.maxx);
+  const float py = fminf(fmaxf(x.y, 0.0f), a.maxy);
+  a.x[i] = make_float2(cx, cy);
+  a.xp[i] = make_float2(px, py);
+  a.gprev[i] = g;
+  const double lx = (double)cx + mn * ((double)cx - px);
+  const double ly = (double)cy + mn * ((double)cy - py);
+  a.look[i] = make_float2(fminf(fmaxf((float)lx, 0.0f), a.maxx), fminf(fmaxf((float)ly, 0.0f), a.maxy));
+}
+
+__global__ void __launch_bounds__(kStepBlock, 2) k_step(const StepArgs a) {
   __shared__ double sm[32 * 4];
   __shared__ bool last;
   const uint32_t tid0 = blockIdx.x * blockDim.x + threadIdx.x;
@@ -633,28 +733,17 @@ __global__ void __launch_bounds__(kStepBlock) k_step(const StepArgs a) {
   const bool coop = a.mode == 0;
   double v[4] = {0.0, 0.0, 0.0, 0.0};
   if (a.mode == 0 || a.mode == 2) {
-    // Phase A: gather, read + clear the WA accumulator, combine.
-    for (uint32_t i = tid0; i < a.N; i += gstride) {
-      const float2 p = a.look[i];
-      const float2 gd = gather_cell(a, i, p);
-      const float2 gw = make_float2((float)from_fix(a.acc[2 * i]), (float)from_fix(a.acc[2 * i + 1]));
-      a.acc[2 * i] = 0ull;
-      a.acc[2 * i + 1] = 0ull;
-      if (was_init) {
-        const float2 g = combine(a, i, gw, gd, lam);
-        a.g[i] = g;
-        const float2 x = a.x[i], xp = a.xp[i], gp = a.gprev[i];
-        const double dx = (double)x.x - xp.x, dy = (double)x.y - xp.y;
-        v[0] += dx * dx;
-        v[1] += dx * ((double)g.x - gp.x);
-        v[2] += dy * dy;
-        v[3] += dy * ((double)g.y - gp.y);
-      } else {
-        a.tmp_wl[i] = gw;
-        a.tmp_den[i] = gd;
-        v[0] += (double)gw.x * gw.x + (double)gw.y * gw.y;
-        v[1] += (double)gd.x * gd.x + (double)gd.y * gd.y;
-      }
+    // Phase A: gather, read + clear the WA accumulator, combine.  Two cells
+    // per thread and pass (i and i + gstride): every load of both is issued
+    // before the first store, so their latencies overlap; partial sums run
+    // in the same cell order as a one-cell loop.
+    for (uint32_t i0 = tid0; i0 < a.N; i0 += 2 * gstride) {
+      const uint32_t i1 = i0 + gstride;
+      const bool h1 = i1 < a.N;
+      CellA c0 = load_a(a, i0, was_init);
+      CellA c1 = h1 ? load_a(a, i1, was_init) : c0;
+      finish_a(a, i0, c0, was_init, lam, v);
+      if (h1) finish_a(a, i1, c1, was_init, lam, v);
     }
     block_sum<4>(v, sm);
     if (threadIdx.x == 0)
@@ -714,23 +803,18 @@ __global__ void __launch_bounds__(kStepBlock) k_step(const StepArgs a) {
   // (:95-101) clamped to the chip (common.rs:410-415).
   const double m = a.mom[it], mn = a.mom[it + 1];
   double nrm[2] = {0.0, 0.0};
-  for (uint32_t i = tid0; i < a.N; i += gstride) {
-    const float2 x = a.x[i], xp = a.xp[i], g = a.g[i];
-    const double yx = (double)x.x + m * ((double)x.x - xp.x);
-    const double yy = (double)x.y + m * ((double)x.y - xp.y);
-    const double nx = yx - alpha[0] * g.x, ny = yy - alpha[1] * g.y;
-    nrm[0] += (nx - x.x) * (nx - x.x);
-    nrm[1] += (ny - x.y) * (ny - x.y);
-    const float cx = fminf(fmaxf((float)nx, 0.0f), a.maxx);
-    const float cy = fminf(fmaxf((float)ny, 0.0f), a.maxy);
-    const float px = fminf(fmaxf(x.x, 0.0f), a.maxx);
-    const float py = fminf(fmaxf(x.y, 0.0f), a.maxy);
-    a.x[i] = make_float2(cx, cy);
-    a.xp[i] = make_float2(px, py);
-    a.gprev[i] = g;
-    const double lx = (double)cx + mn * ((double)cx - px);
-    const double ly = (double)cy + mn * ((double)cy - py);
-    a.look[i] = make_float2(fminf(fmaxf((float)lx, 0.0f), a.maxx), fminf(fmaxf((float)ly, 0.0f), a.maxy));
+  for (uint32_t i0 = tid0; i0 < a.N; i0 += 2 * gstride) {  // two cells per pass, loads first
+    const uint32_t i1 = i0 + gstride;
+    const bool h1 = i1 < a.N;
+    const float2 x0 = a.x[i0], xp0 = a.xp[i0], g0 = a.g[i0];
+    float2 x1 = x0, xp1 = xp0, g1 = g0;
+    if (h1) {
+      x1 = a.x[i1];
+      xp1 = a.xp[i1];
+      g1 = a.g[i1];
+    }
+    fista_cell(a, i0, x0, xp0, g0, m, mn, alpha, nrm);
+    if (h1) fista_cell(a, i1, x1, xp1, g1, m, mn, alpha, nrm);
   }
   double w2[2] = {nrm[0], nrm[1]};
   block_sum<2>(w2, sm);
@@ -805,15 +889,21 @@ cudaError_t launch_density_final(const FinalArgs &a, int grid, cudaStream_t s) {
 }
 
 cudaError_t launch_sgemm(const GemmOp *ops, int nb, int M, int N, int K, cudaStream_t s) {
-  dim3 grid((N + GT - 1) / GT, (M + GT - 1) / GT, nb);
-  k_sgemm<false><<<grid, 256, 0, s>>>(ops, M, N, K, SpectralArgs{});
+  if (sgemm_small_tile(M, N, nb)) {
+    k_sgemm<false, 32, 32><<<dim3((N + 31) / 32, (M + 31) / 32, nb), 64, 0, s>>>(ops, M, N, K, SpectralArgs{});
+  } else {
+    k_sgemm<false, 64, 64><<<dim3((N + 63) / 64, (M + 63) / 64, nb), 256, 0, s>>>(ops, M, N, K, SpectralArgs{});
+  }
   return cudaGetLastError();
 }
 
 cudaError_t launch_sgemm_spectral(const GemmOp *ops, int M, int N, int K, const SpectralArgs &sp,
                                   cudaStream_t s) {
-  dim3 grid((N + GT - 1) / GT, (M + GT - 1) / GT, 1);
-  k_sgemm<true><<<grid, 256, 0, s>>>(ops, M, N, K, sp);
+  if (sgemm_small_tile(M, N, 1)) {
+    k_sgemm<true, 32, 32><<<dim3((N + 31) / 32, (M + 31) / 32, 1), 64, 0, s>>>(ops, M, N, K, sp);
+  } else {
+    k_sgemm<true, 64, 64><<<dim3((N + 63) / 64, (M + 63) / 64, 1), 256, 0, s>>>(ops, M, N, K, sp);
+  }
   return cudaGetLastError();
 }
 
