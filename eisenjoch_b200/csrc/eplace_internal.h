@@ -75,6 +75,7 @@ struct Legalizer {
   const HostProblem &hp_;
   const LegalBase &base_;
   std::vector<uint64_t> free_, sum_;
+  std::vector<int32_t> lc_, rc_;  // per-row candidate cache of the unit-cell search
 };
 
 // total_hpwl (metrics/wirelength.rs:10-51) on the host.

@@ -195,6 +195,8 @@ LegalBase::LegalBase(const HostProblem &hp) : W(hp.W), H(hp.H) {
 Legalizer::Legalizer(const HostProblem &hp, const LegalBase &base) : hp_(hp), base_(base) {
   free_.resize(base.free0.size());
   sum_.resize(base.sum0.size());
+  lc_.resize(std::max(base.H, 0));
+  rc_.resize(std::max(base.H, 0));
 }
 
 namespace {
@@ -271,6 +273,8 @@ eplace_status Legalizer::run(const float *x, const float *y, size_t stride, int3
   std::copy(base_.sum0.begin(), base_.sum0.end(), sum_.begin());
   uint64_t *fm = free_.data();
   uint64_t *sm = sum_.empty() ? nullptr : sum_.data();
+  std::fill(lc_.begin(), lc_.end(), INT32_MAX);  // every row's cache entry dead
+  int32_t *lc = lc_.data(), *rc = rc_.data();
   double total = 0.0;
   for (uint32_t i : base_.order) {
     const double tx = (double)x[i * stride], ty = (double)y[i * stride];
@@ -294,13 +298,31 @@ eplace_status Legalizer::run(const float *x, const float *y, size_t stride, int3
         int32_t cy = (int32_t)std::floor(ty + 0.5);
         cy = std::min(std::max(cy, 0), H - 1);
         const int32_t fx0 = (int32_t)std::floor(tx);
+        // Per-row candidate cache: (lc, rc) are the nearest free sites left
+        // of / right of an earlier query position in this row, with every
+        // site strictly between them taken.  For any fx0 with
+        // lc <= fx0 < rc they are again this query's two candidates, so a
+        // cell of a crowded region (whose neighbours in the order target the
+        // same region) reads them instead of searching the bitmap.  A row's
+        // entry dies when one of its two sites is taken.
+        const bool cacheable = fx0 >= 0 && fx0 <= W - 1;
         auto scan_row = [&](int32_t row) {
-          const uint64_t *r = fm + (size_t)row * WR;
-          const uint64_t *rs = sm ? sm + row : nullptr;
           const double dy = (double)row - ty;
           const double dy2 = dy * dy;
-          const int32_t l = free_at_or_left(r, rs, std::min(fx0, W - 1));
-          const int32_t rr = free_at_or_right(r, rs, fx0 + 1, W, WR);
+          int32_t l, rr;
+          if (cacheable && lc[row] <= fx0 && fx0 < rc[row]) {
+            l = lc[row];
+            rr = rc[row] < W ? rc[row] : -1;
+          } else {
+            const uint64_t *r = fm + (size_t)row * WR;
+            const uint64_t *rs = sm ? sm + row : nullptr;
+            l = free_at_or_left(r, rs, std::min(fx0, W - 1));
+            rr = free_at_or_right(r, rs, fx0 + 1, W, WR);
+            if (cacheable) {
+              lc[row] = l;
+              rc[row] = rr >= 0 ? rr : W;
+            }
+          }
           if (l >= 0) {
             const double dx = (double)l - tx, cost = dx * dx + dy2;
             const int64_t t = (int64_t)row * W + l;
@@ -439,6 +461,7 @@ eplace_status Legalizer::run(const float *x, const float *y, size_t stride, int3
         uint64_t &word = fm[(size_t)(by + dy) * WR + (xx >> 6)];
         word &= ~(1ull << (xx & 63));
         if (sm && !word) sm[by + dy] &= ~(1ull << (xx >> 6));
+        if (xx == lc[by + dy] || xx == rc[by + dy]) lc[by + dy] = INT32_MAX;
       }
     site_x[i] = bx;
     site_y[i] = by;
