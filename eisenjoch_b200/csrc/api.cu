@@ -335,6 +335,7 @@ struct eplace_ctx {
   uint64_t load_gen = 0;         // bumped by every (re)load of a problem
   WaClass wa_cls[kWaClasses] = {};  // degree classes of the sorted CSR
   int wa_warps = 0;
+  int grad_k = 24;  // fixed-point scale 2^k of the packed WA gradient (pack_grad)
 
   // Device memory this context holds (allocated capacities).
   uint64_t device_bytes() const;
@@ -382,6 +383,19 @@ void degree_sorted_csr(const HostProblem &hp, std::vector<uint32_t> &off, std::v
     for (uint32_t q = hp.net_off[n]; q < hp.net_off[n + 1]; ++q) pins[k++] = hp.pin_cell[q];
     off[i + 1] = k;
   }
+}
+
+// Fixed-point exponent k of the packed WA gradient: every cell's x and y
+// sums must stay below 2^31 in magnitude.  With at most D pins on one cell
+// and a bound of 4 per pin, 4 D 2^k < 2^31; k is at most 24.
+int grad_scale_log2(const HostProblem &hp) {
+  std::vector<uint32_t> pins(hp.N, 0);
+  uint32_t d = 1;
+  for (uint32_t q = 0; q < hp.P; ++q)
+    if (hp.pin_cell[q] < hp.N) d = std::max(d, ++pins[hp.pin_cell[q]]);
+  int k = 24;
+  while (k > 0 && 4.0 * (double)d * std::ldexp(1.0, k) >= 2147483648.0) --k;
+  return k;
 }
 
 // Splits the degree-sorted nets into the WA kernel's degree classes and
@@ -531,6 +545,7 @@ void launch_wa_stage(eplace_ctx *c, float gamma) {
   a.acc = c->acc.p;
   a.N = c->hp.N;
   a.gamma = gamma;
+  a.grad_scale = (float)std::ldexp(1.0, c->grad_k);
   CK(launch_wa(a, grid_for(c->wa_warps * 32, kWaBlock, c->num_sms * 16), c->stream));
 }
 
@@ -769,6 +784,7 @@ StepArgs step_args(eplace_ctx *c) {
   a.area = hp.any_macro ? c->area.p : nullptr;
   a.pw = c->pw.p;
   a.acc = c->acc.p;
+  a.grad_inv = std::ldexp(1.0, -c->grad_k);
   a.Ex = c->Ex.p;
   a.Ey = c->Ey.p;
   a.x = c->x.p;
@@ -975,8 +991,9 @@ void load_into(eplace_ctx *c, HostProblem &&hp_in) {
   if (hp.F) CK(cudaMemcpyAsync(c->look.p + hp.N, fixed.data(), sizeof(float2) * hp.F, cudaMemcpyHostToDevice, s));
   g_h2d += sizeof(float2) * hp.F;
   for (auto *b : {&c->x, &c->xp, &c->g, &c->gprev, &c->tmp_wl, &c->tmp_den}) b->ensure(N1);
-  c->acc.ensure(2 * N1);
+  c->acc.ensure(N1);
   c->acc.zero(s);
+  c->grad_k = grad_scale_log2(hp);
   const size_t nb = (size_t)hp.BX * hp.BY;
   c->dens.ensure(nb);
   c->dens.zero(s);
@@ -2061,14 +2078,18 @@ eplace_status eplace_stage_wa_grad(eplace_ctx *c, double wl_coeff, const float *
     upload_look(c, x, y);
     c->acc.zero(c->stream);
     launch_wa_stage(c, (float)wl_coeff);
-    std::vector<long long> acc(2 * (size_t)c->hp.N);
+    std::vector<unsigned long long> acc((size_t)c->hp.N);
     if (c->hp.N)
-      CK(cudaMemcpyAsync(acc.data(), c->acc.p, sizeof(long long) * acc.size(), cudaMemcpyDeviceToHost, c->stream));
+      CK(cudaMemcpyAsync(acc.data(), c->acc.p, sizeof(unsigned long long) * acc.size(), cudaMemcpyDeviceToHost,
+                         c->stream));
     c->acc.zero(c->stream);
     CK(cudaStreamSynchronize(c->stream));
+    const double inv = std::ldexp(1.0, -c->grad_k);
     for (uint32_t i = 0; i < c->hp.N; ++i) {
-      gx[i] = (float)((double)acc[2 * i] * kFixInv);
-      gy[i] = (float)((double)acc[2 * i + 1] * kFixInv);
+      long long sx, sy;
+      unpack_grad(acc[i], &sx, &sy);
+      gx[i] = (float)((double)sx * inv);
+      gy[i] = (float)((double)sy * inv);
     }
   } catch (const CudaError &e) {
     return cuda_fail(c, e);
@@ -2211,12 +2232,12 @@ eplace_status eplace_stage_step(eplace_ctx *c, uint64_t iter, const float *look_
     upload_look(c, look_x, look_y);
     c->Ex.upload(ex, nb, s);
     c->Ey.upload(ey, nb, s);
-    std::vector<long long> acc(2 * (size_t)N);
-    for (uint32_t i = 0; i < N; ++i) {
-      acc[2 * i] = llrint((double)gwl_x[i] * kFixScale);
-      acc[2 * i + 1] = llrint((double)gwl_y[i] * kFixScale);
-    }
-    if (N) CK(cudaMemcpyAsync(c->acc.p, acc.data(), sizeof(long long) * acc.size(), cudaMemcpyHostToDevice, s));
+    std::vector<unsigned long long> acc((size_t)N);
+    const double scale = std::ldexp(1.0, c->grad_k);
+    for (uint32_t i = 0; i < N; ++i)
+      acc[i] = pack_grad(llrint((double)gwl_x[i] * scale), llrint((double)gwl_y[i] * scale));
+    if (N)
+      CK(cudaMemcpyAsync(c->acc.p, acc.data(), sizeof(unsigned long long) * acc.size(), cudaMemcpyHostToDevice, s));
     std::vector<float2> vx = pack2(x, y, N), vxp = pack2(x_prev, y_prev, N), vg = pack2(gprev_x, gprev_y, N);
     c->x.upload(vx.data(), N, s);
     c->xp.upload(vxp.data(), N, s);

@@ -241,8 +241,7 @@ __device__ __forceinline__ void wa_group(const WaArgs &a, const WaClass &cl, int
     }
     const float gx = wa_pin_grad(ux, vx, epx, emx, ipx, s[1], imx, s[3], a.gamma);
     const float gy = wa_pin_grad(uy, vy, epy, emy, ipy, s[5], imy, s[7], a.gamma);
-    atomicAdd(&a.acc[2 * c], to_fix(gx));
-    atomicAdd(&a.acc[2 * c + 1], to_fix(gy));
+    atomicAdd(&a.acc[c], pack_grad(__float2ll_rn(gx * a.grad_scale), __float2ll_rn(gy * a.grad_scale)));
   }
 }
 
@@ -280,8 +279,7 @@ __device__ void wa_big_net(const WaArgs &a, int pb, int pe, int lane) {
     const float ux = p.x - mx, vx = p.x - mn, uy = p.y - my, vy = p.y - ny;
     const float gx = wa_pin_grad(ux, vx, ex2(kg * ux), ex2(-kg * vx), ipx, s[1], imx, s[3], a.gamma);
     const float gy = wa_pin_grad(uy, vy, ex2(kg * uy), ex2(-kg * vy), ipy, s[5], imy, s[7], a.gamma);
-    atomicAdd(&a.acc[2 * c], to_fix(gx));
-    atomicAdd(&a.acc[2 * c + 1], to_fix(gy));
+    atomicAdd(&a.acc[c], pack_grad(__float2ll_rn(gx * a.grad_scale), __float2ll_rn(gy * a.grad_scale)));
   }
 }
 
@@ -657,7 +655,9 @@ struct CellA {
 __device__ __forceinline__ CellA load_a(const StepArgs &a, uint32_t i, bool was_init) {
   CellA c;
   c.gd = gather_cell(a, i, a.look[i]);
-  c.gw = make_float2((float)from_fix(a.acc[2 * i]), (float)from_fix(a.acc[2 * i + 1]));
+  long long sx, sy;
+  unpack_grad(a.acc[i], &sx, &sy);
+  c.gw = make_float2((float)((double)sx * a.grad_inv), (float)((double)sy * a.grad_inv));
   if (was_init) {
     c.x = a.x[i];
     c.xp = a.xp[i];
@@ -668,8 +668,7 @@ __device__ __forceinline__ CellA load_a(const StepArgs &a, uint32_t i, bool was_
 
 __device__ __forceinline__ void finish_a(const StepArgs &a, uint32_t i, const CellA &c, bool was_init, double lam,
                                          double (&v)[4]) {
-  a.acc[2 * i] = 0ull;
-  a.acc[2 * i + 1] = 0ull;
+  a.acc[i] = 0ull;
   if (was_init) {
     const float2 g = combine(a, i, c.gw, c.gd, lam);
     a.g[i] = g;

@@ -38,6 +38,22 @@ constexpr int kWaClasses = 9;
 constexpr int kWaDegHi[kWaClasses] = {2, 4, 8, 16, 32, 64, 128, 224, 0x7fffffff};
 constexpr int kWaGroup[kWaClasses] = {1, 1, 2, 4, 8, 32, 32, 32, 32};
 
+// The WA gradient of a cell is accumulated as one 64-bit integer per cell:
+// x and y in fixed point (scale 2^k), packed as gx + 2^32 gy and summed with
+// one 64-bit atomic per pin.  Two's-complement sums are exact modulo 2^64,
+// so while |sum gx| and |sum gy| stay below 2^31 the low word is the x sum
+// and the rest the y sum.  k is chosen per problem from the largest pin
+// count of a cell (a pin's gradient is below 2 in magnitude; the bound used
+// is 4 per pin), at most 24.
+__host__ __device__ inline unsigned long long pack_grad(long long gx, long long gy) {
+  return (unsigned long long)gx + ((unsigned long long)gy << 32);
+}
+__host__ __device__ inline void unpack_grad(unsigned long long v, long long *gx, long long *gy) {
+  const int lo = (int)(unsigned)(v & 0xffffffffull);
+  *gx = lo;
+  *gy = (long long)(v - (unsigned long long)(long long)lo) >> 32;
+}
+
 struct WaClass {
   int first_net;   // index into the degree-sorted CSR
   int nets;
@@ -50,9 +66,10 @@ struct WaArgs {
   const uint32_t *net_off;
   const uint32_t *pin_cell;
   const float2 *pos;        // [N + F]: look-ahead positions, then fixed cells
-  unsigned long long *acc;  // [2N] fixed-point gradient (x, y interleaved)
+  unsigned long long *acc;  // [N] packed fixed-point gradient (see pack_grad)
   uint32_t N;
   float gamma;
+  float grad_scale;         // 2^k fixed-point scale of the packed gradient
 };
 
 struct ScatterArgs {
@@ -102,7 +119,8 @@ struct StepArgs {
   const float2 *half;       // nullptr => unit cells
   const float *area;
   const float *pw;
-  unsigned long long *acc;  // WA accumulator, read then zeroed
+  unsigned long long *acc;  // [N] packed WA accumulator, read then zeroed
+  double grad_inv;          // 1 / WaArgs::grad_scale
   const float *Ex, *Ey;
   float2 *x, *xp, *g, *gprev;
   float2 *tmp_wl, *tmp_den; // [N] scratch for the penalty-initialisation phase
