@@ -700,7 +700,7 @@ void launch_final_stage(eplace_ctx *c, double *dens_out, bool tc = false) {
   const double c0 = c->total_area / (double)nb;
   FinalArgs a{c->dens.p, nb, (double)hp.sx * hp.sy, c0, tc ? nullptr : c->rho.p, tc ? c->rho_h.p : nullptr,
               tc ? c->rho_l.p : nullptr, dens_out, c->part.p, c->bar.p + 2, c->sc.p, c->log.p};
-  CK(launch_density_final(a, grid_for(nb, kFinalBlock, c->num_sms * 4), c->stream));
+  CK(launch_density_final(a, grid_for((nb + 3) / 4, kFinalBlock, c->num_sms * 4), c->stream));
 }
 
 // One of the four GEMM launches of a field solve (density.rs:96-166):

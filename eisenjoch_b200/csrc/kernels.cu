@@ -364,7 +364,46 @@ __global__ void __launch_bounds__(kFinalBlock) k_density_final(const FinalArgs a
   __shared__ double sm[64];
   __shared__ bool last;
   double v[2] = {0.0, 0.0};
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.nb; i += gridDim.x * blockDim.x) {
+  // Groups of four consecutive bins per thread and step: 16-byte loads and
+  // stores (the bin count of every supported grid is a multiple of 4; a
+  // ragged tail takes the scalar loop below).
+  const int ng = a.nb >> 2;
+  const int t0 = blockIdx.x * blockDim.x + threadIdx.x, ts = gridDim.x * blockDim.x;
+  for (int gi = t0; gi < ng; gi += ts) {
+    ulonglong2 *dp = reinterpret_cast<ulonglong2 *>(a.dens) + 2 * gi;
+    const ulonglong2 q0 = dp[0], q1 = dp[1];
+    dp[0] = make_ulonglong2(0ull, 0ull);
+    dp[1] = make_ulonglong2(0ull, 0ull);
+    const double d[4] = {from_fix(q0.x), from_fix(q0.y), from_fix(q1.x), from_fix(q1.y)};
+    float r[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      r[k] = (float)(d[k] - a.c0);
+      v[0] += d[k];
+      v[1] += fmax(d[k] - a.cap, 0.0);
+    }
+    if (a.rho) reinterpret_cast<float4 *>(a.rho)[gi] = make_float4(r[0], r[1], r[2], r[3]);
+    if (a.rho_hi) {
+      __nv_bfloat16 h[4], l[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        h[k] = __float2bfloat16_rn(r[k]);
+        l[k] = __float2bfloat16_rn(r[k] - __bfloat162float(h[k]));
+      }
+      uint2 hv, lv;
+      hv.x = (uint32_t)__bfloat16_as_ushort(h[0]) | ((uint32_t)__bfloat16_as_ushort(h[1]) << 16);
+      hv.y = (uint32_t)__bfloat16_as_ushort(h[2]) | ((uint32_t)__bfloat16_as_ushort(h[3]) << 16);
+      lv.x = (uint32_t)__bfloat16_as_ushort(l[0]) | ((uint32_t)__bfloat16_as_ushort(l[1]) << 16);
+      lv.y = (uint32_t)__bfloat16_as_ushort(l[2]) | ((uint32_t)__bfloat16_as_ushort(l[3]) << 16);
+      reinterpret_cast<uint2 *>(a.rho_hi)[gi] = hv;
+      reinterpret_cast<uint2 *>(a.rho_lo)[gi] = lv;
+    }
+    if (a.dens_out) {
+      reinterpret_cast<double2 *>(a.dens_out)[2 * gi] = make_double2(d[0], d[1]);
+      reinterpret_cast<double2 *>(a.dens_out)[2 * gi + 1] = make_double2(d[2], d[3]);
+    }
+  }
+  for (int i = 4 * ng + t0; i < a.nb; i += ts) {
     const double d = from_fix(a.dens[i]);
     a.dens[i] = 0ull;
     const float r = (float)(d - a.c0);
@@ -677,12 +716,12 @@ __device__ __forceinline__ void finish_a(const StepArgs &a, uint32_t i, const Ce
     v[1] += dx * ((double)g.x - c.gp.x);
     v[2] += dy * dy;
     v[3] += dy * ((double)g.y - c.gp.y);
-  } else {
-    a.tmp_wl[i] = c.gw;
-    a.tmp_den[i] = c.gd;
-    v[0] += (double)c.gw.x * c.gw.x + (double)c.gw.y * c.gw.y;
-    v[1] += (double)c.gd.x * c.gd.x + (double)c.gd.y * c.gd.y;
+    return;
   }
+  a.tmp_wl[i] = c.gw;
+  a.tmp_den[i] = c.gd;
+  v[0] += (double)c.gw.x * c.gw.x + (double)c.gw.y * c.gw.y;
+  v[1] += (double)c.gd.x * c.gd.x + (double)c.gd.y * c.gd.y;
 }
 
 // FISTA step (nesterov.rs:41-64), clamp (:67-72), next look-ahead (:95-101)
