@@ -2030,20 +2030,60 @@ eplace_status eplace_profile_stages(eplace_ctx *c, const eplace_cfg *cfg, const 
     const float gamma = (float)cfg->wl_coeff;
     double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     cudaStream_t s = c->stream;
-    for (uint32_t r = 0; r < reps; ++r) {
-      CK(cudaEventRecord(ev[0], s));
+    bool capturing = false;
+    // Inside a capture the records become event-record nodes of the graph
+    // (cudaEventRecordExternal), which the host can wait on and time.
+    auto rec = [&](cudaEvent_t e) {
+      CK(capturing ? cudaEventRecordWithFlags(e, s, cudaEventRecordExternal) : cudaEventRecord(e, s));
+    };
+    auto one_iteration = [&]() {
+      rec(ev[0]);
       launch_wa_stage(c, gamma);
-      CK(cudaEventRecord(ev[1], s));
+      rec(ev[1]);
       launch_scatter_stage(c);
-      CK(cudaEventRecord(ev[2], s));
+      rec(ev[2]);
       launch_final_stage(c, nullptr, tc);
-      CK(cudaEventRecord(ev[3], s));
+      rec(ev[3]);
       for (int g = 0; g < 4; ++g) {
         launch_field_gemm(c, g, nullptr, opts.field_mode, tc);
-        CK(cudaEventRecord(ev[4 + g], s));
+        rec(ev[4 + g]);
       }
       launch_step_stage(c);
-      CK(cudaEventRecord(ev[8], s));
+      rec(ev[8]);
+    };
+    // The iteration is timed as a CUDA graph (event-record nodes between the
+    // kernel nodes), as the loop replays it, so host launch latency is not
+    // counted; plain launches if capture is not available.
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+      bool ok = true;
+      capturing = true;
+      try {
+        one_iteration();
+      } catch (const CudaError &) {
+        ok = false;
+      }
+      capturing = false;
+      if (cudaStreamEndCapture(s, &graph) != cudaSuccess || !ok ||
+          cudaGraphInstantiate(&gexec, graph, 0) != cudaSuccess) {
+        cudaGetLastError();
+        gexec = nullptr;
+      }
+      if (graph) cudaGraphDestroy(graph);
+    } else {
+      cudaGetLastError();
+    }
+    for (uint32_t r = 0; r < reps; ++r) {
+      if (gexec) {
+        const cudaError_t le = cudaGraphLaunch(gexec, s);
+        if (le != cudaSuccess) {
+          cudaGraphExecDestroy(gexec);
+          throw CudaError{le, "cudaGraphLaunch (profile)"};
+        }
+      } else {
+        one_iteration();
+      }
       CK(cudaEventSynchronize(ev[8]));
       for (int k = 0; k < 8; ++k) {
         float ms = 0.f;
@@ -2051,6 +2091,7 @@ eplace_status eplace_profile_stages(eplace_ctx *c, const eplace_cfg *cfg, const 
         acc[k] += ms;
       }
     }
+    if (gexec) cudaGraphExecDestroy(gexec);
     for (int k = 0; k < 8; ++k) stage_ms[k] = acc[k] / reps;
   } catch (const CudaError &e) {
     st = cuda_fail(c, e);

@@ -252,7 +252,9 @@ eplace_status eplace_stage_hpwl(eplace_ctx *ctx, const int32_t *site_x,
 
 /* Device time of each kernel of the iteration, measured with CUDA events on
  * the context's stream over `reps` real iterations started from the initial
- * placement of cfg.  stage_ms[8] = {WA gradient, density scatter, density
+ * placement of cfg.  The iteration (kernels with event records between them)
+ * is replayed as one CUDA graph, as the placement loop runs it, so host
+ * launch latency is not counted.  stage_ms[8] = {WA gradient, density scatter, density
  * finalise, DCT GEMM 1, DCT GEMM 2 + spectral, DCT GEMM 3 (x2), DCT GEMM 4
  * (x2), fused gather/step}, mean milliseconds per launch. */
 eplace_status eplace_profile_stages(eplace_ctx *ctx, const eplace_cfg *cfg, const eplace_opts *opts,
