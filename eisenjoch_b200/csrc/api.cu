@@ -258,6 +258,10 @@ struct eplace_ctx {
   HostProblem hp;
   int device = 0;
   cudaStream_t stream = nullptr;
+  // Second stream of the iteration: the WA kernel runs on it beside the
+  // density -> transform chain (fork / join events, captured into the graph).
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   std::string err;
   int num_sms = 0;
   int step_grid = 0;
@@ -348,6 +352,10 @@ struct eplace_ctx {
     pool.reset();
     if (gexec) cudaGraphExecDestroy(gexec);
     for (auto e : slot_ev) cudaEventDestroy(e);
+    if (side) cudaStreamSynchronize(side);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
+    if (side) cudaStreamDestroy(side);
     if (stream) cudaStreamDestroy(stream);
   }
 };
@@ -535,7 +543,7 @@ int grid_for(int n, int block, int cap) {
 }
 
 // --- kernel sequence of one iteration ------------------------------------
-void launch_wa_stage(eplace_ctx *c, float gamma) {
+void launch_wa_stage(eplace_ctx *c, float gamma, cudaStream_t st = nullptr) {
   WaArgs a{};
   std::copy(c->wa_cls, c->wa_cls + kWaClasses, a.cls);
   a.nwarps = c->wa_warps;
@@ -546,7 +554,7 @@ void launch_wa_stage(eplace_ctx *c, float gamma) {
   a.N = c->hp.N;
   a.gamma = gamma;
   a.grad_scale = (float)std::ldexp(1.0, c->grad_k);
-  CK(launch_wa(a, grid_for(c->wa_warps * 32, kWaBlock, c->num_sms * 16), c->stream));
+  CK(launch_wa(a, grid_for(c->wa_warps * 32, kWaBlock, c->num_sms * 16), st ? st : c->stream));
 }
 
 void launch_scatter_stage(eplace_ctx *c) {
@@ -811,11 +819,19 @@ void launch_step_stage(eplace_ctx *c) {
   else CK(launch_step(a, c->step_grid, c->stream));
 }
 
+// One iteration.  The WA gradient and the density -> field chain both read
+// only the look-ahead positions and write separate buffers, so WA runs on
+// the side stream beside scatter / finalise / the four GEMMs; the step joins
+// both.  (In a captured graph this is a fork and a join.)
 void launch_iteration(eplace_ctx *c, float gamma, int field_mode, bool tc) {
-  launch_wa_stage(c, gamma);
+  CK(cudaEventRecord(c->ev_fork, c->stream));
+  CK(cudaStreamWaitEvent(c->side, c->ev_fork, 0));
+  launch_wa_stage(c, gamma, c->side);
+  CK(cudaEventRecord(c->ev_join, c->side));
   launch_scatter_stage(c);
   launch_final_stage(c, nullptr, tc);
   launch_field_stage(c, nullptr, field_mode, tc);
+  CK(cudaStreamWaitEvent(c->stream, c->ev_join, 0));
   launch_step_stage(c);
 }
 
@@ -1890,6 +1906,9 @@ eplace_ctx *ctx_new(int32_t device, eplace_status *st) {
     int prio_lo = 0, prio_hi = 0;
     CK(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
     CK(cudaStreamCreateWithPriority(&c->stream, cudaStreamNonBlocking, prio_hi));
+    CK(cudaStreamCreateWithPriority(&c->side, cudaStreamNonBlocking, prio_hi));
+    CK(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming));
     CK(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device));
     c->sc.alloc(1);
     c->bar.alloc(4);
