@@ -59,6 +59,8 @@ def parse():
                     help="reference: the reference's field formula (default, parity); potential_gradient: the "
                          "opt-in extension that spreads cells")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched (64 mixed-size jobs) arm")
+    ap.add_argument("--no-precision-form", action="store_true",
+                    help="skip the per-kernel roofline of the 800k precision form (BF16x3 transform)")
     ap.add_argument("--no-served", action="store_true", help="skip the served (Poisson stream) arm")
     ap.add_argument("--batched-jobs", type=int, default=64)
     ap.add_argument("--served-jobs", type=int, default=200,
@@ -206,6 +208,31 @@ def algorithmic(nl, chip):
         "dct_gemm4": ("flops", 2 * 2 * H * W * H),
         "gather_step": ("hbm", 68 * N + 8 * W * H),
     }
+
+
+def precision_form_roofline(E, args, hbm, bf16, workload="electro_800k_2048"):
+    """Per-kernel CUDA-event times (one graph-replayed iteration) and their
+    fractions of the measured peaks on the 800k-cell precision form."""
+    w = E.WORKLOADS[workload]
+    nl, chip = E.synth_netlist(w["spec"])
+    cfg = E.ElectroPlaceCfg(**w["cfg"])
+    opts = E.RunOptions(field_mode=1, dct_mode=1)
+    with E.PlacementContext(nl, chip) as ctx:
+        ms = ctx.profile_stages(cfg, reps=args.profile_reps, opts=opts)
+    algo = algorithmic(nl, chip)
+    out = {"workload": workload, "dct": "bf16x3 tcgen05", "peak_source": "measured (MEASURED_PEAKS.json)",
+           "stages": {}}
+    for k, t in ms.items():
+        kd, am = algo[k]
+        d = {"ms": t}
+        if kd == "hbm":
+            d.update({"algorithmic_bytes": am, "GB/s": am / (t / 1e3) / 1e9, "frac_hbm": am / (t / 1e3) / 1e9 / hbm,
+                      "traffic": ncu_traffic(k, workload)})
+        else:
+            d.update({"algorithmic_flops": am, "TFLOP/s": am / (t / 1e3) / 1e12,
+                      "frac_bf16": am / (t / 1e3) / 1e12 / bf16})
+        out["stages"][k] = d
+    return out
 
 
 def ncu_traffic(kernel, workload):
@@ -532,6 +559,12 @@ def ours(args, dist):
     e2e_value = jobs / e2e_s
     ctx.close()
 
+    # --- per-kernel roofline of the precision form (800k cells, 1024^2 bins,
+    # BF16x3 transform): the configuration whose bytes exceed L2 ---
+    prec = None
+    if not args.no_precision_form and dist.rank == 0:
+        prec = precision_form_roofline(E, args, hbm, bf16)
+
     mixed_cfg = E.ElectroPlaceCfg(max_iters=500)
     batched = None if args.no_batched else batched_arm(args, dist, E, mixed_cfg)
     served = None if args.no_served else served_arm(args, dist, E, mixed_cfg, args.served_rate)
@@ -618,6 +651,7 @@ def ours(args, dist):
         "cpu_baseline": cpu,
         "gpu_launches": int(launches),
         "clocks": ck,
+        "precision_form_stages": prec,
         "batched": batched,
         "served": served,
         "served_saturated": served_sat,
