@@ -272,8 +272,12 @@ struct eplace_ctx {
   DBuf<uint32_t> net_off, pin_cell;
   DBuf<uint8_t> has_driver;
   DBuf<uint32_t> wa_off, wa_pins;  // CSR copy, nets ordered by pin count
+  DBuf<uint32_t> wa_slots;         // padded pin table of the degree classes (kWaSlots)
   DBuf<float2> half;
   DBuf<float> area, pw;
+  DBuf<uint8_t> mflag;      // [N] 1 for a macro
+  DBuf<uint32_t> mac_idx;   // the macros' cell ids
+  uint32_t n_mac = 0;
   // state
   DBuf<float2> look;  // [N + F]
   DBuf<float2> x, xp, g, gprev, tmp_wl, tmp_den;
@@ -393,6 +397,34 @@ void degree_sorted_csr(const HostProblem &hp, std::vector<uint32_t> &off, std::v
   }
 }
 
+// The padded pin table of the degree classes: net idx of class j takes
+// G * S slots (G = kWaGroup[j], S = kWaSlots[j]) from the class base (a
+// multiple of 4 slots, for 16-byte loads); pin q of the net goes to lane
+// q % G, slot q / G of that lane.  Sets each class's slot_base.
+std::vector<uint32_t> build_wa_slots(const std::vector<uint32_t> &off, const std::vector<uint32_t> &pins,
+                                     WaClass (&cls)[kWaClasses]) {
+  size_t total = 0;
+  for (int j = 0; j < kWaClasses; ++j) {
+    total = (total + 3) & ~(size_t)3;
+    cls[j].slot_base = (long long)total;
+    total += (size_t)cls[j].nets * kWaGroup[j] * kWaSlots[j];
+  }
+  std::vector<uint32_t> t(std::max<size_t>(total, 4), 0xffffffffu);
+  for (int j = 0; j < kWaClasses; ++j) {
+    const int G = kWaGroup[j], S = kWaSlots[j];
+    if (S == 0) continue;
+    for (int idx = 0; idx < cls[j].nets; ++idx) {
+      const uint32_t n = (uint32_t)(cls[j].first_net + idx);
+      const size_t base = (size_t)cls[j].slot_base + (size_t)idx * G * S;
+      for (uint32_t q = off[n]; q < off[n + 1]; ++q) {
+        const uint32_t r = q - off[n];
+        t[base + (size_t)(r % G) * S + r / G] = pins[q];
+      }
+    }
+  }
+  return t;
+}
+
 // Fixed-point exponent k of the packed WA gradient: every cell's x and y
 // sums must stay below 2^31 in magnitude.  With at most D pins on one cell
 // and a bound of 4 per pin, 4 D 2^k < 2^31; k is at most 24.
@@ -417,7 +449,7 @@ int build_wa_classes(const std::vector<uint32_t> &off, WaClass (&cls)[kWaClasses
     const uint32_t first = n;
     while (n < NN && off[n + 1] - off[n] <= (uint32_t)kWaDegHi[j]) ++n;
     const int per_warp = 32 / kWaGroup[j];
-    cls[j] = WaClass{(int)first, (int)(n - first), warps};
+    cls[j] = WaClass{(int)first, (int)(n - first), warps, 0};
     warps += (int)((n - first + per_warp - 1) / per_warp);
   }
   return warps;
@@ -547,6 +579,7 @@ void launch_wa_stage(eplace_ctx *c, float gamma, cudaStream_t st = nullptr) {
   WaArgs a{};
   std::copy(c->wa_cls, c->wa_cls + kWaClasses, a.cls);
   a.nwarps = c->wa_warps;
+  a.slots = c->wa_slots.p;
   a.net_off = c->wa_off.p;
   a.pin_cell = c->wa_pins.p;
   a.pos = c->look.p;
@@ -559,7 +592,8 @@ void launch_wa_stage(eplace_ctx *c, float gamma, cudaStream_t st = nullptr) {
 
 void launch_scatter_stage(eplace_ctx *c) {
   const HostProblem &hp = c->hp;
-  ScatterArgs a{c->look.p, hp.any_macro ? c->half.p : nullptr, hp.N, hp.BX, hp.BY,
+  ScatterArgs a{c->look.p, hp.any_macro ? c->half.p : nullptr, hp.any_macro ? c->mflag.p : nullptr,
+                hp.any_macro ? c->mac_idx.p : nullptr, hp.any_macro ? c->n_mac : 0u, hp.N, hp.BX, hp.BY,
                 (float)hp.sx, (float)hp.sy, 1.0f / (float)hp.sx, 1.0f / (float)hp.sy, c->dens.p};
   CK(launch_scatter(a, grid_for((int)hp.N, kScatterBlock, c->num_sms * 16), c->stream));
 }
@@ -707,7 +741,7 @@ void launch_final_stage(eplace_ctx *c, double *dens_out, bool tc = false) {
   const int nb = hp.BX * hp.BY;
   const double c0 = c->total_area / (double)nb;
   FinalArgs a{c->dens.p, nb, (double)hp.sx * hp.sy, c0, tc ? nullptr : c->rho.p, tc ? c->rho_h.p : nullptr,
-              tc ? c->rho_l.p : nullptr, dens_out, c->part.p, c->bar.p + 2, c->sc.p, c->log.p};
+              tc ? c->rho_l.p : nullptr, dens_out, 0, c->part.p, c->bar.p + 2, c->sc.p, c->log.p};
   CK(launch_density_final(a, grid_for((nb + 3) / 4, kFinalBlock, c->num_sms * 4), c->stream));
 }
 
@@ -790,6 +824,9 @@ StepArgs step_args(eplace_ctx *c) {
   a.look = c->look.p;
   a.half = hp.any_macro ? c->half.p : nullptr;
   a.area = hp.any_macro ? c->area.p : nullptr;
+  a.mflag = hp.any_macro ? c->mflag.p : nullptr;
+  a.mac_idx = hp.any_macro ? c->mac_idx.p : nullptr;
+  a.n_mac = hp.any_macro ? c->n_mac : 0;
   a.pw = c->pw.p;
   a.acc = c->acc.p;
   a.grad_inv = std::ldexp(1.0, -c->grad_k);
@@ -982,6 +1019,9 @@ void load_into(eplace_ctx *c, HostProblem &&hp_in) {
     c->wa_pins.ensure(std::max<size_t>(spins.size(), 1));
     c->wa_pins.upload(spins.data(), spins.size(), s);
     c->wa_warps = build_wa_classes(soff, c->wa_cls);
+    std::vector<uint32_t> slots = build_wa_slots(soff, spins, c->wa_cls);
+    c->wa_slots.ensure(slots.size());
+    c->wa_slots.upload(slots.data(), slots.size(), s);
   }
   const size_t N1 = std::max<size_t>(hp.N, 1);
   std::vector<float2> half(hp.N);
@@ -997,6 +1037,20 @@ void load_into(eplace_ctx *c, HostProblem &&hp_in) {
   c->half.upload(half.data(), hp.N, s);
   c->area.ensure(N1);
   c->area.upload(area.data(), hp.N, s);
+  {
+    std::vector<uint8_t> mf(hp.N, 0);
+    std::vector<uint32_t> mi;
+    for (uint32_t i = 0; i < hp.N; ++i)
+      if (hp.cw[i] * hp.ch[i] > 1) {
+        mf[i] = 1;
+        mi.push_back(i);
+      }
+    c->n_mac = (uint32_t)mi.size();
+    c->mflag.ensure(N1);
+    c->mflag.upload(mf.data(), hp.N, s);
+    c->mac_idx.ensure(std::max<size_t>(mi.size(), 1));
+    c->mac_idx.upload(mi.data(), mi.size(), s);
+  }
   pin_weights(hp, c->pw_host);
   std::vector<float> pwf(c->pw_host.begin(), c->pw_host.end());
   c->pw.ensure(N1);
@@ -1941,8 +1995,8 @@ eplace_status ctx_load_problem(eplace_ctx *c, HostProblem &&hp) {
 uint64_t eplace_ctx::device_bytes() const {
   uint64_t b = 0;
   auto add = [&b](const auto &buf) { b += (uint64_t)buf.cap * sizeof(*buf.p); };
-  add(net_off); add(pin_cell); add(has_driver); add(wa_off); add(wa_pins);
-  add(half); add(area); add(pw); add(look); add(x); add(xp); add(g); add(gprev); add(tmp_wl); add(tmp_den);
+  add(net_off); add(pin_cell); add(has_driver); add(wa_off); add(wa_slots); add(wa_pins);
+  add(half); add(area); add(mflag); add(mac_idx); add(pw); add(look); add(x); add(xp); add(g); add(gprev); add(tmp_wl); add(tmp_den);
   add(acc); add(dens); add(rho); add(T); add(Exh); add(Eyh); add(U); add(V); add(Ex); add(Ey); add(phi);
   add(mB1); add(mL2); add(mB3); add(mL4); add(mB5); add(mL6); add(mB3g); add(mL6g);
   add(wx); add(gx2); add(wy); add(gy2); add(ops); add(mom); add(part); add(part2); add(part_b);

@@ -166,24 +166,41 @@ __device__ __forceinline__ float group_allreduce(float v, int g, Op op) {
 // otherwise (register budget).  Nets with fewer than two pins contribute
 // nothing (wa.rs:58).
 template <int P>
-__device__ __forceinline__ void wa_group(const WaArgs &a, const WaClass &cl, int g, int np, int wi, int lane) {
+__device__ __forceinline__ void wa_group(const WaArgs &a, const WaClass &cl, int g, int pp, int wi, int lane) {
   constexpr bool kKeep = P <= 4;
   const float kg = a.gamma * kLog2e;
   const int gl = lane & (g - 1);
   const int idx = wi * (32 / g) + lane / g;
   const bool valid = idx < cl.nets;
-  uint32_t pb = 0, pe = 0;
-  if (valid) {
-    pb = a.net_off[cl.first_net + idx];
-    pe = a.net_off[cl.first_net + idx + 1];
-  }
+  // The lane's pp (<= P) pin slots in one vector load: no CSR offsets.
   uint32_t cc[P];
-  float px[P], py[P];
 #pragma unroll
-  for (int k = 0; k < P; ++k) {
-    const uint32_t q = pb + gl + g * k;
-    cc[k] = (k < np && q < pe) ? a.pin_cell[q] : 0xffffffffu;
+  for (int k = 0; k < P; ++k) cc[k] = 0xffffffffu;
+  if (valid) {
+    const uint32_t *sp = a.slots + cl.slot_base + (long long)idx * (g * pp) + gl * pp;
+    if (pp == 2) {
+      const uint2 v = *reinterpret_cast<const uint2 *>(sp);
+      cc[0] = v.x;
+      cc[1] = v.y;
+    } else if (pp == 4 || P < 8) {
+      const uint4 v = *reinterpret_cast<const uint4 *>(sp);
+      cc[0] = v.x;
+      cc[1] = v.y;
+      cc[P > 2 ? 2 : 0] = P > 2 ? v.z : cc[0];
+      cc[P > 3 ? 3 : 0] = P > 3 ? v.w : cc[0];
+    } else {
+      const uint4 v0 = *reinterpret_cast<const uint4 *>(sp), v1 = *reinterpret_cast<const uint4 *>(sp + 4);
+      cc[0] = v0.x;
+      cc[1] = v0.y;
+      cc[P > 2 ? 2 : 0] = P > 2 ? v0.z : cc[0];
+      cc[P > 3 ? 3 : 0] = P > 3 ? v0.w : cc[0];
+      cc[P > 4 ? 4 : 0] = P > 4 ? v1.x : cc[0];
+      cc[P > 5 ? 5 : 0] = P > 5 ? v1.y : cc[0];
+      cc[P > 6 ? 6 : 0] = P > 6 ? v1.z : cc[0];
+      cc[P > 7 ? 7 : 0] = P > 7 ? v1.w : cc[0];
+    }
   }
+  float px[P], py[P];
   float mx = -INFINITY, mn = INFINITY, my = -INFINITY, ny = INFINITY;
 #pragma unroll
   for (int k = 0; k < P; ++k) {
@@ -220,7 +237,7 @@ __device__ __forceinline__ void wa_group(const WaArgs &a, const WaClass &cl, int
   }
 #pragma unroll
   for (int k = 0; k < 8; ++k) s[k] = group_allreduce(s[k], g, OpAdd());
-  if (pe - pb < 2) return;  // also the lanes of an empty slot (pb == pe)
+  if (!valid) return;  // every net of a class has two pins or more
   const float ipx = 1.0f / s[0], imx = 1.0f / s[2], ipy = 1.0f / s[4], imy = 1.0f / s[6];
 #pragma unroll
   for (int k = 0; k < P; ++k) {
@@ -301,11 +318,11 @@ __global__ void __launch_bounds__(kWaBlock) k_wa(const WaArgs a) {
     switch (j) {
       case 0: case 1: case 2: case 3: case 4: {  // up to 32 pins: 1..8 lanes per net, <= 4 pins per lane
         const int g = j <= 1 ? 1 : (1 << (j - 1));   // kWaGroup
-        wa_group<4>(a, cl, g, j == 0 ? 2 : 4, wi, lane);
+        wa_group<4>(a, cl, g, j == 0 ? 2 : 4, wi, lane);  // kWaSlots
         break;
       }
-      case 5: case 6: case 7:  // 33..224 pins: a warp per net, <= 7 pins per lane
-        wa_group<7>(a, cl, 32, j == 5 ? 2 : (j == 6 ? 4 : 7), wi, lane);
+      case 5: case 6: case 7:  // 33..224 pins: a warp per net, <= 8 slots per lane
+        wa_group<8>(a, cl, 32, j == 5 ? 2 : (j == 6 ? 4 : 8), wi, lane);
         break;
       default: {
         const uint32_t n = cl.first_net + wi;
@@ -345,11 +362,42 @@ __device__ __forceinline__ float overlap_1d(float lo, float hi, int b, float s) 
   return fmaxf(fminf(hi, b0 + s) - fmaxf(lo, b0), 0.0f);
 }
 
+// Unit cells first (a 1x1 footprint covers at most 2 x 2 bins: unrolled, no
+// footprint load), then the macros from their own list, so a warp of unit
+// cells never waits for one macro's loop.  Fixed-point atomics make the
+// order irrelevant.  Without a macro list but with footprints, every cell
+// takes the general loop.
 __global__ void __launch_bounds__(kScatterBlock) k_scatter(const ScatterArgs a) {
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < a.N; i += gridDim.x * blockDim.x) {
-    const float2 p = a.pos[i];
-    const float2 hf = a.half ? a.half[i] : make_float2(0.5f, 0.5f);
-    const Foot f = make_foot(p, hf.x, hf.y, a.BX, a.BY, a.inv_sx, a.inv_sy);
+  const uint32_t t0 = blockIdx.x * blockDim.x + threadIdx.x, ts = gridDim.x * blockDim.x;
+  if (a.half && !a.mflag) {
+    for (uint32_t i = t0; i < a.N; i += ts) {
+      const float2 hf = a.half[i];
+      const Foot f = make_foot(a.pos[i], hf.x, hf.y, a.BX, a.BY, a.inv_sx, a.inv_sy);
+      for (int by = f.by0; by < f.by1; ++by) {
+        const float oy = overlap_1d(f.ylo, f.yhi, by, a.sy);
+        for (int bx = f.bx0; bx < f.bx1; ++bx) {
+          const float ar = overlap_1d(f.xlo, f.xhi, bx, a.sx) * oy;
+          if (ar > 0.0f) atomicAdd(&a.dens[(size_t)by * a.BX + bx], to_fix(ar));
+        }
+      }
+    }
+    return;
+  }
+  for (uint32_t i = t0; i < a.N; i += ts) {
+    if (a.mflag && a.mflag[i]) continue;
+    const Foot f = make_foot(a.pos[i], 0.5f, 0.5f, a.BX, a.BY, a.inv_sx, a.inv_sy);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int by = f.by0 + (k >> 1), bx = f.bx0 + (k & 1);
+      if (by >= f.by1 || bx >= f.bx1) continue;
+      const float ar = overlap_1d(f.xlo, f.xhi, bx, a.sx) * overlap_1d(f.ylo, f.yhi, by, a.sy);
+      if (ar > 0.0f) atomicAdd(&a.dens[(size_t)by * a.BX + bx], to_fix(ar));
+    }
+  }
+  for (uint32_t k = t0; k < a.n_mac; k += ts) {
+    const uint32_t i = a.mac_idx[k];
+    const float2 hf = a.half[i];
+    const Foot f = make_foot(a.pos[i], hf.x, hf.y, a.BX, a.BY, a.inv_sx, a.inv_sy);
     for (int by = f.by0; by < f.by1; ++by) {
       const float oy = overlap_1d(f.ylo, f.yhi, by, a.sy);
       for (int bx = f.bx0; bx < f.bx1; ++bx) {
@@ -365,9 +413,9 @@ __global__ void __launch_bounds__(kFinalBlock) k_density_final(const FinalArgs a
   __shared__ bool last;
   double v[2] = {0.0, 0.0};
   // Groups of four consecutive bins per thread and step: 16-byte loads and
-  // stores (the bin count of every supported grid is a multiple of 4; a
-  // ragged tail takes the scalar loop below).
-  const int ng = a.nb >> 2;
+  // stores (when every pointer is aligned for them; a ragged tail, or
+  // unaligned caller buffers, take the scalar loop below).
+  const int ng = a.vec4 ? (a.nb >> 2) : 0;
   const int t0 = blockIdx.x * blockDim.x + threadIdx.x, ts = gridDim.x * blockDim.x;
   for (int gi = t0; gi < ng; gi += ts) {
     ulonglong2 *dp = reinterpret_cast<ulonglong2 *>(a.dens) + 2 * gi;
@@ -615,45 +663,54 @@ __device__ __forceinline__ void grid_barrier(unsigned *bar, DevScalars *sc) {
   __syncthreads();
 }
 
+// Field gather of a 1x1 footprint: it touches at most 2 x 2 bins (bins are
+// >= 1 site wide); weights first, then all field loads at once, summed in the
+// same row-major order as the general loop of gather_cell.
+__device__ __forceinline__ float2 gather_unit_foot(const StepArgs &a, const Foot &f) {
+  float fx = 0.f, fy = 0.f, wt = 0.f;
+  float w[4];
+  size_t id[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int by = f.by0 + (k >> 1), bx = f.bx0 + (k & 1);
+    const bool in = by < f.by1 && bx < f.bx1;
+    w[k] = in ? overlap_1d(f.xlo, f.xhi, bx, a.sx) * overlap_1d(f.ylo, f.yhi, by, a.sy) : 0.0f;
+    id[k] = (w[k] > 0.0f) ? (size_t)by * a.BX + bx : 0;
+  }
+  float e[4], h[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    e[k] = (w[k] > 0.0f) ? a.Ex[id[k]] : 0.0f;
+    h[k] = (w[k] > 0.0f) ? a.Ey[id[k]] : 0.0f;
+  }
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+    if (w[k] > 0.0f) {
+      fx = fmaf(w[k], e[k], fx);
+      fy = fmaf(w[k], h[k], fy);
+      wt += w[k];
+    }
+  float2 g = make_float2(0.f, 0.f);
+  if (wt > 1e-10f) {
+    g.x = fx / wt;
+    g.y = fy / wt;
+  }
+  return g;
+}
+
+// Field gather of a 1x1 cell (no footprint load).
+__device__ __forceinline__ float2 gather_unit(const StepArgs &a, float2 p) {
+  const Foot f = make_foot(p, 0.5f, 0.5f, a.BX, a.BY, a.inv_sx, a.inv_sy);
+  return gather_unit_foot(a, f);
+}
+
 // Weighted-mean field gather for one cell, scaled by its area
 // (compute_density_gradient, density.rs:171-206).
 __device__ __forceinline__ float2 gather_cell(const StepArgs &a, uint32_t i, float2 p) {
   const float2 hf = a.half ? a.half[i] : make_float2(0.5f, 0.5f);
   const Foot f = make_foot(p, hf.x, hf.y, a.BX, a.BY, a.inv_sx, a.inv_sy);
   float fx = 0.f, fy = 0.f, wt = 0.f;
-  if (hf.x == 0.5f && hf.y == 0.5f) {
-    // A 1x1 footprint touches at most 2 x 2 bins (bins are >= 1 site wide):
-    // weights first, then all field loads at once, summed in the same
-    // row-major order as the general loop below.
-    float w[4];
-    size_t id[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const int by = f.by0 + (k >> 1), bx = f.bx0 + (k & 1);
-      const bool in = by < f.by1 && bx < f.bx1;
-      w[k] = in ? overlap_1d(f.xlo, f.xhi, bx, a.sx) * overlap_1d(f.ylo, f.yhi, by, a.sy) : 0.0f;
-      id[k] = (w[k] > 0.0f) ? (size_t)by * a.BX + bx : 0;
-    }
-    float e[4], h[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      e[k] = (w[k] > 0.0f) ? a.Ex[id[k]] : 0.0f;
-      h[k] = (w[k] > 0.0f) ? a.Ey[id[k]] : 0.0f;
-    }
-#pragma unroll
-    for (int k = 0; k < 4; ++k)
-      if (w[k] > 0.0f) {
-        fx = fmaf(w[k], e[k], fx);
-        fy = fmaf(w[k], h[k], fy);
-        wt += w[k];
-      }
-    float2 g = make_float2(0.f, 0.f);
-    if (wt > 1e-10f) {
-      g.x = fx / wt;
-      g.y = fy / wt;
-    }
-    return g;
-  }
+  if (hf.x == 0.5f && hf.y == 0.5f) return gather_unit_foot(a, f);
   for (int by = f.by0; by < f.by1; ++by) {
     const float oy = overlap_1d(f.ylo, f.yhi, by, a.sy);
     for (int bx = f.bx0; bx < f.bx1; ++bx) {
@@ -676,9 +733,10 @@ __device__ __forceinline__ float2 gather_cell(const StepArgs &a, uint32_t i, flo
 }
 
 // g = (g_wl + lam g_den) / max(1, pw + lam area)   (mod.rs:145-156)
+// unit: a 1x1 cell, whose area is 1 (no load).
 __device__ __forceinline__ float2 combine(const StepArgs &a, uint32_t i, float2 gw, float2 gd,
-                                          double lam) {
-  const double ar = a.area ? (double)a.area[i] : 1.0;
+                                          double lam, bool unit) {
+  const double ar = (unit || !a.area) ? 1.0 : (double)a.area[i];
   const double ipc = 1.0 / fmax((double)a.pw[i] + lam * ar, 1.0);
   return make_float2((float)(((double)gw.x + lam * (double)gd.x) * ipc),
                      (float)(((double)gw.y + lam * (double)gd.y) * ipc));
@@ -691,9 +749,10 @@ struct CellA {
   float2 x, xp, gp;  // for the Barzilai-Borwein dots (after the first penalty)
 };
 
-__device__ __forceinline__ CellA load_a(const StepArgs &a, uint32_t i, bool was_init) {
+// unit: the cell is 1x1 (the 2 x 2-bin gather, no footprint load).
+__device__ __forceinline__ CellA load_a(const StepArgs &a, uint32_t i, bool was_init, bool unit) {
   CellA c;
-  c.gd = gather_cell(a, i, a.look[i]);
+  c.gd = unit ? gather_unit(a, a.look[i]) : gather_cell(a, i, a.look[i]);
   long long sx, sy;
   unpack_grad(a.acc[i], &sx, &sy);
   c.gw = make_float2((float)((double)sx * a.grad_inv), (float)((double)sy * a.grad_inv));
@@ -706,10 +765,10 @@ __device__ __forceinline__ CellA load_a(const StepArgs &a, uint32_t i, bool was_
 }
 
 __device__ __forceinline__ void finish_a(const StepArgs &a, uint32_t i, const CellA &c, bool was_init, double lam,
-                                         double (&v)[4]) {
+                                         bool unit, double (&v)[4]) {
   a.acc[i] = 0ull;
   if (was_init) {
-    const float2 g = combine(a, i, c.gw, c.gd, lam);
+    const float2 g = combine(a, i, c.gw, c.gd, lam, unit);
     a.g[i] = g;
     const double dx = (double)c.x.x - c.xp.x, dy = (double)c.x.y - c.xp.y;
     v[0] += dx * dx;
@@ -773,15 +832,27 @@ __global__ void __launch_bounds__(kStepBlock, 2) k_step(const StepArgs a) {
   if (a.mode == 0 || a.mode == 2) {
     // Phase A: gather, read + clear the WA accumulator, combine.  Two cells
     // per thread and pass (i and i + gstride): every load of both is issued
-    // before the first store, so their latencies overlap; partial sums run
-    // in the same cell order as a one-cell loop.
+    // before the first store, so their latencies overlap.  Macros (w*h > 1)
+    // are skipped here and done afterwards from their own list, so a warp
+    // of unit cells never waits for one macro's multi-bin gather.
     for (uint32_t i0 = tid0; i0 < a.N; i0 += 2 * gstride) {
       const uint32_t i1 = i0 + gstride;
       const bool h1 = i1 < a.N;
-      CellA c0 = load_a(a, i0, was_init);
-      CellA c1 = h1 ? load_a(a, i1, was_init) : c0;
-      finish_a(a, i0, c0, was_init, lam, v);
-      if (h1) finish_a(a, i1, c1, was_init, lam, v);
+      const bool u0 = !a.mflag || !a.mflag[i0];
+      const bool u1 = h1 && (!a.mflag || !a.mflag[i1]);
+      CellA c0, c1;
+      if (u0) c0 = load_a(a, i0, was_init, true);
+      if (u1) c1 = load_a(a, i1, was_init, true);
+      if (u0) finish_a(a, i0, c0, was_init, lam, true, v);
+      if (u1) finish_a(a, i1, c1, was_init, lam, true, v);
+    }
+    // Macro k goes to thread gstride - 1 - k (mod gstride): the threads at
+    // the end of the grid hold the fewest unit cells when N is not a
+    // multiple of 2 * gstride.
+    for (uint32_t k = gstride - 1 - tid0; k < a.n_mac; k += gstride) {
+      const uint32_t i = a.mac_idx[k];
+      const CellA c = load_a(a, i, was_init, false);
+      finish_a(a, i, c, was_init, lam, false, v);
     }
     block_sum<4>(v, sm);
     if (threadIdx.x == 0)
@@ -806,7 +877,7 @@ __global__ void __launch_bounds__(kStepBlock, 2) k_step(const StepArgs a) {
       if (coop) grid_barrier(a.bar, a.sc);  // everyone has read part[] before it is reused
       for (int k = 0; k < 4; ++k) v[k] = 0.0;
       for (uint32_t i = tid0; i < a.N; i += gstride) {
-        const float2 g = combine(a, i, a.tmp_wl[i], a.tmp_den[i], lam);
+        const float2 g = combine(a, i, a.tmp_wl[i], a.tmp_den[i], lam, false);
         a.g[i] = g;
         const float2 x = a.x[i], xp = a.xp[i], gp = a.gprev[i];
         const double dx = (double)x.x - xp.x, dy = (double)x.y - xp.y;
@@ -921,7 +992,10 @@ cudaError_t launch_scatter(const ScatterArgs &a, int grid, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-cudaError_t launch_density_final(const FinalArgs &a, int grid, cudaStream_t s) {
+cudaError_t launch_density_final(const FinalArgs &a_in, int grid, cudaStream_t s) {
+  FinalArgs a = a_in;
+  auto al = [](const void *p, uintptr_t m) { return ((uintptr_t)p & (m - 1)) == 0; };
+  a.vec4 = al(a.dens, 16) && al(a.rho, 16) && al(a.rho_hi, 8) && al(a.rho_lo, 8) && al(a.dens_out, 16);
   k_density_final<<<grid, kFinalBlock, 0, s>>>(a);
   return cudaGetLastError();
 }

@@ -32,11 +32,15 @@ struct IterLog {
 // Degree classes of the WA kernel over the degree-sorted nets: class j holds
 // the nets of degree (kWaDegHi[j-1], kWaDegHi[j]] (class 0 from degree 2;
 // nets of fewer pins have no gradient) and runs kWaGroup[j] lanes per net,
-// kWaPins[j] pins per lane; the last class (more than 224 pins) runs a warp
-// per net over its pins in three passes.
+// kWaSlots[j] pin slots per lane; the last class (more than 224 pins) runs a
+// warp per net over its CSR pins in three passes.
 constexpr int kWaClasses = 9;
 constexpr int kWaDegHi[kWaClasses] = {2, 4, 8, 16, 32, 64, 128, 224, 0x7fffffff};
 constexpr int kWaGroup[kWaClasses] = {1, 1, 2, 4, 8, 32, 32, 32, 32};
+// Padded pin table: lane l of a net's group holds that net's pins l, l + G,
+// l + 2G, ... in its kWaSlots[j] consecutive slots (one 8-, 16- or 32-byte
+// load), unused slots 0xffffffff; a net takes G * kWaSlots[j] slots.
+constexpr int kWaSlots[kWaClasses] = {2, 4, 4, 4, 4, 2, 4, 8, 0};
 
 // The WA gradient of a cell is accumulated as one 64-bit integer per cell:
 // x and y in fixed point (scale 2^k), packed as gx + 2^32 gy and summed with
@@ -55,14 +59,16 @@ __host__ __device__ inline void unpack_grad(unsigned long long v, long long *gx,
 }
 
 struct WaClass {
-  int first_net;   // index into the degree-sorted CSR
+  int first_net;        // index into the degree-sorted CSR
   int nets;
-  int first_warp;  // warps of the classes before this one
+  int first_warp;       // warps of the classes before this one
+  long long slot_base;  // first slot of the class in the padded pin table (multiple of 4)
 };
 
 struct WaArgs {
   WaClass cls[kWaClasses];
   int nwarps;
+  const uint32_t *slots;    // padded pin table (kWaSlots)
   const uint32_t *net_off;
   const uint32_t *pin_cell;
   const float2 *pos;        // [N + F]: look-ahead positions, then fixed cells
@@ -75,6 +81,9 @@ struct WaArgs {
 struct ScatterArgs {
   const float2 *pos;
   const float2 *half;       // half extents, nullptr => unit cells
+  const uint8_t *mflag;     // [N] 1 for a macro, nullptr: no macro list (general loop when half is set)
+  const uint32_t *mac_idx;  // [n_mac] the macros' cell ids
+  uint32_t n_mac;
   uint32_t N;
   int BX, BY;
   float sx, sy, inv_sx, inv_sy;
@@ -90,6 +99,7 @@ struct FinalArgs {
   __nv_bfloat16 *rho_hi;    // BF16 hi/lo charge map (tensor-core transform), or nullptr
   __nv_bfloat16 *rho_lo;
   double *dens_out;         // optional FP64 copy (stage entry)
+  int vec4;                 // set by launch_density_final: every pointer allows 16-byte groups
   double *part;             // [2 * grid]
   unsigned *ticket;
   DevScalars *sc;
@@ -118,6 +128,9 @@ struct StepArgs {
   float2 *look;             // [N] (fixed cells follow in the same buffer)
   const float2 *half;       // nullptr => unit cells
   const float *area;
+  const uint8_t *mflag;     // [N] 1 for a macro (w*h > 1), nullptr when there are none
+  const uint32_t *mac_idx;  // [n_mac] the macros' cell ids, ascending
+  uint32_t n_mac;
   const float *pw;
   unsigned long long *acc;  // [N] packed WA accumulator, read then zeroed
   double grad_inv;          // 1 / WaArgs::grad_scale

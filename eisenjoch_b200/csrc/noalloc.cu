@@ -99,8 +99,8 @@ extern "C" eplace_status eplace_density_noalloc(const float *pos_xy, const float
       cudaMemsetAsync(ticket, 0, 256, s) != cudaSuccess || cudaMemsetAsync(sc, 0, 256, s) != cudaSuccess)
     return EPLACE_ERR_CUDA;
   const float sx = (float)(width / bins_x), sy = (float)(height / bins_y);
-  ScatterArgs a{reinterpret_cast<const float2 *>(pos_xy), reinterpret_cast<const float2 *>(half_wh), num_cells,
-                bins_x, bins_y, sx, sy, 1.0f / sx, 1.0f / sy, map};
+  ScatterArgs a{reinterpret_cast<const float2 *>(pos_xy), reinterpret_cast<const float2 *>(half_wh), nullptr,
+                nullptr, 0u, num_cells, bins_x, bins_y, sx, sy, 1.0f / sx, 1.0f / sy, map};
   if (num_cells) {
     long long g = ((long long)num_cells + kScatterBlock - 1) / kScatterBlock;
     if (g > (long long)sms * 16) g = (long long)sms * 16;
@@ -109,7 +109,7 @@ extern "C" eplace_status eplace_density_noalloc(const float *pos_xy, const float
   long long fg = ((long long)nb + kFinalBlock - 1) / kFinalBlock;
   if (fg > (long long)sms * 2) fg = (long long)sms * 2;
   if (fg > kNoAllocMaxBlocks) fg = kNoAllocMaxBlocks;
-  FinalArgs f{map, nb, (double)sx * (double)sy, 0.0, nullptr, nullptr, nullptr, density, part, ticket, sc, lg};
+  FinalArgs f{map, nb, (double)sx * (double)sy, 0.0, nullptr, nullptr, nullptr, density, 0, part, ticket, sc, lg};
   if (launch_density_final(f, (int)fg, s) != cudaSuccess) return EPLACE_ERR_CUDA;
   if (cudaMemcpyAsync(overlap, &sc->overlap, sizeof(double), cudaMemcpyDeviceToDevice, s) != cudaSuccess)
     return EPLACE_ERR_CUDA;
