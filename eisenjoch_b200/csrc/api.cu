@@ -382,11 +382,12 @@ eplace_status cuda_fail(eplace_ctx *c, const CudaError &e) {
 // count (stable), so nets of one degree class are contiguous.  Net order
 // does not change the result: the gradient accumulates in fixed point.
 void degree_sorted_csr(const HostProblem &hp, std::vector<uint32_t> &off, std::vector<uint32_t> &pins) {
+  // Counting sort by degree (stable: nets of one degree keep their order).
+  std::vector<uint32_t> start((size_t)hp.max_degree + 2, 0);
+  for (uint32_t n = 0; n < hp.NN; ++n) ++start[hp.net_off[n + 1] - hp.net_off[n] + 1];
+  for (size_t d = 1; d < start.size(); ++d) start[d] += start[d - 1];
   std::vector<uint32_t> order(hp.NN);
-  for (uint32_t n = 0; n < hp.NN; ++n) order[n] = n;
-  std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
-    return hp.net_off[a + 1] - hp.net_off[a] < hp.net_off[b + 1] - hp.net_off[b];
-  });
+  for (uint32_t n = 0; n < hp.NN; ++n) order[start[hp.net_off[n + 1] - hp.net_off[n]]++] = n;
   off.assign(hp.NN + 1, 0);
   pins.resize(hp.P);
   uint32_t k = 0;
@@ -1005,21 +1006,44 @@ void load_into(eplace_ctx *c, HostProblem &&hp_in) {
     c->g_valid = false;  // updated in place by the next capture
   }
   ++c->buf_epoch;
+  // Host-side derived arrays are built on two helper threads while this
+  // thread uploads the netlist; all CUDA calls stay on this thread.
+  std::vector<uint32_t> soff, spins, slots;
+  WaClass cls[kWaClasses];
+  int wa_warps = 0;
+  std::thread t_wa([&] {
+    degree_sorted_csr(hp, soff, spins);
+    wa_warps = build_wa_classes(soff, cls);
+    slots = build_wa_slots(soff, spins, cls);
+  });
+  int grad_k = 24;
+  std::thread t_pw([&] {
+    pin_weights(hp, c->pw_host);
+    grad_k = grad_scale_log2(hp);
+  });
+  struct Joiner {  // joins the helpers on every exit, an upload error included
+    std::thread &a, &b;
+    ~Joiner() {
+      if (a.joinable()) a.join();
+      if (b.joinable()) b.join();
+    }
+  } joiner{t_wa, t_pw};
   c->net_off.ensure(hp.net_off.size());
   c->net_off.upload(hp.net_off.data(), hp.net_off.size(), s);
   c->pin_cell.ensure(std::max<size_t>(hp.P, 1));
   c->pin_cell.upload(hp.pin_cell.data(), hp.P, s);
   c->has_driver.ensure(std::max<size_t>(hp.NN, 1));
   c->has_driver.upload(hp.has_driver.data(), hp.NN, s);
+  t_wa.join();
   {
-    std::vector<uint32_t> soff, spins;
-    degree_sorted_csr(hp, soff, spins);
+    std::copy(cls, cls + kWaClasses, c->wa_cls);
+    c->wa_warps = wa_warps;
+    // The sorted CSR itself is read only by the last class (nets of more
+    // than 224 pins); the others read the padded table.
     c->wa_off.ensure(soff.size());
     c->wa_off.upload(soff.data(), soff.size(), s);
     c->wa_pins.ensure(std::max<size_t>(spins.size(), 1));
-    c->wa_pins.upload(spins.data(), spins.size(), s);
-    c->wa_warps = build_wa_classes(soff, c->wa_cls);
-    std::vector<uint32_t> slots = build_wa_slots(soff, spins, c->wa_cls);
+    if (c->wa_cls[kWaClasses - 1].nets > 0) c->wa_pins.upload(spins.data(), spins.size(), s);
     c->wa_slots.ensure(slots.size());
     c->wa_slots.upload(slots.data(), slots.size(), s);
   }
@@ -1051,7 +1075,7 @@ void load_into(eplace_ctx *c, HostProblem &&hp_in) {
     c->mac_idx.ensure(std::max<size_t>(mi.size(), 1));
     c->mac_idx.upload(mi.data(), mi.size(), s);
   }
-  pin_weights(hp, c->pw_host);
+  t_pw.join();
   std::vector<float> pwf(c->pw_host.begin(), c->pw_host.end());
   c->pw.ensure(N1);
   c->pw.upload(pwf.data(), hp.N, s);
@@ -1063,7 +1087,7 @@ void load_into(eplace_ctx *c, HostProblem &&hp_in) {
   for (auto *b : {&c->x, &c->xp, &c->g, &c->gprev, &c->tmp_wl, &c->tmp_den}) b->ensure(N1);
   c->acc.ensure(N1);
   c->acc.zero(s);
-  c->grad_k = grad_scale_log2(hp);
+  c->grad_k = grad_k;
   const size_t nb = (size_t)hp.BX * hp.BY;
   c->dens.ensure(nb);
   c->dens.zero(s);
