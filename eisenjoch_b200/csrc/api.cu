@@ -23,6 +23,7 @@
 #include <deque>
 #include <functional>
 #include <map>
+#include <tuple>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -341,6 +342,11 @@ struct eplace_ctx {
   bool shared_device = false;  // set by the job engine: other jobs' kernels run beside this one
   int mat_bx = -1, mat_by = -1;  // bin grid the DCT matrices were built for
   uint64_t load_gen = 0;         // bumped by every (re)load of a problem
+  // Launch shapes picked by autotune_launches (none of them changes a bit
+  // of any result): grid caps of the WA and scatter kernels in blocks per
+  // SM, and the SIMT GEMM tile of each of the four transform GEMMs.
+  int wa_blocks_per_sm = 16, sc_blocks_per_sm = 16;
+  int gemm_tile[4] = {0, 0, 0, 0};
   WaClass wa_cls[kWaClasses] = {};  // degree classes of the sorted CSR
   int wa_warps = 0;
   int grad_k = 24;  // fixed-point scale 2^k of the packed WA gradient (pack_grad)
@@ -588,7 +594,7 @@ void launch_wa_stage(eplace_ctx *c, float gamma, cudaStream_t st = nullptr) {
   a.N = c->hp.N;
   a.gamma = gamma;
   a.grad_scale = (float)std::ldexp(1.0, c->grad_k);
-  CK(launch_wa(a, grid_for(c->wa_warps * 32, kWaBlock, c->num_sms * 16), st ? st : c->stream));
+  CK(launch_wa(a, grid_for(c->wa_warps * 32, kWaBlock, c->num_sms * c->wa_blocks_per_sm), st ? st : c->stream));
 }
 
 void launch_scatter_stage(eplace_ctx *c) {
@@ -596,7 +602,7 @@ void launch_scatter_stage(eplace_ctx *c) {
   ScatterArgs a{c->look.p, hp.any_macro ? c->half.p : nullptr, hp.any_macro ? c->mflag.p : nullptr,
                 hp.any_macro ? c->mac_idx.p : nullptr, hp.any_macro ? c->n_mac : 0u, hp.N, hp.BX, hp.BY,
                 (float)hp.sx, (float)hp.sy, 1.0f / (float)hp.sx, 1.0f / (float)hp.sy, c->dens.p};
-  CK(launch_scatter(a, grid_for((int)hp.N, kScatterBlock, c->num_sms * 16), c->stream));
+  CK(launch_scatter(a, grid_for((int)hp.N, kScatterBlock, c->num_sms * c->sc_blocks_per_sm), c->stream));
 }
 
 // --- tensor-core transform set-up ------------------------------------------
@@ -790,24 +796,129 @@ void launch_field_gemm(eplace_ctx *c, int g, float *phi, int field_mode, bool tc
   const GemmOp *ops = c->ops.p + (fm ? 6 : 0);
   switch (g) {
     case 0:
-      CK(launch_sgemm(ops + 0, 1, H, W, W, c->stream));
+      CK(launch_sgemm(ops + 0, 1, H, W, W, c->stream, c->gemm_tile[0]));
       break;
     case 1: {
       SpectralArgs sp{c->wx.p, c->gx2.p, c->wy.p, c->gy2.p, (float)(4.0 / ((double)W * H)), phi};
-      CK(launch_sgemm_spectral(ops + 1, H, W, H, sp, c->stream));
+      CK(launch_sgemm_spectral(ops + 1, H, W, H, sp, c->stream, c->gemm_tile[1]));
       break;
     }
     case 2:
-      CK(launch_sgemm(ops + 2, 2, H, W, W, c->stream));
+      CK(launch_sgemm(ops + 2, 2, H, W, W, c->stream, c->gemm_tile[2]));
       break;
     default:
-      CK(launch_sgemm(ops + 4, 2, H, W, H, c->stream));
+      CK(launch_sgemm(ops + 4, 2, H, W, H, c->stream, c->gemm_tile[3]));
       break;
   }
 }
 
 void launch_field_stage(eplace_ctx *c, float *phi, int field_mode, bool tc = false) {
   for (int g = 0; g < 4; ++g) launch_field_gemm(c, g, phi, field_mode, tc);
+}
+
+// --- launch-shape autotuner ------------------------------------------------
+// Picks, by timing on the context's stream, the grid caps of the WA and
+// scatter kernels (4, 8, 16 or 32 blocks per SM) and the CTA tile of each
+// SIMT GEMM (64 or 32).  Every candidate computes the same bits (fixed-point
+// atomics; the GEMM sums each output in order whatever the tile), so the
+// choice only moves time.  Results are kept per process for a shape class
+// (cells and pins to the next power of two, bin grid, transform) and reused
+// by every context of that class.  Runs after reset_state (positions are the
+// initial placement), and clears the accumulators it dirtied.
+struct TuneKey {
+  int n2, p2, bx, by, tc;
+  bool operator<(const TuneKey &o) const {
+    return std::tie(n2, p2, bx, by, tc) < std::tie(o.n2, o.p2, o.bx, o.by, o.tc);
+  }
+};
+struct TuneVal {
+  int wa, sc, tile[4];
+};
+
+void autotune_launches(eplace_ctx *c, float gamma, int field_mode, bool tc) {
+  static std::mutex mu;
+  static std::map<TuneKey, TuneVal> *cache = new std::map<TuneKey, TuneVal>();  // process lifetime
+  const HostProblem &hp = c->hp;
+  auto lg = [](uint64_t v) {
+    int k = 0;
+    while ((1ull << k) < v) ++k;
+    return k;
+  };
+  const TuneKey key{lg(hp.N), lg(hp.P), hp.BX, hp.BY, tc ? 1 : 0};
+  {
+    std::lock_guard<std::mutex> g(mu);
+    auto it = cache->find(key);
+    if (it != cache->end()) {
+      c->wa_blocks_per_sm = it->second.wa;
+      c->sc_blocks_per_sm = it->second.sc;
+      std::copy(it->second.tile, it->second.tile + 4, c->gemm_tile);
+      return;
+    }
+  }
+  cudaStream_t s = c->stream;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  auto timed = [&](auto &&launch) {
+    launch();  // warm
+    float best = 1e30f;
+    for (int r = 0; r < 3; ++r) {
+      CK(cudaEventRecord(e0, s));
+      launch();
+      CK(cudaEventRecord(e1, s));
+      CK(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      CK(cudaEventElapsedTime(&ms, e0, e1));
+      best = std::min(best, ms);
+    }
+    return best;
+  };
+  TuneVal v{16, 16, {0, 0, 0, 0}};
+  try {
+    const int cand[4] = {4, 8, 16, 32};
+    float bw = 1e30f, bs = 1e30f;
+    for (int m : cand) {
+      c->wa_blocks_per_sm = m;
+      const float t = timed([&] { launch_wa_stage(c, gamma); });
+      if (t < bw) {
+        bw = t;
+        v.wa = m;
+      }
+      c->sc_blocks_per_sm = m;
+      const float u = timed([&] { launch_scatter_stage(c); });
+      if (u < bs) {
+        bs = u;
+        v.sc = m;
+      }
+    }
+    if (!tc) {
+      for (int g = 0; g < 4; ++g) {
+        float bt = 1e30f;
+        for (int tile : {64, 32}) {
+          c->gemm_tile[g] = tile;
+          const float t = timed([&] { launch_field_gemm(c, g, nullptr, field_mode, false); });
+          if (t < bt) {
+            bt = t;
+            v.tile[g] = tile;
+          }
+        }
+      }
+    }
+    c->acc.zero(s);
+    c->dens.zero(s);
+    CK(cudaStreamSynchronize(s));
+  } catch (...) {
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    throw;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  c->wa_blocks_per_sm = v.wa;
+  c->sc_blocks_per_sm = v.sc;
+  std::copy(v.tile, v.tile + 4, c->gemm_tile);
+  std::lock_guard<std::mutex> g(mu);
+  (*cache)[key] = v;
 }
 
 StepArgs step_args(eplace_ctx *c) {
@@ -1353,6 +1464,7 @@ struct JobState {
         ++c->buf_epoch;
       }
       reset_state(c, isx, isy, &cfg);
+      autotune_launches(c, gamma, opts.field_mode, tc);
       mark("device_reset");
       // Host resources persist in the context across runs.
       if (!c->lbase) c->lbase.reset(new LegalBase(hp));
@@ -2123,6 +2235,7 @@ eplace_status eplace_profile_stages(eplace_ctx *c, const eplace_cfg *cfg, const 
     upload_momentum(c, reps);
     if (tc) setup_tc(c);
     reset_state(c, isx, isy, cfg);
+    autotune_launches(c, (float)cfg->wl_coeff, opts.field_mode, tc);
     for (auto &e : ev) CK(cudaEventCreate(&e));
     const float gamma = (float)cfg->wl_coeff;
     double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};

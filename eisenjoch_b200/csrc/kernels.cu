@@ -1000,8 +1000,8 @@ cudaError_t launch_density_final(const FinalArgs &a_in, int grid, cudaStream_t s
   return cudaGetLastError();
 }
 
-cudaError_t launch_sgemm(const GemmOp *ops, int nb, int M, int N, int K, cudaStream_t s) {
-  if (sgemm_small_tile(M, N, nb)) {
+cudaError_t launch_sgemm(const GemmOp *ops, int nb, int M, int N, int K, cudaStream_t s, int tile) {
+  if (tile == 32 || (tile == 0 && sgemm_small_tile(M, N, nb))) {
     k_sgemm<false, 32, 32><<<dim3((N + 31) / 32, (M + 31) / 32, nb), 64, 0, s>>>(ops, M, N, K, SpectralArgs{});
   } else {
     k_sgemm<false, 64, 64><<<dim3((N + 63) / 64, (M + 63) / 64, nb), 256, 0, s>>>(ops, M, N, K, SpectralArgs{});
@@ -1010,8 +1010,8 @@ cudaError_t launch_sgemm(const GemmOp *ops, int nb, int M, int N, int K, cudaStr
 }
 
 cudaError_t launch_sgemm_spectral(const GemmOp *ops, int M, int N, int K, const SpectralArgs &sp,
-                                  cudaStream_t s) {
-  if (sgemm_small_tile(M, N, 1)) {
+                                  cudaStream_t s, int tile) {
+  if (tile == 32 || (tile == 0 && sgemm_small_tile(M, N, 1))) {
     k_sgemm<true, 32, 32><<<dim3((N + 31) / 32, (M + 31) / 32, 1), 64, 0, s>>>(ops, M, N, K, sp);
   } else {
     k_sgemm<true, 64, 64><<<dim3((N + 63) / 64, (M + 63) / 64, 1), 256, 0, s>>>(ops, M, N, K, sp);

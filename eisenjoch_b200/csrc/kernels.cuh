@@ -162,10 +162,12 @@ cudaError_t launch_wa(const WaArgs &a, int grid, cudaStream_t s);
 cudaError_t launch_scatter(const ScatterArgs &a, int grid, cudaStream_t s);
 cudaError_t launch_density_final(const FinalArgs &a, int grid, cudaStream_t s);
 // C[b] = A[b] (M x K) * B[b] (K x N), row-major FP32; batches from ops[0..nb).
-cudaError_t launch_sgemm(const GemmOp *ops_dev, int nb, int M, int N, int K, cudaStream_t s);
+// tile: 64 or 32 (CTA tile edge), 0 = pick by grid size.  Both tiles sum
+// every output in the same order, so the choice never changes the bits.
+cudaError_t launch_sgemm(const GemmOp *ops_dev, int nb, int M, int N, int K, cudaStream_t s, int tile = 0);
 // As above with the spectral epilogue: C = Ex_hat, C2 = Ey_hat.
 cudaError_t launch_sgemm_spectral(const GemmOp *ops_dev, int M, int N, int K,
-                                  const SpectralArgs &sp, cudaStream_t s);
+                                  const SpectralArgs &sp, cudaStream_t s, int tile = 0);
 cudaError_t launch_step(const StepArgs &a, int grid, cudaStream_t s);
 // The same step as three ordinary launches (modes 2, 3, 4): no grid barrier,
 // safe beside long-running kernels of other streams.
