@@ -346,6 +346,14 @@ struct eplace_ctx {
   // of any result): grid caps of the WA and scatter kernels in blocks per
   // SM, and the SIMT GEMM tile of each of the four transform GEMMs.
   int wa_blocks_per_sm = 16, sc_blocks_per_sm = 16;
+  // Initial placement computed during a load for the seed the caller will
+  // run with (one-shot eplace_place); the next run with that seed takes it
+  // and clears it, every other run computes its own.
+  bool pre_ip = false;
+  uint64_t pre_seed = 0;
+  std::vector<int32_t> pre_isx, pre_isy;
+  eplace_status pre_st = EPLACE_OK;
+  std::string pre_msg;
   int gemm_tile[4] = {0, 0, 0, 0};
   WaClass wa_cls[kWaClasses] = {};  // degree classes of the sorted CSR
   int wa_warps = 0;
@@ -1102,7 +1110,7 @@ void launch_gpu_legal(eplace_ctx *c, LegalSlot &L) {
 // (capacity reuse: no frees, which would synchronise the device); the DCT
 // matrices and the tensor-core operands are rebuilt only when the bin grid
 // changes; every captured graph is invalidated.
-void load_into(eplace_ctx *c, HostProblem &&hp_in) {
+void load_into(eplace_ctx *c, HostProblem &&hp_in, const uint64_t *ip_seed = nullptr) {
   AllocOn on_stream(c->stream);
   const bool same_bins = c->mat_bx == hp_in.BX && c->mat_by == hp_in.BY;
   c->hp = std::move(hp_in);
@@ -1128,17 +1136,25 @@ void load_into(eplace_ctx *c, HostProblem &&hp_in) {
     slots = build_wa_slots(soff, spins, cls);
   });
   int grad_k = 24;
+  c->pre_ip = false;
   std::thread t_pw([&] {
     pin_weights(hp, c->pw_host);
     grad_k = grad_scale_log2(hp);
   });
+  std::thread t_ip;
+  if (ip_seed)
+    t_ip = std::thread([&] {
+      c->pre_st = initial_placement(hp, *ip_seed, c->pre_isx, c->pre_isy, c->pre_msg);
+      c->pre_seed = *ip_seed;
+    });
   struct Joiner {  // joins the helpers on every exit, an upload error included
-    std::thread &a, &b;
+    std::thread &a, &b, &d;
     ~Joiner() {
       if (a.joinable()) a.join();
       if (b.joinable()) b.join();
+      if (d.joinable()) d.join();
     }
-  } joiner{t_wa, t_pw};
+  } joiner{t_wa, t_pw, t_ip};
   c->net_off.ensure(hp.net_off.size());
   c->net_off.upload(hp.net_off.data(), hp.net_off.size(), s);
   c->pin_cell.ensure(std::max<size_t>(hp.P, 1));
@@ -1223,6 +1239,10 @@ void load_into(eplace_ctx *c, HostProblem &&hp_in) {
   for (uint32_t f = 0; f < hp.F; ++f) floc[f] = make_int2(hp.fx[f], hp.fy[f]);
   if (hp.F) CK(cudaMemcpyAsync(c->loc.p + hp.N, floc.data(), sizeof(int2) * hp.F, cudaMemcpyHostToDevice, s));
   g_h2d += sizeof(int2) * hp.F;
+  if (t_ip.joinable()) {
+    t_ip.join();
+    c->pre_ip = true;
+  }
 }
 
 }  // namespace
@@ -1442,7 +1462,16 @@ struct JobState {
     gpu_legal = opts.legal_mode == EPLACE_LEGAL_GPU && legalize_supported(hp.W, hp.H);
     if (!res->bel_tile && hp.N) return final_st = EPLACE_ERR_INVALID;
     std::string msg;
-    eplace_status st = initial_placement(hp, cfg.seed, isx, isy, msg);
+    eplace_status st;
+    if (c->pre_ip && c->pre_seed == cfg.seed) {  // computed during the load, used once
+      st = c->pre_st;
+      msg = c->pre_msg;
+      isx = std::move(c->pre_isx);
+      isy = std::move(c->pre_isy);
+      c->pre_ip = false;
+    } else {
+      st = initial_placement(hp, cfg.seed, isx, isy, msg);
+    }
     mark("initial_placement");
     if (st != EPLACE_OK) {
       set_err(c, msg);
@@ -2112,13 +2141,13 @@ eplace_ctx *ctx_new(int32_t device, eplace_status *st) {
   return c.release();
 }
 
-eplace_status ctx_load_problem(eplace_ctx *c, HostProblem &&hp) {
+eplace_status ctx_load_problem(eplace_ctx *c, HostProblem &&hp, const uint64_t *ip_seed) {
   try {
     CK(cudaSetDevice(c->device));
     CK(cudaStreamSynchronize(c->stream));
     for (auto &l : c->lslots)
       if (l && l->stream) CK(cudaStreamSynchronize(l->stream));
-    load_into(c, std::move(hp));
+    load_into(c, std::move(hp), ip_seed);
     CK(cudaStreamSynchronize(c->stream));
   } catch (const CudaError &e) {
     return cuda_fail(c, e);
@@ -2184,7 +2213,8 @@ eplace_status eplace_place(const eplace_netlist *nl, const eplace_chip *chip, co
     c = ctx_new(device, &st);
     if (!c) return st;
   }
-  st = ctx_load_problem(c, std::move(hp));
+  const uint64_t ip_seed = cfg ? cfg->seed : 1;
+  st = ctx_load_problem(c, std::move(hp), &ip_seed);
   if (st != EPLACE_OK) {
     g_thread_error = c->err;
     eplace_ctx_destroy(c);

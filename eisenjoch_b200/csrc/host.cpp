@@ -122,9 +122,28 @@ eplace_status initial_placement(const HostProblem &hp, uint64_t seed, std::vecto
   for (int64_t t = 0; t < nsites; ++t)
     if (!occ[(size_t)t]) avail.push_back((int32_t)t);
   uint64_t rng = seed ? seed : 1;
-  for (size_t i = avail.size(); i-- > 1;) {
-    size_t j = (uint32_t)xorshift64(rng) % (uint32_t)(i + 1);
-    std::swap(avail[i], avail[j]);
+  // Fisher-Yates from the end, j = (u32)rng % (i + 1).  The random stream
+  // does not depend on the array, so the j of step i - D is drawn D steps
+  // early and its element prefetched: the same swaps, with the cache misses
+  // of the random accesses overlapped.
+  {
+    constexpr int D = 16;
+    const size_t n = avail.size();
+    uint32_t jq[D];
+    for (int k = 0; k < D && (size_t)k + 1 < n; ++k) {
+      jq[k] = (uint32_t)xorshift64(rng) % (uint32_t)(n - k);  // step i = n - 1 - k
+      __builtin_prefetch(&avail[jq[k]], 1);
+    }
+    int head = 0;
+    for (size_t i = n; i-- > 1;) {
+      const uint32_t j = jq[head];
+      if (i >= (size_t)D + 1) {  // draw for step i - D
+        jq[head] = (uint32_t)xorshift64(rng) % (uint32_t)(i - D + 1);
+        __builtin_prefetch(&avail[jq[head]], 1);
+      }
+      head = (head + 1) % D;
+      std::swap(avail[i], avail[j]);
+    }
   }
   if (unbound > avail.size()) {
     msg = "logic (need " + std::to_string(unbound) + " BELs but only " + std::to_string(avail.size()) +
