@@ -358,3 +358,34 @@ def test_ctx_load_equals_fresh_context():
             assert a.trajectory == b.trajectory
     finally:
         ctx.close()
+
+
+def test_wa_gradient_every_degree_class():
+    """Nets at both edges of every degree class of the WA kernel (one thread
+    per net up to a warp per net, and the three-pass loop beyond 224 pins),
+    pads on some nets, and one cell on 150 nets (which lowers the packed
+    gradient's fixed-point scale): parity with the FP64 oracle."""
+    rng = np.random.default_rng(31)
+    n, nf, w = 3000, 60, 96
+    degrees = [1, 2, 3, 4, 5, 8, 9, 16, 17, 32, 33, 64, 65, 128, 129, 224, 225, 600] * 6
+    off, pins = [0], []
+    for k, d in enumerate(degrees):
+        net = rng.choice(n + nf, size=d, replace=False)
+        if k < 150 and 7 not in net:
+            net[-1] = 7  # cell 7 joins 150 nets
+        pins.extend(int(p) for p in net)
+        off.append(len(pins))
+    fx = rng.integers(0, w, nf).astype(np.int32)
+    fy = rng.integers(0, w, nf).astype(np.int32)
+    nl = E.Netlist(num_cells=n, net_offsets=np.array(off, np.uint32), pin_cell=np.array(pins, np.uint32),
+                   fixed_x=fx, fixed_y=fy)
+    chip = E.Chip(w, w)
+    orc = Oracle(nl, chip)
+    with E.PlacementContext(nl, chip) as ctx:
+        for seed, coeff in ((3, 0.5), (4, 0.1)):
+            r = np.random.default_rng(seed)
+            x = r.uniform(0, w - 1, n).astype(np.float32)
+            y = r.uniform(0, w - 1, n).astype(np.float32)
+            gx, gy = ctx.wa_grad(x, y, coeff)
+            rx, ry = orc.wa_gradient(x, y, coeff)
+            assert rel_err(gx, rx) <= 1e-4 and rel_err(gy, ry) <= 1e-4, coeff
