@@ -728,6 +728,8 @@ void setup_tc(eplace_ctx *c) {
     m.a_lo = make_map(al.p, mrows, k, 128);
     m.b_hi = make_map(bh.p, nrows, k, kTcBN);
     m.b_lo = make_map(bl.p, nrows, k, kTcBN);
+    m.b_hi32 = make_map(bh.p, nrows, k, 32);
+    m.b_lo32 = make_map(bl.p, nrows, k, 32);
     return m;
   };
   // GEMM1  T   = rho * B1          A = rho (H x W),  B^T = B1t (W x W)

@@ -176,8 +176,8 @@ __global__ void __launch_bounds__(128, 1)
       mbar_expect_tx(&full[s], S::STAGE_BYTES);
       tma_load_2d(st, &om.a_hi, kb * BK, m0, &full[s]);
       tma_load_2d(st + S::A_BYTES, &om.a_lo, kb * BK, m0, &full[s]);
-      tma_load_2d(st + 2 * S::A_BYTES, &om.b_hi, kb * BK, n0, &full[s]);
-      tma_load_2d(st + 2 * S::A_BYTES + S::B_BYTES, &om.b_lo, kb * BK, n0, &full[s]);
+      tma_load_2d(st + 2 * S::A_BYTES, BN == 32 ? &om.b_hi32 : &om.b_hi, kb * BK, n0, &full[s]);
+      tma_load_2d(st + 2 * S::A_BYTES + S::B_BYTES, BN == 32 ? &om.b_lo32 : &om.b_lo, kb * BK, n0, &full[s]);
     }
   } else if (threadIdx.x == 32) {
     // MMA issuer: M = 128, N = BN, BF16 x BF16 -> FP32, both K-major.
@@ -284,20 +284,36 @@ __global__ void __launch_bounds__(128, 1)
 
 bool tc_shape_ok(int M, int N, int K) { return M % BM == 0 && N % kTcBN == 0 && K % BK == 0 && M > 0; }
 
-cudaError_t launch_tc_gemm(const TcGemmMaps &maps, const TcGemmEpi &epi, int nbatch, int M, int N, int K,
-                           cudaStream_t s) {
-  constexpr int STAGES = 4;
-  using S = Smem<kTcBN, STAGES>;
+template <int BN, int STAGES>
+cudaError_t launch_cfg(const TcGemmMaps &maps, const TcGemmEpi &epi, int nbatch, int M, int N, int K,
+                       cudaStream_t s) {
+  using S = Smem<BN, STAGES>;
   static bool attr = false;
   if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(k_tc_gemm<kTcBN, STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = cudaFuncSetAttribute(k_tc_gemm<BN, STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          S::TOTAL);
     if (e != cudaSuccess) return e;
     attr = true;
   }
-  dim3 grid(N / kTcBN, M / BM, nbatch);
-  k_tc_gemm<kTcBN, STAGES><<<grid, 128, S::TOTAL, s>>>(maps, epi, M, N, K);
+  dim3 grid(N / BN, M / BM, nbatch);
+  k_tc_gemm<BN, STAGES><<<grid, 128, S::TOTAL, s>>>(maps, epi, M, N, K);
   return cudaGetLastError();
+}
+
+// Tile shape by grid size (measured on 512^2 and 1024^2 bin grids): a grid
+// of 128 x 64 tiles that covers at most half the SMs takes 128 x 32 tiles
+// (twice the CTAs); one that would need a second wave takes two smaller
+// rings (2 stages, 97 KB) so that two CTAs share an SM and one's epilogue
+// overlaps the other's main loop; in between, 128 x 64 with a 4-deep ring.
+// Each output sums its K steps in the same order whatever the tile.
+cudaError_t launch_tc_gemm(const TcGemmMaps &maps, const TcGemmEpi &epi, int nbatch, int M, int N, int K,
+                           cudaStream_t s) {
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const long ctas = (long)(N / kTcBN) * (M / BM) * nbatch;
+  if (2 * ctas <= sms) return launch_cfg<32, 4>(maps, epi, nbatch, M, N, K, s);
+  if (ctas > sms) return launch_cfg<64, 2>(maps, epi, nbatch, M, N, K, s);
+  return launch_cfg<64, 4>(maps, epi, nbatch, M, N, K, s);
 }
 
 }  // namespace eplace

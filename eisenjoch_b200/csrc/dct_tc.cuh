@@ -7,11 +7,12 @@
 
 namespace eplace {
 
-constexpr int kTcBN = 64;  // CTA tile N (M is 128)
+constexpr int kTcBN = 64;  // widest CTA tile N (M is 128); N must be a multiple of it
 
-// TMA maps of one GEMM's operands: A (M x K) and B^T (N x K), hi and lo.
+// TMA maps of one GEMM's operands: A (M x K) and B^T (N x K), hi and lo; the
+// B maps twice, for the 64- and the 32-column tile.
 struct TcOperandMaps {
-  CUtensorMap a_hi, a_lo, b_hi, b_lo;
+  CUtensorMap a_hi, a_lo, b_hi, b_lo, b_hi32, b_lo32;
 };
 
 // Up to two GEMMs of the same shape in one launch (blockIdx.z).
