@@ -237,7 +237,7 @@ __global__ void __launch_bounds__(128, 1)
         const int ky = r;
         const float gy2 = epi.gy2[ky], wy = epi.wy[ky];
         const float sy = (ky == 0) ? 0.5f * epi.scale : epi.scale;
-#pragma unroll 1
+#pragma unroll  // constant indices into v[]: it stays in registers
         for (int j = 0; j < 32; j += 8) {
           uint32_t exh[4], exl[4], eyh[4], eyl[4];
 #pragma unroll
