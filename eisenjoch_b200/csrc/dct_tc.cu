@@ -21,6 +21,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 
 #include "dct_tc.cuh"
@@ -288,12 +289,15 @@ template <int BN, int STAGES>
 cudaError_t launch_cfg(const TcGemmMaps &maps, const TcGemmEpi &epi, int nbatch, int M, int N, int K,
                        cudaStream_t s) {
   using S = Smem<BN, STAGES>;
-  static bool attr = false;
-  if (!attr) {
+  // The shared-memory opt-in is per device: set it once on each.
+  static std::atomic<bool> attr[64];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  if (!attr[dev].load(std::memory_order_acquire)) {
     cudaError_t e = cudaFuncSetAttribute(k_tc_gemm<BN, STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          S::TOTAL);
     if (e != cudaSuccess) return e;
-    attr = true;
+    attr[dev].store(true, std::memory_order_release);
   }
   dim3 grid(N / BN, M / BM, nbatch);
   k_tc_gemm<BN, STAGES><<<grid, 128, S::TOTAL, s>>>(maps, epi, M, N, K);
