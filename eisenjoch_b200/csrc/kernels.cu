@@ -711,16 +711,29 @@ __device__ __forceinline__ float2 gather_cell(const StepArgs &a, uint32_t i, flo
   const Foot f = make_foot(p, hf.x, hf.y, a.BX, a.BY, a.inv_sx, a.inv_sy);
   float fx = 0.f, fy = 0.f, wt = 0.f;
   if (hf.x == 0.5f && hf.y == 0.5f) return gather_unit_foot(a, f);
+  // Bins of a row in chunks of 8 with all field loads of a chunk issued
+  // before the sums (a macro spans up to 9 bins per axis), so a footprint
+  // costs one memory latency per row and chunk instead of one per bin; the
+  // sums keep the row-major bin order.
   for (int by = f.by0; by < f.by1; ++by) {
     const float oy = overlap_1d(f.ylo, f.yhi, by, a.sy);
-    for (int bx = f.bx0; bx < f.bx1; ++bx) {
-      const float w = overlap_1d(f.xlo, f.xhi, bx, a.sx) * oy;
-      if (w > 0.0f) {
-        const size_t idx = (size_t)by * a.BX + bx;
-        fx = fmaf(w, a.Ex[idx], fx);
-        fy = fmaf(w, a.Ey[idx], fy);
-        wt += w;
+    for (int b0 = f.bx0; b0 < f.bx1; b0 += 8) {
+      float w[8], e[8], h[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const int bx = b0 + k;
+        w[k] = (bx < f.bx1) ? overlap_1d(f.xlo, f.xhi, bx, a.sx) * oy : 0.0f;
+        const size_t idx = (size_t)by * a.BX + (w[k] > 0.0f ? bx : 0);
+        e[k] = (w[k] > 0.0f) ? a.Ex[idx] : 0.0f;
+        h[k] = (w[k] > 0.0f) ? a.Ey[idx] : 0.0f;
       }
+#pragma unroll
+      for (int k = 0; k < 8; ++k)
+        if (w[k] > 0.0f) {
+          fx = fmaf(w[k], e[k], fx);
+          fy = fmaf(w[k], h[k], fy);
+          wt += w[k];
+        }
     }
   }
   float2 g = make_float2(0.f, 0.f);
