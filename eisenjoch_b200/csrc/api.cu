@@ -834,7 +834,10 @@ void launch_field_stage(eplace_ctx *c, float *phi, int field_mode, bool tc = fal
 // choice only moves time.  Results are kept per process for a shape class
 // (cells and pins to the next power of two, bin grid, transform) and reused
 // by every context of that class.  Runs after reset_state (positions are the
-// initial placement), and clears the accumulators it dirtied.
+// initial placement), and clears the accumulators it dirtied.  A context on a
+// shared device (the job engine) keeps the default shapes: timings taken
+// beside other jobs' kernels do not rank the candidates, and the host
+// legaliser, not the kernels, bounds the engine's rate.
 struct TuneKey {
   int n2, p2, bx, by, tc;
   bool operator<(const TuneKey &o) const {
@@ -846,6 +849,12 @@ struct TuneVal {
 };
 
 void autotune_launches(eplace_ctx *c, float gamma, int field_mode, bool tc) {
+  if (c->shared_device) {
+    c->wa_blocks_per_sm = 16;
+    c->sc_blocks_per_sm = 16;
+    std::fill(c->gemm_tile, c->gemm_tile + 4, 0);
+    return;
+  }
   static std::mutex mu;
   static std::map<TuneKey, TuneVal> *cache = new std::map<TuneKey, TuneVal>();  // process lifetime
   const HostProblem &hp = c->hp;
