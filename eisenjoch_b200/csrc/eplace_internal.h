@@ -11,6 +11,10 @@
 #include <thread>
 #include <vector>
 
+#include <sys/resource.h>
+#include <sys/syscall.h>
+#include <unistd.h>
+
 #include "../../include/eplace.h"
 
 namespace eplace {
@@ -87,11 +91,18 @@ eplace_status synth(const eplace_synth_spec &spec, eplace_synth_info *info, uint
                     uint32_t *pin_cell);
 
 // FIFO worker pool of the host legaliser; one pool may serve many placement
-// jobs (the job engine shares one across its contexts).
+// jobs (the job engine shares one across its contexts).  With nice > 0 the
+// workers run below the priority of the threads that feed the device (the
+// job engine's scheduler and loaders), which then never wait behind a full
+// set of legalisations for a core.
 class Pool {
  public:
-  explicit Pool(int n) {
-    for (int i = 0; i < n; ++i) th_.emplace_back([this, i] { loop(i); });
+  explicit Pool(int n, int nice = 0) {
+    for (int i = 0; i < n; ++i)
+      th_.emplace_back([this, i, nice] {
+        if (nice > 0) setpriority(PRIO_PROCESS, (id_t)syscall(SYS_gettid), nice);  // this thread only (Linux)
+        loop(i);
+      });
   }
   ~Pool() {
     {

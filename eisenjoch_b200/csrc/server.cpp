@@ -323,7 +323,7 @@ eplace_status eplace_server_create(const eplace_server_cfg *cfg, eplace_server *
     s->budget = fr / 2;
   }
   const int nt = s->cfg.legal_threads > 0 ? s->cfg.legal_threads : (int)std::max(1u, std::thread::hardware_concurrency());
-  s->pool.reset(new Pool(std::min(nt, 64)));
+  s->pool.reset(new Pool(std::min(nt, 64), 5));
   s->loaders.reset(new Pool(4));
   eplace_server *raw = s.get();
   s->sched = std::thread([raw] { raw->loop(); });
