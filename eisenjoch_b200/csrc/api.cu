@@ -310,6 +310,13 @@ struct eplace_ctx {
   std::vector<std::unique_ptr<PinBuf<DevScalars>>> scs;
   std::vector<cudaEvent_t> slot_ev;
   size_t slot_log_cap = 0;
+  // Device copies of an interval's positions and scalars, one per slot: the
+  // loop's stream writes them (device to device, microseconds) and the copy
+  // stream moves them to the host while the next interval computes.
+  cudaStream_t copy = nullptr;
+  std::vector<std::unique_ptr<DBuf<float2>>> snap_pos;
+  std::vector<std::unique_ptr<DBuf<DevScalars>>> snap_sc;
+  std::vector<cudaEvent_t> snap_ev;
   cudaGraphExec_t gexec = nullptr;
   bool g_valid = false;  // gexec matches the current buffers and settings
   uint64_t g_epoch = 0, g_interval = 0;
@@ -364,12 +371,15 @@ struct eplace_ctx {
 
   ~eplace_ctx() {
     if (stream) cudaStreamSynchronize(stream);
+    if (copy) cudaStreamSynchronize(copy);
     for (auto &l : lslots)
       if (l && l->stream) cudaStreamSynchronize(l->stream);
     lslots.clear();
     pool.reset();
     if (gexec) cudaGraphExecDestroy(gexec);
     for (auto e : slot_ev) cudaEventDestroy(e);
+    for (auto e : snap_ev) cudaEventDestroy(e);
+    if (copy) cudaStreamDestroy(copy);
     if (side) cudaStreamSynchronize(side);
     if (ev_fork) cudaEventDestroy(ev_fork);
     if (ev_join) cudaEventDestroy(ev_join);
@@ -1554,6 +1564,23 @@ struct JobState {
           c->slot_ev.push_back(e);
         }
       }
+      {
+        // Device staging of the slots (stream-ordered on the loop's stream);
+        // no copy of an earlier run still reads them.
+        AllocOn on_stream(s);
+        CK(cudaStreamSynchronize(c->copy));
+        while ((int)c->snap_sc.size() < inflight) {
+          c->snap_pos.emplace_back(new DBuf<float2>());
+          c->snap_sc.emplace_back(new DBuf<DevScalars>());
+          cudaEvent_t e;
+          CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+          c->snap_ev.push_back(e);
+        }
+        for (int i = 0; i < inflight; ++i) {
+          if (!gpu_legal) c->snap_pos[i]->ensure(hp.N);
+          c->snap_sc[i]->ensure(1);
+        }
+      }
       if (!gpu_legal) {
         // Snapshots for the intervals in flight and a few legalisations:
         // pinned allocations here rather than while the loop runs.
@@ -1823,13 +1850,22 @@ struct JobState {
         cps.push_back(std::move(cp));
       } else {
         hs = take_snap();
-        CK(cudaMemcpyAsync(hs->pos, c->x.p, sizeof(float2) * hp.N, cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(c->snap_pos[slot]->p, c->x.p, sizeof(float2) * hp.N, cudaMemcpyDeviceToDevice, s));
+      }
+      // The interval's outputs leave on the copy stream: positions and
+      // scalars from the slot's device copy (the loop overwrites its own),
+      // the log entries from their own places (each iteration has one).
+      CK(cudaMemcpyAsync(c->snap_sc[slot]->p, c->sc.p, sizeof(DevScalars), cudaMemcpyDeviceToDevice, s));
+      CK(cudaEventRecord(c->snap_ev[slot], s));
+      CK(cudaStreamWaitEvent(c->copy, c->snap_ev[slot], 0));
+      if (hs) {
+        CK(cudaMemcpyAsync(hs->pos, c->snap_pos[slot]->p, sizeof(float2) * hp.N, cudaMemcpyDeviceToHost, c->copy));
         g_d2h += sizeof(float2) * hp.N;
       }
-      CK(cudaMemcpyAsync(logs[slot]->p, c->log.p + ch.first, sizeof(IterLog) * n, cudaMemcpyDeviceToHost, s));
-      CK(cudaMemcpyAsync(scs[slot]->p, c->sc.p, sizeof(DevScalars), cudaMemcpyDeviceToHost, s));
+      CK(cudaMemcpyAsync(logs[slot]->p, c->log.p + ch.first, sizeof(IterLog) * n, cudaMemcpyDeviceToHost, c->copy));
+      CK(cudaMemcpyAsync(scs[slot]->p, c->snap_sc[slot]->p, sizeof(DevScalars), cudaMemcpyDeviceToHost, c->copy));
       g_d2h += sizeof(IterLog) * n + sizeof(DevScalars);
-      CK(cudaEventRecord(evs[slot], s));
+      CK(cudaEventRecord(evs[slot], c->copy));
       pending.push_back({next_chunk, slot, hs});
       ++next_chunk;
       progressed = true;
@@ -2065,7 +2101,7 @@ uint64_t problem_device_bytes(const HostProblem &hp) {
   const uint64_t N = hp.N, F = hp.F, NN = hp.NN, P = hp.P;
   const uint64_t nb = (uint64_t)hp.BX * hp.BY;
   const uint64_t m = (uint64_t)hp.BX * hp.BX + (uint64_t)hp.BY * hp.BY;
-  return N * 96 + F * 16 + P * 8 + NN * 16 + nb * 64 + m * 48 + (1u << 20);
+  return N * 120 + F * 16 + P * 8 + NN * 16 + nb * 64 + m * 48 + (1u << 20);
 }
 
 namespace {
@@ -2137,6 +2173,7 @@ eplace_ctx *ctx_new(int32_t device, eplace_status *st) {
     CK(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
     CK(cudaStreamCreateWithPriority(&c->stream, cudaStreamNonBlocking, prio_hi));
     CK(cudaStreamCreateWithPriority(&c->side, cudaStreamNonBlocking, prio_hi));
+    CK(cudaStreamCreateWithFlags(&c->copy, cudaStreamNonBlocking));
     CK(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming));
     CK(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device));
@@ -2177,6 +2214,8 @@ uint64_t eplace_ctx::device_bytes() const {
   add(mB1); add(mL2); add(mB3); add(mL4); add(mB5); add(mL6); add(mB3g); add(mL6g);
   add(wx); add(gx2); add(wy); add(gy2); add(ops); add(mom); add(part); add(part2); add(part_b);
   add(sc); add(log); add(bar); add(loc); add(hp_total);
+  for (const auto &d : snap_pos) add(*d);
+  for (const auto &d : snap_sc) add(*d);
   add(rho_h); add(rho_l); add(Tt_h); add(Tt_l); add(Exh_h); add(Exh_l); add(Eyh_h); add(Eyh_l);
   add(Ut_h); add(Ut_l); add(Vt_h); add(Vt_l); add(B1t_h); add(B1t_l); add(L2_h); add(L2_l);
   add(B3t_h); add(B3t_l); add(B5t_h); add(B5t_l); add(L4_h); add(L4_l); add(L6_h); add(L6_l);
