@@ -321,6 +321,7 @@ struct eplace_ctx {
   bool g_valid = false;  // gexec matches the current buffers and settings
   uint64_t g_epoch = 0, g_interval = 0;
   int g_field = -1;
+  int g_bx = -1, g_by = -1;  // bin grid gexec was instantiated for
   bool g_tc = false;
   float g_gamma = 0.f;
 
@@ -1638,7 +1639,14 @@ struct JobState {
     ok = ok && ce == cudaSuccess;
     // A stale executable graph of the same shape (same kernels, new
     // pointers and sizes) is updated in place, which is cheaper than a new
-    // instantiation.
+    // instantiation.  Only for the bin grid and transform it was made for:
+    // those decide which transform kernels run and how they launch (a
+    // split-K GEMM is a cluster launch, whose cluster shape an in-place
+    // update does not carry), so any other grid gets a new instantiation.
+    if (c->gexec && (c->g_bx != c->hp.BX || c->g_by != c->hp.BY || c->g_tc != tc)) {
+      cudaGraphExecDestroy(c->gexec);
+      c->gexec = nullptr;
+    }
     if (ok && c->gexec) {
       cudaGraphExecUpdateResultInfo info{};
       if (cudaGraphExecUpdate(c->gexec, graph, &info) != cudaSuccess) {
@@ -1668,6 +1676,8 @@ struct JobState {
     c->g_field = opts.field_mode;
     c->g_tc = tc;
     c->g_gamma = gamma;
+    c->g_bx = c->hp.BX;
+    c->g_by = c->hp.BY;
   }
 
   void launch_chunk(const Chunk &ch) {

@@ -496,14 +496,23 @@ __global__ void __launch_bounds__(kFinalBlock) k_density_final(const FinalArgs a
 // ---------------------------------------------------------------------------
 constexpr int GK = 16;
 
-template <bool SPECTRAL, int TM, int TN>
+// S > 1: split K over a cluster of S CTAs (cluster dims 1 x 1 x S along z).
+// CTA rank r sums k in [r K/S, (r+1) K/S) in order, parks its partial tile in
+// its shared memory, and after a cluster barrier adds the S partials of a
+// TM/S-row slice of the tile in rank order ((p0 + p1) + p2) + ... through
+// distributed shared memory, then runs the epilogue on that slice.  The
+// order is the same for both tile sizes, so they still give the same bits.
+template <bool SPECTRAL, int TM, int TN, int S>
 __global__ void __launch_bounds__((TM / 4) * (TN / 4)) k_sgemm(const GemmOp *ops, int M, int N, int K,
                                                                SpectralArgs sp) {
   constexpr int T = (TM / 4) * (TN / 4);
   constexpr int LA = TM * GK / (4 * T), LB = GK * TN / (4 * T);  // float4 loads per thread
-  const GemmOp op = ops[blockIdx.z];
-  __shared__ __align__(16) float As[2][GK][TM + 4];
-  __shared__ __align__(16) float Bs[2][GK][TN + 4];
+  static_assert(S == 1 || (TM % S == 0 && (TM / S) * (TN / 4) == T), "one float4 per thread in the split reduction");
+  const GemmOp op = ops[blockIdx.z / S];
+  __shared__ __align__(16) float smem[2 * GK * (TM + 4) + 2 * GK * (TN + 4)];
+  static_assert(S == 1 || TM * TN <= 2 * GK * (TM + 4) + 2 * GK * (TN + 4), "partial tile fits the staging buffers");
+  auto As = reinterpret_cast<float(*)[GK][TM + 4]>(smem);
+  auto Bs = reinterpret_cast<float(*)[GK][TN + 4]>(smem + 2 * GK * (TM + 4));
   const int tid = threadIdx.x, tx = tid % (TN / 4), ty = tid / (TN / 4);
   const int bm = blockIdx.y * TM, bn = blockIdx.x * TN;
   const bool vec = ((K & 3) == 0) && ((N & 3) == 0);
@@ -554,13 +563,17 @@ __global__ void __launch_bounds__((TM / 4) * (TN / 4)) k_sgemm(const GemmOp *ops
   for (int i = 0; i < 4; ++i)
 #pragma unroll
     for (int j = 0; j < 4; ++j) acc[i][j] = 0.0f;
-  const int nk = (K + GK - 1) / GK;
-  load(0);
+  // This CTA's k range (all of K when S == 1; the launcher splits only when
+  // S * GK divides K).
+  const int kpart = (S == 1) ? K : K / S;
+  const int kbeg = (S == 1) ? 0 : (int)(blockIdx.z % S) * kpart;
+  const int nk = (kpart + GK - 1) / GK;
+  load(kbeg);
   store(0);
   __syncthreads();
   for (int kt = 0; kt < nk; ++kt) {
     const int cur = kt & 1;
-    if (kt + 1 < nk) load((kt + 1) * GK);
+    if (kt + 1 < nk) load(kbeg + (kt + 1) * GK);
 #pragma unroll
     for (int kk = 0; kk < GK; ++kk) {
       const float4 a4 = *reinterpret_cast<const float4 *>(&As[cur][kk][ty * 4]);
@@ -575,6 +588,56 @@ __global__ void __launch_bounds__((TM / 4) * (TN / 4)) k_sgemm(const GemmOp *ops
       store(cur ^ 1);
       __syncthreads();
     }
+  }
+  if constexpr (S > 1) {
+    namespace cg = cooperative_groups;
+    cg::cluster_group cluster = cg::this_cluster();
+    __syncthreads();  // the staging buffers become the partial tile
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+      *reinterpret_cast<float4 *>(&smem[(ty * 4 + i) * TN + tx * 4]) =
+          make_float4(acc[i][0], acc[i][1], acc[i][2], acc[i][3]);
+    cluster.sync();
+    const int rank = (int)cluster.block_rank();
+    const int lr = rank * (TM / S) + tid / (TN / 4), lc = (tid % (TN / 4)) * 4;
+    float4 v = *reinterpret_cast<const float4 *>(cluster.map_shared_rank(&smem[lr * TN + lc], 0));
+#pragma unroll
+    for (int q = 1; q < S; ++q) {
+      const float4 w = *reinterpret_cast<const float4 *>(cluster.map_shared_rank(&smem[lr * TN + lc], q));
+      v.x += w.x;
+      v.y += w.y;
+      v.z += w.z;
+      v.w += w.w;
+    }
+    const float vv[4] = {v.x, v.y, v.z, v.w};
+    const int r = bm + lr;
+    if (r < M) {
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int cidx = bn + lc + j;
+        if (cidx >= N) continue;
+        const size_t o = (size_t)r * N + cidx;
+        if (SPECTRAL) {
+          float s = sp.scale;
+          if (cidx == 0) s *= 0.5f;
+          if (r == 0) s *= 0.5f;
+          const float den = sp.gx2[cidx] + sp.gy2[r];
+          float phi = 0.0f, ex = 0.0f, ey = 0.0f;
+          if (!(den < 1e-30f)) {
+            phi = vv[j] * s / den;
+            ex = phi * sp.wx[cidx];
+            ey = phi * sp.wy[r];
+          }
+          op.C[o] = ex;
+          op.C2[o] = ey;
+          if (sp.phi) sp.phi[o] = phi;
+        } else {
+          op.C[o] = vv[j];
+        }
+      }
+    }
+    cluster.sync();  // no CTA leaves while another reads its partial tile
+    return;
   }
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
@@ -624,8 +687,8 @@ int device_sms() {
 // The small tile when the 64 x 64 grid would leave more than half the SMs
 // without a CTA (measured: 64 CTAs of 512^3 gain from the small tile, 128
 // CTAs do not).
-bool sgemm_small_tile(int M, int N, int nb) {
-  const long ctas = (long)((N + 63) / 64) * ((M + 63) / 64) * nb;
+bool sgemm_small_tile(int M, int N, int nb, int K) {
+  const long ctas = (long)((N + 63) / 64) * ((M + 63) / 64) * nb * (K % 64 == 0 ? 4 : 1);  // split K: 4 CTAs a tile
   return 2L * ctas < device_sms();
 }
 
@@ -1013,23 +1076,46 @@ cudaError_t launch_density_final(const FinalArgs &a_in, int grid, cudaStream_t s
   return cudaGetLastError();
 }
 
-cudaError_t launch_sgemm(const GemmOp *ops, int nb, int M, int N, int K, cudaStream_t s, int tile) {
-  if (tile == 32 || (tile == 0 && sgemm_small_tile(M, N, nb))) {
-    k_sgemm<false, 32, 32><<<dim3((N + 31) / 32, (M + 31) / 32, nb), 64, 0, s>>>(ops, M, N, K, SpectralArgs{});
-  } else {
-    k_sgemm<false, 64, 64><<<dim3((N + 63) / 64, (M + 63) / 64, nb), 256, 0, s>>>(ops, M, N, K, SpectralArgs{});
+// One SIMT GEMM launch: split K four ways over a cluster when 4 * GK
+// divides K (every transform of a power-of-two bin grid of at least 64),
+// else one CTA per tile.  Which form runs depends on K alone, never on the
+// tile, so the tile stays a choice of time only.
+constexpr int kSplitK = 4;
+
+template <bool SPECTRAL, int TM, int TN>
+cudaError_t sgemm_launch(const GemmOp *ops, int nb, int M, int N, int K, const SpectralArgs &sp, cudaStream_t s) {
+  const dim3 tiles((N + TN - 1) / TN, (M + TM - 1) / TM, nb);
+  constexpr int T = (TM / 4) * (TN / 4);
+  if (K % (kSplitK * GK) != 0) {
+    k_sgemm<SPECTRAL, TM, TN, 1><<<tiles, T, 0, s>>>(ops, M, N, K, sp);
+    return cudaGetLastError();
   }
-  return cudaGetLastError();
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(tiles.x, tiles.y, tiles.z * kSplitK);
+  cfg.blockDim = dim3(T);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = 1;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = kSplitK;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k_sgemm<SPECTRAL, TM, TN, kSplitK>, ops, M, N, K, sp);
+}
+
+cudaError_t launch_sgemm(const GemmOp *ops, int nb, int M, int N, int K, cudaStream_t s, int tile) {
+  if (tile == 32 || (tile == 0 && sgemm_small_tile(M, N, nb, K)))
+    return sgemm_launch<false, 32, 32>(ops, nb, M, N, K, SpectralArgs{}, s);
+  return sgemm_launch<false, 64, 64>(ops, nb, M, N, K, SpectralArgs{}, s);
 }
 
 cudaError_t launch_sgemm_spectral(const GemmOp *ops, int M, int N, int K, const SpectralArgs &sp,
                                   cudaStream_t s, int tile) {
-  if (tile == 32 || (tile == 0 && sgemm_small_tile(M, N, 1))) {
-    k_sgemm<true, 32, 32><<<dim3((N + 31) / 32, (M + 31) / 32, 1), 64, 0, s>>>(ops, M, N, K, sp);
-  } else {
-    k_sgemm<true, 64, 64><<<dim3((N + 63) / 64, (M + 63) / 64, 1), 256, 0, s>>>(ops, M, N, K, sp);
-  }
-  return cudaGetLastError();
+  if (tile == 32 || (tile == 0 && sgemm_small_tile(M, N, 1, K)))
+    return sgemm_launch<true, 32, 32>(ops, 1, M, N, K, sp, s);
+  return sgemm_launch<true, 64, 64>(ops, 1, M, N, K, sp, s);
 }
 
 int step_max_grid(int device) {

@@ -162,8 +162,10 @@ cudaError_t launch_wa(const WaArgs &a, int grid, cudaStream_t s);
 cudaError_t launch_scatter(const ScatterArgs &a, int grid, cudaStream_t s);
 cudaError_t launch_density_final(const FinalArgs &a, int grid, cudaStream_t s);
 // C[b] = A[b] (M x K) * B[b] (K x N), row-major FP32; batches from ops[0..nb).
-// tile: 64 or 32 (CTA tile edge), 0 = pick by grid size.  Both tiles sum
-// every output in the same order, so the choice never changes the bits.
+// tile: 64 or 32 (CTA tile edge), 0 = pick by grid size.  When 64 divides K
+// the sum is split into four K quarters (a cluster of four CTAs per tile)
+// added in quarter order; either way both tiles sum every output in the
+// same order, so the tile never changes the bits.
 cudaError_t launch_sgemm(const GemmOp *ops_dev, int nb, int M, int N, int K, cudaStream_t s, int tile = 0);
 // As above with the spectral epilogue: C = Ex_hat, C2 = Ey_hat.
 cudaError_t launch_sgemm_spectral(const GemmOp *ops_dev, int M, int N, int K,
