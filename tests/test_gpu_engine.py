@@ -57,6 +57,23 @@ def test_results_in_the_mix_equal_alone(designs, max_jobs):
         assert st["contexts"] <= max_jobs
 
 
+def test_context_reloaded_across_bin_grids_equals_fresh(designs):
+    """One context re-loaded with designs whose bin grids differ (64^2 ->
+    96^2 -> 64^2 -> 48^2) gives each design the result of a fresh context.
+    On 64-multiple grids the FP32 transform is a split-K cluster launch, on
+    the others a plain one; the interval graph of a context must be made
+    anew, not updated in place, when the grid changes."""
+    order = [0, 2, 1, 4]
+    with E.PlacementContext(designs[order[0]][0], designs[order[0]][1]) as c:
+        for k, d in enumerate(order):
+            nl, chip, _ = designs[d]
+            if k:
+                c.load(nl, chip)
+            got = c.run(CFG, OPTS)
+            with E.PlacementContext(nl, chip) as fresh:
+                same(got, fresh.run(CFG, OPTS))
+
+
 def test_admission_budget_runs_one_at_a_time(designs):
     # any two jobs exceed the budget; a job larger than the budget runs alone
     fp = min(E.footprint(nl, chip) for nl, chip, _ in designs)
