@@ -264,9 +264,19 @@ inline int32_t free_at_or_right(const uint64_t *row, const uint64_t *sum, int32_
 inline bool is_free(const uint64_t *fm, int32_t WR, int32_t x, int32_t y) {
   return (fm[(size_t)y * WR + (x >> 6)] >> (x & 63)) & 1;
 }
+// floor(t), exactly: truncate toward zero and step down for a negative
+// fraction (|t| < 2^62, the legaliser's coordinates); anything else goes to
+// std::floor.  Built for baseline x86-64, std::floor is a library call, and
+// the legaliser takes up to four per cell.
+inline double floor_exact(double t) {
+  if (!(t > -4.0e18 && t < 4.0e18)) return std::floor(t);
+  const double f = (double)(long long)t;
+  return f > t ? f - 1.0 : f;
+}
+
 // Nearest integer(s) to t in [0, n): one, or two when t is exactly k + 1/2.
 inline int nearest_ints(double t, int32_t n, int32_t (&out)[2]) {
-  double f = std::floor(t);
+  double f = floor_exact(t);
   int32_t lo = (int32_t)f;
   double fr = t - f;
   int k = 0;
@@ -314,9 +324,9 @@ eplace_status Legalizer::run(const float *x, const float *y, size_t stride, int3
             break;
           }
       if (best_t < 0) {
-        int32_t cy = (int32_t)std::floor(ty + 0.5);
+        int32_t cy = (int32_t)floor_exact(ty + 0.5);
         cy = std::min(std::max(cy, 0), H - 1);
-        const int32_t fx0 = (int32_t)std::floor(tx);
+        const int32_t fx0 = (int32_t)floor_exact(tx);
         // Per-row candidate cache: (lc, rc) are the nearest free sites left
         // of / right of an earlier query position in this row, with every
         // site strictly between them taken.  For any fx0 with
@@ -394,8 +404,8 @@ eplace_status Legalizer::run(const float *x, const float *y, size_t stride, int3
       const int32_t AW = W - w + 1, AH = H - h + 1;
       if (AW > 0 && AH > 0) {
         const double ux = tx - ox, uy = ty - oy;  // target anchor
-        const int32_t cy = std::min(std::max((int32_t)std::floor(uy + 0.5), 0), AH - 1);
-        const int32_t fa = std::min(std::max((int32_t)std::floor(ux), -1), AW - 1);
+        const int32_t cy = std::min(std::max((int32_t)floor_exact(uy + 0.5), 0), AH - 1);
+        const int32_t fa = std::min(std::max((int32_t)floor_exact(ux), -1), AW - 1);
         const int32_t lastw = (AW - 1) >> 6;
         auto valid_word = [&](int32_t ay, int32_t j) -> uint64_t {
           uint64_t m = ~0ull, mn = ~0ull;
