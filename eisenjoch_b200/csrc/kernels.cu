@@ -698,28 +698,28 @@ bool sgemm_small_tile(int M, int N, int nb, int K) {
 // kernel always terminates and the host reports EPLACE_ERR_TIMEOUT.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void grid_barrier(unsigned *bar, DevScalars *sc) {
+  // bar[0..1] is one 64-bit arrival count that is never reset inside a run:
+  // every launch on it has the same grid and passes whole barriers, so a
+  // launch starts at a multiple of gridDim.x, and barrier k of the run is
+  // complete when the count reaches (k + 1) * gridDim.x.  The last block's
+  // own add releases the others (no reset, no second word to publish).
+  // The host zeroes the count at every load and run start.
   __syncthreads();
   if (threadIdx.x == 0) {
-    unsigned gen;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(gen) : "l"(bar + 1) : "memory");
-    __threadfence();
-    const unsigned arrived = atomicAdd(bar, 1u);
-    if (arrived == gridDim.x - 1) {
-      atomicExch(bar, 0u);
-      __threadfence();
-      atomicAdd(bar + 1, 1u);
-    } else {
-      const long long t0 = clock64();
-      while (true) {
-        unsigned g;
-        asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(g) : "l"(bar + 1) : "memory");
-        if (g != gen) break;
-        if (clock64() - t0 > kSpinCycles) {
-          atomicExch(&sc->err, 1);
-          break;
-        }
-        __nanosleep(32);
+    unsigned long long *cnt = reinterpret_cast<unsigned long long *>(bar);
+    __threadfence();  // this block's writes before its arrival
+    const unsigned long long old = atomicAdd(cnt, 1ull);
+    const unsigned long long target = old - old % gridDim.x + gridDim.x;
+    const long long t0 = clock64();
+    while (true) {
+      unsigned long long v;
+      asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(cnt) : "memory");
+      if (v >= target) break;
+      if (clock64() - t0 > kSpinCycles) {
+        atomicExch(&sc->err, 1);
+        break;
       }
+      __nanosleep(32);
     }
     __threadfence();
   }

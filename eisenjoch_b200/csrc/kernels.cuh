@@ -143,7 +143,7 @@ struct StepArgs {
   double *part;             // [4 * grid]
   double *part2;            // [2 * grid] step-norm partials
   double *part_b;           // [4 * grid] pass-2 partials of the split form
-  unsigned *bar;            // grid barrier {count, generation}
+  unsigned *bar;            // grid barrier: words 0-1 are one 64-bit arrival count
   unsigned *ticket;
   int mode;                 // 0: full step (cooperative); 1: gather only (tmp_den <- density
                             // gradient); 2/3/4: phase A / penalty-init pass / phase C
