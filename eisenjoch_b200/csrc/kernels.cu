@@ -907,24 +907,30 @@ __global__ void __launch_bounds__(kStepBlock, 2) k_step(const StepArgs a) {
   double v[4] = {0.0, 0.0, 0.0, 0.0};
   if (a.mode == 0 || a.mode == 2) {
     // Phase A: gather, read + clear the WA accumulator, combine.  Two cells
-    // per thread and pass (i and i + gstride): every load of both is issued
+    // per thread and pass (i and i + ustride): every load of both is issued
     // before the first store, so their latencies overlap.  Macros (w*h > 1)
     // are skipped here and done afterwards from their own list, so a warp
     // of unit cells never waits for one macro's multi-bin gather.
-    for (uint32_t i0 = tid0; i0 < a.N; i0 += 2 * gstride) {
-      const uint32_t i1 = i0 + gstride;
-      const bool h1 = i1 < a.N;
-      const bool u0 = !a.mflag || !a.mflag[i0];
-      const bool u1 = h1 && (!a.mflag || !a.mflag[i1]);
-      CellA c0, c1;
-      if (u0) c0 = load_a(a, i0, was_init, true);
-      if (u1) c1 = load_a(a, i1, was_init, true);
-      if (u0) finish_a(a, i0, c0, was_init, lam, true, v);
-      if (u1) finish_a(a, i1, c1, was_init, lam, true, v);
-    }
-    // Macro k goes to thread gstride - 1 - k (mod gstride): the threads at
-    // the end of the grid hold the fewest unit cells when N is not a
-    // multiple of 2 * gstride.
+    // When the unit cells still fit one pass of pairs on the other threads,
+    // the last n_mac threads of the grid take macros only (macro k goes to
+    // thread gstride - 1 - k, mod gstride), so a macro's multi-row gather
+    // does not queue behind a unit cell in the same thread (200k cells:
+    // step 29.1 -> 26.9 us); otherwise (800k) every thread takes unit cells.
+    const uint32_t nm =
+        (a.n_mac <= gstride / 4 && (uint64_t)a.N <= 2ull * (gstride - a.n_mac)) ? a.n_mac : 0u;
+    const uint32_t ustride = gstride - nm;
+    if (tid0 < ustride)
+      for (uint32_t i0 = tid0; i0 < a.N; i0 += 2 * ustride) {
+        const uint32_t i1 = i0 + ustride;
+        const bool h1 = i1 < a.N;
+        const bool u0 = !a.mflag || !a.mflag[i0];
+        const bool u1 = h1 && (!a.mflag || !a.mflag[i1]);
+        CellA c0, c1;
+        if (u0) c0 = load_a(a, i0, was_init, true);
+        if (u1) c1 = load_a(a, i1, was_init, true);
+        if (u0) finish_a(a, i0, c0, was_init, lam, true, v);
+        if (u1) finish_a(a, i1, c1, was_init, lam, true, v);
+      }
     for (uint32_t k = gstride - 1 - tid0; k < a.n_mac; k += gstride) {
       const uint32_t i = a.mac_idx[k];
       const CellA c = load_a(a, i, was_init, false);
