@@ -19,8 +19,9 @@ bin map and global dot products), so N ranks run N independent replicas
 time ("weak" scaling).
 
 `--impl reference` times the reference algorithm's CPU form (the FP64 C
-restatement in oracle/, single thread, like the reference loop) on a bounded
-sample of the same workload and prints the same metric.
+restatement in oracle/, one thread per job like the reference loop) on whole
+jobs of the same workload, K jobs spread over all host cores, and prints the
+same metric.  It loads only oracle/liboracle.so.
 """
 
 import argparse
@@ -235,6 +236,100 @@ def precision_form_roofline(E, args, hbm, bf16, workload="electro_800k_2048"):
     return out
 
 
+def field_fp64(density, field_mode=1, target_density=1.0, device="cpu"):
+    """FP64 reference of the field solve (density.rs:96-166, with the
+    potential-gradient extension for field_mode 1) as dense DCT-matrix
+    products in torch float64: the yardstick for the precision report of the
+    two FP32-accumulating transforms.  Conventions (rustdct, unnormalised):
+    DCT-II C2[k,n] = cos(pi k (n+1/2)/N); DCT-III C3[k,n] = cos(pi n (k+1/2)/N)
+    with input 0 halved; DST-III S3[k,n] = sin(pi (n+1)(k+1/2)/N) with input
+    N-1 halved.  Returns (ex, ey, phi_hat) as [H, W] float64 tensors."""
+    import torch
+
+    d = torch.as_tensor(np.asarray(density, np.float64), device=device)
+    H, W = d.shape
+
+    def mats(N):
+        k = torch.arange(N, dtype=torch.float64, device=device)[:, None]
+        n = torch.arange(N, dtype=torch.float64, device=device)[None, :]
+        c2 = torch.cos(np.pi * k * (n + 0.5) / N)
+        c3 = torch.cos(np.pi * n * (k + 0.5) / N)
+        c3[:, 0] *= 0.5
+        s3 = torch.sin(np.pi * (n + 1) * (k + 0.5) / N)
+        s3[:, N - 1] *= 0.5
+        return c2, c3, s3
+
+    c2w, c3w, s3w = mats(W)
+    c2h, c3h, s3h = mats(H)
+    rho = d - target_density * max(float(d.mean()), 1e-30)
+    a = c2h @ (rho @ c2w.T)
+    a = a * (4.0 / (W * H))
+    a[:, 0] *= 0.5
+    a[0, :] *= 0.5
+    wx = (np.pi * torch.arange(W, dtype=torch.float64, device=device) / W)[None, :]
+    wy = (np.pi * torch.arange(H, dtype=torch.float64, device=device) / H)[:, None]
+    den = 2.0 * (1.0 - torch.cos(wx)) + 2.0 * (1.0 - torch.cos(wy))
+    phi = torch.where(den < 1e-30, torch.zeros_like(a), a / torch.where(den < 1e-30, torch.ones_like(den), den))
+    exh, eyh = phi * wx, phi * wy
+    if field_mode == 1:
+        exh = torch.cat([-exh[:, 1:], torch.zeros_like(exh[:, :1])], dim=1)
+        eyh = torch.cat([-eyh[1:, :], torch.zeros_like(eyh[:1, :])], dim=0)
+    ex = c3h @ (exh @ s3w.T)
+    ey = s3h @ (eyh @ c3w.T)
+    return ex, ey, phi
+
+
+def _rel(a, b):
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    s = np.abs(b).max()
+    return float(np.abs(a - b).max() / s) if s > 0 else float(np.abs(a).max())
+
+
+def precision_report(E, dev, workload="electro_800k_2048", state_iters=30):
+    """The precision form's report: field and potential-spectrum error of the
+    BF16x3 tensor-core transform and of the FP32 SIMT transform against an
+    FP64 solve of the same density map (taken from the workload's own run
+    after `state_iters` iterations), and the whole job in both transforms:
+    HPWL trajectory, final legalised HPWL and overflow, beside the FP64
+    oracle's committed run of the same job."""
+    import torch
+
+    nl, chip, cfg = E.workload(workload)
+    out = {"workload": workload, "fields": {}, "jobs": {}}
+    with E.PlacementContext(nl, chip, device=dev) as ctx:
+        c = E.ElectroPlaceCfg(**E.WORKLOADS[workload]["cfg"])
+        c.max_iters = state_iters
+        st = ctx.run(c, E.RunOptions(field_mode=1, dct_mode=0))
+        d, _ = ctx.density(st.x, st.y)
+        rex, rey, rphi = (t.cpu().numpy() for t in field_fp64(d, 1, cfg.target_density, "cuda:%d" % dev))
+        out["state"] = "density map of the best positions after %d iterations" % state_iters
+        for name, mode in (("bf16x3_tcgen05", 1), ("fp32_simt", 0)):
+            ex, ey, phi = ctx.field(d, dct_mode=mode, want_phi=True, field_mode=1)
+            out["fields"][name] = {"field_x_rel_err": _rel(ex, rex), "field_y_rel_err": _rel(ey, rey),
+                                   "potential_spectrum_rel_err": _rel(phi, rphi)}
+        for name, mode in (("bf16x3_tcgen05", 1), ("fp32_simt", 0)):
+            r = ctx.run(cfg, E.RunOptions(field_mode=1, dct_mode=mode))
+            out["jobs"][name] = {"iters": r.iters, "converged": r.converged, "overflow": r.overlap,
+                                 "final_hpwl": r.hpwl,
+                                 "trajectory": [[t["iter"], int(t["hpwl"]), round(t["overlap"], 5)]
+                                                for t in r.trajectory]}
+    gp = os.path.join(ROOT, "tests", "golden", "job_summaries.json")
+    key = workload + ":stable_wa"
+    if os.path.exists(gp):
+        with open(gp) as f:
+            g = json.load(f).get(key)
+        if g:
+            out["jobs"]["fp64_oracle"] = {
+                "iters": g["iters"], "converged": g["converged"], "final_hpwl": g["hpwl"],
+                "source": "tests/golden/job_summaries.json %s (committed FP64 CPU run)" % key,
+                "trajectory": [[c["iter"], int(c["hpwl"]), c["overlap"]] for c in g["checkpoints"]]}
+            for name in ("bf16x3_tcgen05", "fp32_simt"):
+                j = out["jobs"][name]
+                j["final_hpwl_vs_fp64"] = j["final_hpwl"] / g["hpwl"] - 1.0
+    out["error_definition"] = "max|x - x_fp64| / max|x_fp64| over the bin grid"
+    return out
+
+
 def ncu_traffic(kernel, workload):
     """dram bytes per launch from a committed ncu summary, if one exists."""
     p = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
@@ -396,64 +491,97 @@ def served_arm(args, dist, E, cfg, rate):
 
 
 # ---------------------------------------------------------------------------
-# CPU form (oracle restatement, single thread) on a bounded sample
+# CPU form of the reference loop (the FP64 C restatement in oracle/): whole
+# jobs, every checkpoint legalised, as place_electro runs them.  This part
+# loads oracle/liboracle.so only: the netlist comes from the oracle's own
+# copy of the generator and the workload table is read as data.
 # ---------------------------------------------------------------------------
-def cpu_sample(nl, chip, cfg, iters_per_job, checkpoints_per_job, field_mode=1):
-    """Times the FP64 CPU loop on this workload: k Nesterov iterations (no
-    intermediate legalisation) and one legalisation, and extrapolates to one
-    job of `iters_per_job` iterations with `checkpoints_per_job`
-    legalisations."""
-    from oracle.oracle import Oracle
+def _workload_table(name):
+    with open(os.path.join(ROOT, "eisenjoch_b200", "workloads.json")) as f:
+        w = json.load(f)[name]
+    spec = dict(bins_x=0, bins_y=0, cluster_size=32, locality=0.6, macro_fraction=0.0, macro_min=2, macro_max=8)
+    spec.update(w["spec"])
+    return spec, w["cfg"]
 
-    import copy
 
-    orc = Oracle(nl, chip)
-    c = copy.copy(cfg)
-    # 2 iterations: fixed costs (set-up, legalisation at iterations 0 and 1, final)
-    c.legalize_interval = 10 ** 9
-    c.max_iters = 2
+_ORACLE_JOB = {}
+
+
+def _oracle_problem(name):
+    """The workload's netlist on the oracle (generated once per process)."""
+    from types import SimpleNamespace
+
+    from oracle.oracle import Cfg, Oracle, synth
+
+    if name not in _ORACLE_JOB:
+        spec, cfg = _workload_table(name)
+        nl, chip = synth(SimpleNamespace(**spec))
+        _ORACLE_JOB[name] = (Oracle(nl, chip), Cfg(**cfg))
+    return _ORACLE_JOB[name]
+
+
+def _oracle_job(name, field_mode):
+    """One full placement job of workload `name` on the FP64 CPU form, in
+    this process (1 thread).  Returns (seconds, summary)."""
+    orc, cfg = _oracle_problem(name)
     t0 = time.perf_counter()
-    orc.place(c, field_mode=field_mode)
-    t2 = time.perf_counter() - t0
-    k = 4
-    c.max_iters = 2 + k
-    t0 = time.perf_counter()
-    orc.place(c, field_mode=field_mode)
-    tk = time.perf_counter() - t0
-    t_iter = max((tk - t2) / k, 1e-9)
-    # one legalisation of a spread-out state
-    st, sx, sy = orc.initial_placement(cfg.seed)
-    rng = np.random.default_rng(0)
-    x = np.clip(sx + rng.normal(0, 1.5, sx.size), 0, chip.width - 1)
-    y = np.clip(sy + rng.normal(0, 1.5, sy.size), 0, chip.height - 1)
-    t0 = time.perf_counter()
-    orc.legalize(x, y, 1)
-    t_leg = time.perf_counter() - t0
-    job = iters_per_job * t_iter + checkpoints_per_job * t_leg
-    sample = ("FP64 oracle loop, 1 thread: %d+%d iterations timed (%.3f s/iter), one ring-search legalisation "
-              "(%.3f s), extrapolated to %d iterations + %d legalisations per job" %
-              (2, k, t_iter, t_leg, iters_per_job, checkpoints_per_job))
-    return 1.0 / job, sample, t_iter, t_leg
+    st, r = orc.place(cfg, field_mode=field_mode)
+    dt = time.perf_counter() - t0
+    return dt, {"status": st, "iters": r["iters"], "converged": r["converged"], "hpwl": r["hpwl"]}
+
+
+def _oracle_pool_jobs(name, field_mode, count, workers):
+    """`count` full jobs on `workers` processes; returns (wall seconds of the
+    batch, per-job summaries)."""
+    import concurrent.futures as cf
+    import multiprocessing as mp
+
+    ctx = mp.get_context("spawn")
+    with cf.ProcessPoolExecutor(max_workers=workers, mp_context=ctx) as ex:
+        # every worker generates the netlist before the clock starts
+        list(ex.map(_prepare_worker, [(name, workers)] * workers))
+        t0 = time.perf_counter()
+        out = list(ex.map(_oracle_job, [name] * count, [field_mode] * count))
+        dt = time.perf_counter() - t0
+    return dt, [o for _, o in out]
+
+
+def _prepare_worker(arg):
+    name, _ = arg
+    _oracle_problem(name)
+    time.sleep(0.2)  # so that each worker takes one of the preparation tasks
+    return os.getpid()
+
+
+def cpu_baseline_one_job(name, field_mode):
+    """cpu_baseline: one whole job of the workload on one host thread."""
+    dt, r = _oracle_job(name, field_mode)
+    sample = ("one full job of %s on the FP64 CPU form (oracle/), 1 thread: %d iterations, every checkpoint "
+              "legalised, %.2f s" % (name, r["iters"], dt))
+    return 1.0 / dt, sample, r
 
 
 def reference_arm(args, dist):
+    """The reference loop's CPU form on the host cores: each step is one
+    whole job (initial placement, Nesterov iterations to overflow <= 0.10,
+    every checkpoint legalised, final legalisation), K jobs spread over all
+    host cores (one process per core, one job per process at a time);
+    value = K / wall time of the K jobs.  W untimed jobs first."""
     if dist.rank != 0:
         return
-    import eisenjoch_b200 as E
-
-    nl, chip, cfg = E.workload(args.workload)
     fm = 1 if args.field_mode == "potential_gradient" else 0
-    summary = load_job_summary(args.workload, fm)
-    iters = summary["iters"]
-    cps = iters // cfg.legalize_interval + 2
-    vals = []
-    sample = ""
+    spec, cfg = _workload_table(args.workload)
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
     t_start = time.perf_counter()
-    for i in range(args.warmup + args.steps):
-        v, sample, _, _ = cpu_sample(nl, chip, cfg, iters, cps, fm)
-        if i >= args.warmup:
-            vals.append(v)
-    value = statistics.mean(vals)
+    if args.warmup > 0:
+        _oracle_pool_jobs(args.workload, fm, args.warmup, min(cores, args.warmup))
+    workers = min(cores, args.steps)
+    dt, runs = _oracle_pool_jobs(args.workload, fm, args.steps, workers)
+    value = args.steps / dt
+    iters = sorted({r["iters"] for r in runs})
+    sample = ("%d whole jobs of %s (FP64 CPU form of the reference loop, oracle/), %d processes x 1 thread on %d "
+              "host cores; %s iterations per job, every checkpoint legalised; %.1f s wall" %
+              (args.steps, args.workload, workers, cores, "/".join(map(str, iters)), dt))
     line = {
         "impl": "reference",
         "metric": METRIC,
@@ -462,36 +590,23 @@ def reference_arm(args, dist):
         "n_gpus": args.gpus,
         "steps": args.steps,
         "warmup": args.warmup,
-        "ms_per_step": 1000.0 / value,
+        "ms_per_step": 1000.0 * dt / args.steps,
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic (seeded generator, benchmark shapes)",
-        "config": {"workload": args.workload, "cells": nl.num_cells, "nets": nl.num_nets, "pins": nl.num_pins,
-                   "bins": [chip.bins_x, chip.bins_y], "sites": [chip.width, chip.height],
-                   "iters_per_job": iters, "iters_source": summary["source"], "field_mode": args.field_mode},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port", "sample": sample},
+        "config": {"workload": args.workload, "cells": spec["num_cells"], "nets": spec["num_nets"],
+                   "pads": spec["num_pads"], "sites": [spec["width"], spec["height"]],
+                   "bins": [spec["bins_x"], spec["bins_y"]], "max_iters": cfg.get("max_iters", 500),
+                   "legalize_interval": cfg.get("legalize_interval", 5),
+                   "field_mode": args.field_mode, "parallelism": "%d processes" % workers},
+        "job": {"iters": runs[0]["iters"], "converged": runs[0]["converged"], "hpwl": runs[0]["hpwl"]},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": workers, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "wall_s": time.perf_counter() - t_start,
     }
     print(json.dumps(line), flush=True)
-
-
-def load_job_summary(workload, field_mode=1):
-    """Iterations to overflow <= 0.10 of this workload's job: the committed
-    FP64 oracle summary when present (tests/golden), else the benchmark
-    configuration's iteration cap."""
-    p = os.path.join(ROOT, "tests", "golden", "job_summaries.json")
-    if os.path.exists(p):
-        with open(p) as f:
-            d = json.load(f)
-        key = workload if field_mode == 1 else workload + ":reference_field"
-        if key in d:
-            return {"iters": int(d[key]["iters"]), "source": "FP64 oracle full run (tests/golden/job_summaries.json)"}
-    import eisenjoch_b200 as E
-
-    return {"iters": int(E.WORKLOADS[workload]["cfg"].get("max_iters", 500)), "source": "max_iters"}
 
 
 def replica_spec(spec, rank):
@@ -575,9 +690,10 @@ def ours(args, dist):
 
     # --- per-kernel roofline of the precision form (800k cells, 1024^2 bins,
     # BF16x3 transform): the configuration whose bytes exceed L2 ---
-    prec = None
+    prec = prec_report = None
     if not args.no_precision_form and dist.rank == 0:
         prec = precision_form_roofline(E, args, hbm, bf16)
+        prec_report = precision_report(E, dev)
 
     mixed_cfg = E.ElectroPlaceCfg(max_iters=500)
     batched = None if args.no_batched else batched_arm(args, dist, E, mixed_cfg)
@@ -616,8 +732,7 @@ def ours(args, dist):
 
     cpu = None
     if not args.no_cpu_baseline and dist.world == 1:
-        cps = r0.iters // cfg.legalize_interval + 2
-        v, sample, t_iter, t_leg = cpu_sample(nl, chip, cfg, r0.iters, cps, opts.field_mode)
+        v, sample, _ = cpu_baseline_one_job(args.workload, opts.field_mode)
         cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "port", "sample": sample}
 
     launches = sum(r.gpu_launches for r in results)
@@ -666,6 +781,7 @@ def ours(args, dist):
         "gpu_launches": int(launches),
         "clocks": ck,
         "precision_form_stages": prec,
+        "precision_form": prec_report,
         "batched": batched,
         "served": served,
         "served_saturated": served_sat,

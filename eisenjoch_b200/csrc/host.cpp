@@ -644,7 +644,7 @@ eplace_status synth(const eplace_synth_spec &sp, eplace_synth_info *info, uint8_
       }
     }
   }
-  for (uint32_t f = 0; f < F; ++f) {
+  for (uint32_t f = 0; f < F && NN > 0; ++f) {  // with no nets, pads join none
     uint32_t n = pad_net[f];
     pin_cell[net_off[n] + deg[n] + pad_cursor[n]++] = N + f;
   }

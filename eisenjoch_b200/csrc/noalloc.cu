@@ -1,19 +1,22 @@
 // noalloc.cu -- the density stage (cell -> bin overlap map and overlap
 // metric) for callers that cannot allocate device memory.
 //
-// Some callers run where cudaMalloc is not available to them: code inside a
-// CUDA-graph capture, a real-time loop that must not allocate or take the
-// allocator's locks, or a host application whose device memory is owned and
-// handed out by another component.  They own their inputs and outputs
-// already; what they cannot do is give this library the working memory the
-// density stage needs (the fixed-point accumulation map, the per-block
-// partial sums and the completion counter).  For them the scratch lives in
-// one file-scope __device__ array, sized for at most kNoAllocMaxBins bins
-// (512 x 512).  It is part of the library image: every GPU that loads
-// libeplace.so holds it (about 2 MiB) until the process exits.
+// Some callers cannot call cudaMalloc: a real-time control loop that must
+// not take the allocator's locks or stall on it, a host application whose
+// device memory is handed out by another component (its own pool, a
+// framework's caching allocator) and may not be grown behind its back, or
+// code running under a fixed device-memory budget.  They own their inputs
+// and outputs already; what they cannot do is give this library the working
+// memory the density stage needs (the fixed-point accumulation map, the
+// per-block partial sums and the completion counter).  For them the scratch
+// lives in one file-scope __device__ array, sized for at most
+// kNoAllocMaxBins bins (512 x 512).  It is part of the library image: every
+// GPU that loads libeplace.so holds it (about 2 MiB) until the process
+// exits.
 //
 // The kernels are the library's own scatter and finalise kernels; only the
 // scratch they are given differs.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstddef>
@@ -46,23 +49,69 @@ static_assert(sizeof(DevScalars) <= 256 && sizeof(IterLog) <= 256, "scratch slot
 
 static __device__ __align__(256) unsigned char g_density_scratch[kScratchBytes];
 
-// Device address of g_density_scratch per device.  In host code the symbol
-// is only a host-side stand-in, so the address is looked up once per device,
-// with that device current, and cached.
+// Device address of g_density_scratch.  In host code the symbol is only a
+// host-side stand-in, so its device address is looked up with the device
+// current (cudaGetSymbolAddress) at set-up and cached per device.  The
+// cache entry also records the unique id of the CUDA context it was looked
+// up in: after cudaDeviceReset (or any other end of the primary context)
+// the module is loaded again, possibly elsewhere, and the next call looks
+// the address up again instead of using a stale one.  The driver calls are
+// reached through the runtime's entry-point table, so the library does not
+// link libcuda directly.
+typedef CUresult (*CtxGetCurrentFn)(CUcontext *);
+typedef CUresult (*CtxGetIdFn)(CUcontext, unsigned long long *);
+
+struct ScratchSlot {
+  unsigned long long ctx_id = 0;
+  void *addr = nullptr;
+};
+
 std::mutex g_mu;
-void *g_addr[128] = {};
+ScratchSlot g_slot[128];
+CtxGetCurrentFn g_ctx_current = nullptr;
+CtxGetIdFn g_ctx_id = nullptr;
+
+// Id of the current context; 0 when no context is current yet.
+eplace_status current_context_id(unsigned long long *id) {
+  *id = 0;
+  if (!g_ctx_current || !g_ctx_id) {
+    void *f1 = nullptr, *f2 = nullptr;
+    cudaDriverEntryPointQueryResult q1, q2;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f1, 12000, cudaEnableDefault, &q1) != cudaSuccess ||
+        cudaGetDriverEntryPointByVersion("cuCtxGetId", &f2, 12000, cudaEnableDefault, &q2) != cudaSuccess ||
+        q1 != cudaDriverEntryPointSuccess || q2 != cudaDriverEntryPointSuccess || !f1 || !f2)
+      return EPLACE_ERR_CUDA;
+    g_ctx_current = reinterpret_cast<CtxGetCurrentFn>(f1);
+    g_ctx_id = reinterpret_cast<CtxGetIdFn>(f2);
+  }
+  CUcontext c = nullptr;
+  if (g_ctx_current(&c) != CUDA_SUCCESS) return EPLACE_ERR_CUDA;
+  if (!c) return EPLACE_OK;
+  return g_ctx_id(c, id) == CUDA_SUCCESS ? EPLACE_OK : EPLACE_ERR_CUDA;
+}
 
 eplace_status scratch_for_current_device(void **out) {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return EPLACE_ERR_NO_DEVICE;
   if (dev < 0 || dev >= 128) return EPLACE_ERR_NO_DEVICE;
   std::lock_guard<std::mutex> g(g_mu);
-  if (!g_addr[dev]) {
+  unsigned long long id = 0;
+  eplace_status st = current_context_id(&id);
+  if (st != EPLACE_OK) return st;
+  ScratchSlot &slot = g_slot[dev];
+  if (id == 0 || !slot.addr || slot.ctx_id != id) {
+    // Set-up: the symbol's device address in the current context (the
+    // lookup also creates the device's primary context when none is current
+    // yet, so the id is read again afterwards).
     void *p = nullptr;
     if (cudaGetSymbolAddress(&p, g_density_scratch) != cudaSuccess || !p) return EPLACE_ERR_CUDA;
-    g_addr[dev] = p;
+    st = current_context_id(&id);
+    if (st != EPLACE_OK) return st;
+    if (id == 0) return EPLACE_ERR_CUDA;
+    slot.addr = p;
+    slot.ctx_id = id;
   }
-  *out = g_addr[dev];
+  *out = slot.addr;
   return EPLACE_OK;
 }
 
@@ -78,6 +127,10 @@ extern "C" eplace_status eplace_density_noalloc(const float *pos_xy, const float
     return EPLACE_ERR_INVALID;
   if ((size_t)bins_x * (size_t)bins_y > kNoAllocMaxBins) return EPLACE_ERR_INVALID;  // over the scratch size
   if (!density || !overlap || (num_cells && !pos_xy)) return EPLACE_ERR_INVALID;
+  // The kernels read (x, y) and (w/2, h/2) as 8-byte pairs and write
+  // doubles: a misaligned pointer would fault the caller's whole context.
+  if (((uintptr_t)pos_xy | (uintptr_t)half_wh | (uintptr_t)density | (uintptr_t)overlap) & 7u)
+    return EPLACE_ERR_INVALID;
   void *base = nullptr;
   eplace_status st = scratch_for_current_device(&base);
   if (st != EPLACE_OK) return st;
@@ -93,8 +146,11 @@ extern "C" eplace_status eplace_density_noalloc(const float *pos_xy, const float
   auto *ticket = reinterpret_cast<unsigned *>(b + kTicketOff);
   auto *sc = reinterpret_cast<DevScalars *>(b + kScalOff);
   auto *lg = reinterpret_cast<IterLog *>(b + kLogOff);
-  // The scratch keeps the previous call's contents: clear the map, the
-  // counter and the scalar slot (iteration 0, read by the finalise).
+  // The scratch keeps the previous call's contents.  A completed call
+  // leaves the map at zero (the finalise re-zeroes every bin it reads) and
+  // the counter back at zero; the clears below make a call correct also
+  // after an earlier call whose kernels did not all run (a launch error part
+  // way through), and set the scalar slot the finalise reads (iteration 0).
   if (cudaMemsetAsync(map, 0, (size_t)nb * sizeof(unsigned long long), s) != cudaSuccess ||
       cudaMemsetAsync(ticket, 0, 256, s) != cudaSuccess || cudaMemsetAsync(sc, 0, 256, s) != cudaSuccess)
     return EPLACE_ERR_CUDA;

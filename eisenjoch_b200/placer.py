@@ -15,6 +15,8 @@ module only marshals arrays.
 """
 
 import ctypes
+import json
+import os
 from dataclasses import dataclass, field, fields
 from typing import List, Optional, Sequence
 
@@ -279,27 +281,16 @@ def synth_netlist(spec: SynthSpec):
 
 
 # The benchmark workloads (seeded synthetic stand-ins for the configurations
-# the placer is measured on; shapes and distributions as specified there).
-WORKLOADS = {
-    # 5,000 unit cells, 128x128 sites and bins, 400 pads, 5,500 nets.
-    "electro_5k_128": dict(
-        spec=SynthSpec(seed=1, num_cells=5000, num_nets=5500, num_pads=400, width=128, height=128,
-                       bins_x=128, bins_y=128, cluster_size=32),
-        cfg=dict(target_density=0.9, max_iters=300),
-    ),
-    # 200,000 cells (5% macros 2x2..8x8), 1024^2 sites, 512^2 bins, 2,000 pads, 220,000 nets.
-    "electro_200k_1024": dict(
-        spec=SynthSpec(seed=2, num_cells=200000, num_nets=220000, num_pads=2000, width=1024, height=1024,
-                       bins_x=512, bins_y=512, cluster_size=64, macro_fraction=0.05),
-        cfg=dict(max_iters=500),
-    ),
-    # 800,000 cells, 2048^2 sites, 1024^2 bins, 880,000 nets.
-    "electro_800k_2048": dict(
-        spec=SynthSpec(seed=3, num_cells=800000, num_nets=880000, num_pads=4000, width=2048, height=2048,
-                       bins_x=1024, bins_y=1024, cluster_size=64, macro_fraction=0.05),
-        cfg=dict(max_iters=500),
-    ),
-}
+# the placer is measured on; shapes and distributions as specified there),
+# kept as data so that tools that must not load this package can read them.
+def _load_workloads():
+    with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "workloads.json")) as f:
+        table = json.load(f)
+    return {name: dict(spec=SynthSpec(**w["spec"]), cfg=dict(w["cfg"]))
+            for name, w in table.items() if not name.startswith("_")}
+
+
+WORKLOADS = _load_workloads()
 
 
 def workload(name):

@@ -289,20 +289,23 @@ eplace_status eplace_initial_placement_host(const eplace_netlist *nl, const epla
 
 /* Density map + overlap without any allocation.  No counterpart in the
  * reference: it is the density stage (eplace_stage_density) for callers
- * that cannot call cudaMalloc -- code inside a CUDA-graph capture, a
- * real-time loop that must not allocate, or an application whose device
- * memory is owned by another component.  All pointers are DEVICE pointers
- * the caller owns: pos_xy [2*num_cells] (x0, y0, x1, y1, ...), half_wh
- * [2*num_cells] half extents or NULL for 1x1 cells, density
- * [bins_y*bins_x] (out), overlap [1] (out).  stream is a cudaStream_t (NULL
- * = the legacy default stream); the call is asynchronous on it.
- * The working memory is a fixed array inside the library, sized for at most
- * 512 x 512 bins; larger grids are rejected with EPLACE_ERR_INVALID.  Every
- * GPU that loads the library holds that array (about 2 MiB) until exit.
- * The first call on a device looks the array up on the current device; make
- * that first call before any stream capture.  All calls share the one
- * array: calls that overlap on the GPU (other streams, other threads) race,
- * so serialise them.  Nothing is allocated or freed. */
+ * that cannot call cudaMalloc -- a real-time loop that must not allocate or
+ * wait on the allocator, an application whose device memory is owned and
+ * handed out by another component, or code under a fixed device-memory
+ * budget.  All pointers are DEVICE pointers the caller owns, each 8-byte
+ * aligned (a misaligned one is rejected with EPLACE_ERR_INVALID): pos_xy
+ * [2*num_cells] (x0, y0, x1, y1, ...), half_wh [2*num_cells] half extents or
+ * NULL for 1x1 cells, density [bins_y*bins_x] (out), overlap [1] (out).
+ * stream is a cudaStream_t (NULL = the legacy default stream); the call is
+ * asynchronous on it.  The working memory is a fixed array inside the
+ * library, sized for at most 512 x 512 bins; larger grids are rejected with
+ * EPLACE_ERR_INVALID.  Every GPU that loads the library holds that array
+ * (about 2 MiB) until exit.  The first call on a device (and the first after
+ * the device's context was destroyed, e.g. by cudaDeviceReset) looks the
+ * array's device address up in the current context; make that first call
+ * before any stream capture.  All calls share the one array: calls that
+ * overlap on the GPU (other streams, other threads) race, so serialise
+ * them.  Nothing is allocated or freed. */
 eplace_status eplace_density_noalloc(const float *pos_xy, const float *half_wh,
                                      uint32_t num_cells, int32_t width, int32_t height,
                                      int32_t bins_x, int32_t bins_y, double *density,

@@ -119,18 +119,45 @@ void orc_pin_weights(const orc_problem *p, double *w) {
 /* ------------------------------------------------------------------------ */
 #define WA_EXP_CLAMP_MIN (-3000.0) /* wa.rs:14 */
 
-/* wa_axis_value (wa.rs:17-46) */
-double orc_wa_axis_value(const double *c, size_t n, double coeff) {
-  if (n < 2) return 0.0;
+static int g_wa_mode = ORC_WA_REFERENCE;
+
+void orc_set_wa_mode(int mode) { g_wa_mode = mode; }
+
+/* The exponent shifts of one axis.  Reference (wa.rs:58, :68, :73): both
+ * exponentials are shifted by the pin mean, so exp() overflows once a pin
+ * sits more than ~709/coeff sites from it (and S^2 in the gradient at half
+ * that).  ORC_WA_STABLE (extension): e+ is shifted by the largest
+ * coordinate and e- by the smallest, so every exponent is <= 0 and S >= 1;
+ * WA value and gradient are the same functions of the coordinates (the
+ * shift cancels in every quotient), only the rounding differs. */
+static void wa_shifts(const double *c, size_t n, double *up, double *down) {
+  if (g_wa_mode == ORC_WA_STABLE) {
+    double lo = c[0], hi = c[0];
+    for (size_t i = 1; i < n; ++i) {
+      lo = fmin(lo, c[i]);
+      hi = fmax(hi, c[i]);
+    }
+    *up = hi;
+    *down = lo;
+    return;
+  }
   double center = 0.0;
   for (size_t i = 0; i < n; ++i) center += c[i];
   center /= (double)n;
+  *up = *down = center;
+}
+
+/* wa_axis_value (wa.rs:17-46) */
+double orc_wa_axis_value(const double *c, size_t n, double coeff) {
+  if (n < 2) return 0.0;
+  double up, down;
+  wa_shifts(c, n, &up, &down);
   double smax = 0, xmax = 0, smin = 0, xmin = 0;
   for (size_t i = 0; i < n; ++i) {
-    double ea = exp(fmax(coeff * (c[i] - center), WA_EXP_CLAMP_MIN));
+    double ea = exp(fmax(coeff * (c[i] - up), WA_EXP_CLAMP_MIN));
     smax += ea;
     xmax += c[i] * ea;
-    double eb = exp(fmax(coeff * (center - c[i]), WA_EXP_CLAMP_MIN));
+    double eb = exp(fmax(coeff * (down - c[i]), WA_EXP_CLAMP_MIN));
     smin += eb;
     xmin += c[i] * eb;
   }
@@ -141,17 +168,16 @@ double orc_wa_axis_value(const double *c, size_t n, double coeff) {
 /* wa_axis_grad (wa.rs:51-101): quotient rule, accumulates into grad. */
 void orc_wa_axis_grad(const double *c, size_t n, double coeff, double *grad) {
   if (n < 2) return;
-  double center = 0.0;
-  for (size_t i = 0; i < n; ++i) center += c[i];
-  center /= (double)n;
+  double up, down;
+  wa_shifts(c, n, &up, &down);
   double *ea = (double *)malloc(sizeof(double) * n * 2);
   double *eb = ea + n;
   double smax = 0, smin = 0, xmax = 0, xmin = 0;
   for (size_t i = 0; i < n; ++i) {
-    ea[i] = exp(fmax(coeff * (c[i] - center), WA_EXP_CLAMP_MIN));
+    ea[i] = exp(fmax(coeff * (c[i] - up), WA_EXP_CLAMP_MIN));
     smax += ea[i];
     xmax += c[i] * ea[i];
-    eb[i] = exp(fmax(coeff * (center - c[i]), WA_EXP_CLAMP_MIN));
+    eb[i] = exp(fmax(coeff * (down - c[i]), WA_EXP_CLAMP_MIN));
     smin += eb[i];
     xmin += c[i] * eb[i];
   }
@@ -851,6 +877,7 @@ int orc_place(const orc_problem *p, const orc_cfg *cfg, int be, int lm, orc_resu
   res->converged = 0;
   res->hpwl = 0;
   res->final_overlap = 0.0;
+  res->first_nonfinite_grad_iter = -1;
   if (cfg->legalize_interval == 0) return ORC_ERR_INVALID; /* `%` by zero panics */
 
   /* reseed_rng + initial_placement (mod.rs:66-69) */
@@ -897,6 +924,12 @@ int orc_place(const orc_problem *p, const orc_cfg *cfg, int be, int lm, orc_resu
     }
     memset(g, 0, sizeof(double) * n * 4); /* g and gd */
     orc_wa_gradient(p, c, c + n, cfg->wl_coeff, g, g + n);
+    if (res->first_nonfinite_grad_iter < 0)
+      for (size_t k = 0; k < (size_t)n * 2; ++k)
+        if (!isfinite(g[k])) {
+          res->first_nonfinite_grad_iter = (int32_t)it;
+          break;
+        }
     orc_density(p, c, c + n, d);
     double overlap = orc_overlap(d, nb, cap);
     last_overlap = overlap;

@@ -104,6 +104,12 @@ void orc_dst3(double *v, size_t n, int backend);
 enum { ORC_FIELD_REFERENCE = 0, ORC_FIELD_POTENTIAL_GRADIENT = 1 };
 void orc_set_field_mode(int mode);
 
+/* WA exponent shift: ORC_WA_REFERENCE = the pin mean (wa.rs:58, overflows in
+ * FP64 on wide nets); ORC_WA_STABLE = per-net max / min (extension: the same
+ * value and gradient, never overflows; the shift the CUDA kernel uses). */
+enum { ORC_WA_REFERENCE = 0, ORC_WA_STABLE = 1 };
+void orc_set_wa_mode(int mode);
+
 /* --- Poisson field (density.rs:96-166) ---
  * phi_hat (optional) receives the scaled potential spectrum.  */
 int orc_field(const double *d, int32_t bw, int32_t bh, double target_density,
@@ -172,6 +178,7 @@ typedef struct {
   int32_t best_iter;
   int converged;
   double overlap_trace_last;
+  int32_t first_nonfinite_grad_iter; /* first iteration whose WA gradient had a NaN/inf, or -1 */
 } orc_result;
 
 /* dct_backend: 0 direct, 1 FFT.  legal_method: 0 brute, 1 ring.
@@ -180,6 +187,22 @@ int orc_place(const orc_problem *p, const orc_cfg *cfg, int dct_backend,
               int legal_method, orc_result *res, double *overlap_trace);
 
 void orc_cfg_default(orc_cfg *cfg);
+
+/* --- benchmark input generator (orc_synth.c; no reference counterpart) --- */
+typedef struct {
+  uint64_t seed;
+  uint32_t num_cells, num_nets, num_pads;
+  int32_t width, height, bins_x, bins_y;
+  uint32_t cluster_size;
+  double locality;
+  double macro_fraction;
+  uint32_t macro_min, macro_max;
+} orc_synth_spec;
+
+/* With net_off == NULL: only *num_pins.  Else fills cw/ch [num_cells] (may
+ * be NULL), fx/fy [num_pads], net_off [num_nets + 1], pin_cell [num_pins]. */
+int orc_synth(const orc_synth_spec *spec, uint32_t *num_pins, uint8_t *cw, uint8_t *ch, int32_t *fx,
+              int32_t *fy, uint32_t *net_off, uint32_t *pin_cell);
 
 #ifdef __cplusplus
 }

@@ -86,6 +86,7 @@ class _Result(ctypes.Structure):
         ("best_iter", ctypes.c_int32),
         ("converged", ctypes.c_int),
         ("overlap_trace_last", ctypes.c_double),
+        ("first_nonfinite_grad_iter", ctypes.c_int32),
     ]
 
 
@@ -110,6 +111,24 @@ class _State(ctypes.Structure):
     ]
 
 
+class _SynthSpec(ctypes.Structure):
+    _fields_ = [
+        ("seed", ctypes.c_uint64),
+        ("num_cells", ctypes.c_uint32),
+        ("num_nets", ctypes.c_uint32),
+        ("num_pads", ctypes.c_uint32),
+        ("width", ctypes.c_int32),
+        ("height", ctypes.c_int32),
+        ("bins_x", ctypes.c_int32),
+        ("bins_y", ctypes.c_int32),
+        ("cluster_size", ctypes.c_uint32),
+        ("locality", ctypes.c_double),
+        ("macro_fraction", ctypes.c_double),
+        ("macro_min", ctypes.c_uint32),
+        ("macro_max", ctypes.c_uint32),
+    ]
+
+
 _lib = None
 
 
@@ -121,8 +140,8 @@ def build():
 def lib():
     global _lib
     if _lib is None:
-        src = os.path.join(_HERE, "eplace_oracle.c")
-        if not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < os.path.getmtime(src):
+        srcs = [os.path.join(_HERE, f) for f in ("eplace_oracle.c", "orc_synth.c", "eplace_oracle.h")]
+        if not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < max(map(os.path.getmtime, srcs)):
             build()
         L = ctypes.CDLL(LIB_PATH)
         d, i32, u64, f64p = ctypes.c_double, ctypes.c_int32, ctypes.c_uint64, P(ctypes.c_double)
@@ -153,6 +172,11 @@ def lib():
         L.orc_place.restype = ctypes.c_int
         L.orc_place.argtypes = [P(_Problem), P(_Cfg), ctypes.c_int, ctypes.c_int, P(_Result), f64p]
         L.orc_set_field_mode.argtypes = [ctypes.c_int]
+        L.orc_set_wa_mode.argtypes = [ctypes.c_int]
+        L.orc_cfg_default.argtypes = [P(_Cfg)]
+        L.orc_synth.restype = ctypes.c_int
+        L.orc_synth.argtypes = [P(_SynthSpec), P(ctypes.c_uint32), P(ctypes.c_uint8), P(ctypes.c_uint8), P(i32),
+                                P(i32), P(ctypes.c_uint32), P(ctypes.c_uint32)]
         L.orc_step.argtypes = [P(_Problem), P(_State), u64, f64p, f64p, f64p, d, d, f64p]
         L.orc_nesterov_init.argtypes = [P(_Nest), f64p, f64p, ctypes.c_size_t, d]
         L.orc_nesterov_set_positions.argtypes = [P(_Nest), f64p]
@@ -177,6 +201,74 @@ def _p(a, t):
 
 def _d(a):
     return np.ascontiguousarray(a, dtype=np.float64)
+
+
+# --- benchmark inputs -------------------------------------------------------
+class FlatNetlist:
+    """The flat netlist the oracle takes (the attributes of the product's
+    Netlist, without importing it)."""
+
+    def __init__(self, num_cells, net_offsets, pin_cell, fixed_x, fixed_y, cell_w=None, cell_h=None):
+        self.num_cells = int(num_cells)
+        self.net_offsets, self.pin_cell = net_offsets, pin_cell
+        self.fixed_x, self.fixed_y = fixed_x, fixed_y
+        self.cell_w, self.cell_h = cell_w, cell_h
+        self.cell_init_x = self.cell_init_y = self.fixed_on_logic = self.net_has_driver = None
+
+    @property
+    def num_fixed(self):
+        return int(self.fixed_x.size)
+
+    @property
+    def num_nets(self):
+        return int(self.net_offsets.size - 1)
+
+    @property
+    def num_pins(self):
+        return int(self.net_offsets[-1])
+
+
+class FlatChip:
+    def __init__(self, width, height, bins_x=0, bins_y=0):
+        self.width, self.height, self.bins_x, self.bins_y = width, height, bins_x, bins_y
+
+
+class Cfg:
+    """ElectroPlaceCfg (electro_place/config.rs:5-40): the nine fields with
+    the defaults of ElectroPlaceCfg::default() (config.rs:29-40), from the
+    C restatement, then `overrides`."""
+
+    def __init__(self, **overrides):
+        c = _Cfg()
+        lib().orc_cfg_default(ctypes.byref(c))
+        for name, _ in _Cfg._fields_:
+            setattr(self, name, getattr(c, name))
+        for k, v in overrides.items():
+            if not hasattr(self, k):
+                raise AttributeError(k)
+            setattr(self, k, v)
+
+
+def synth(spec):
+    """The seeded benchmark netlist of `spec` (any object with the fields of
+    _SynthSpec), generated by the oracle's own copy of the generator.
+    Returns (FlatNetlist, FlatChip)."""
+    s = _SynthSpec()
+    for name, _ in _SynthSpec._fields_:
+        setattr(s, name, getattr(spec, name))
+    L = lib()
+    npins = ctypes.c_uint32()
+    assert L.orc_synth(ctypes.byref(s), ctypes.byref(npins), None, None, None, None, None, None) == 0
+    n, nn, f = spec.num_cells, spec.num_nets, spec.num_pads
+    cw, ch = np.ones(n, np.uint8), np.ones(n, np.uint8)
+    fx, fy = np.zeros(f, np.int32), np.zeros(f, np.int32)
+    off, pins = np.zeros(nn + 1, np.uint32), np.zeros(npins.value, np.uint32)
+    assert L.orc_synth(ctypes.byref(s), ctypes.byref(npins), _p(cw, ctypes.c_uint8), _p(ch, ctypes.c_uint8),
+                       _p(fx, ctypes.c_int32), _p(fy, ctypes.c_int32), _p(off, ctypes.c_uint32),
+                       _p(pins, ctypes.c_uint32)) == 0
+    macro = spec.macro_fraction > 0
+    nl = FlatNetlist(n, off, pins, fx, fy, cw if macro else None, ch if macro else None)
+    return nl, FlatChip(spec.width, spec.height, spec.bins_x, spec.bins_y)
 
 
 # --- transforms and WA on plain arrays -------------------------------------
@@ -359,12 +451,18 @@ class Oracle:
         self._L.orc_pin_weights(ctypes.byref(self.p), _p(w, ctypes.c_double))
         return w
 
-    def wa_gradient(self, x, y, coeff=0.5):
-        """add_wa_wirelength_gradient (placer/common.rs:205-291)."""
+    def wa_gradient(self, x, y, coeff=0.5, wa_mode=0):
+        """add_wa_wirelength_gradient (placer/common.rs:205-291).  wa_mode 1
+        shifts the exponents by the per-net max / min instead of the mean
+        (extension: same function, no FP64 overflow on wide nets)."""
         x, y = _d(x), _d(y)
         gx, gy = np.zeros(self.n), np.zeros(self.n)
-        self._L.orc_wa_gradient(ctypes.byref(self.p), _p(x, ctypes.c_double), _p(y, ctypes.c_double), coeff,
-                                _p(gx, ctypes.c_double), _p(gy, ctypes.c_double))
+        self._L.orc_set_wa_mode(wa_mode)
+        try:
+            self._L.orc_wa_gradient(ctypes.byref(self.p), _p(x, ctypes.c_double), _p(y, ctypes.c_double), coeff,
+                                    _p(gx, ctypes.c_double), _p(gy, ctypes.c_double))
+        finally:
+            self._L.orc_set_wa_mode(0)
         return gx, gy
 
     def density(self, x, y):
@@ -464,10 +562,11 @@ class Oracle:
         out["look_x"], out["look_y"] = la
         return out, norms
 
-    def place(self, cfg, dct_backend=1, legal_method=1, want_trace=False, field_mode=0):
+    def place(self, cfg, dct_backend=1, legal_method=1, want_trace=False, field_mode=0, wa_mode=0):
         """place_electro (electro_place/mod.rs:65-204).  cfg: any object with
         the nine ElectroPlaceCfg fields.  field_mode 1 is the
-        potential-gradient extension.  Returns (status, dict)."""
+        potential-gradient extension, wa_mode 1 the overflow-free WA shift
+        (both extensions).  Returns (status, dict)."""
         c = _Cfg()
         for name, _ in _Cfg._fields_:
             setattr(c, name, getattr(cfg, name))
@@ -483,14 +582,17 @@ class Oracle:
         r.traj_capacity = cap
         trace = np.zeros(max(1, int(cfg.max_iters))) if want_trace else None
         self._L.orc_set_field_mode(field_mode)
+        self._L.orc_set_wa_mode(wa_mode)
         try:
             st = self._L.orc_place(ctypes.byref(self.p), ctypes.byref(c), dct_backend, legal_method,
                                    ctypes.byref(r), _p(trace, ctypes.c_double))
         finally:
             self._L.orc_set_field_mode(0)
+            self._L.orc_set_wa_mode(0)
         out = dict(
             site_x=sx, site_y=sy, best_x=bx, best_y=by, hpwl=int(r.hpwl), iters=int(r.iters),
             best_iter=int(r.best_iter), converged=bool(r.converged), final_overlap=r.final_overlap,
+            first_nonfinite_grad_iter=int(r.first_nonfinite_grad_iter),
             trajectory=[dict(iter=traj[k].iter, hpwl=traj[k].hpwl, disp=traj[k].displacement,
                              step_x=traj[k].step_x, step_y=traj[k].step_y,
                              density_penalty=traj[k].density_penalty, overlap=traj[k].overlap)

@@ -229,9 +229,10 @@ def test_legalizer_bit_exact(case):
 
 # --- whole loop ------------------------------------------------------------
 def test_full_run_matches_oracle():
-    """5k-cell reference-geometry run: final legalised HPWL within 0.5% of
-    the FP64 oracle's, and the overlap at each legalisation checkpoint
-    tracks the oracle's."""
+    """5k-cell reference-geometry run with the reference field formula:
+    final legalised HPWL within 0.5 % of the FP64 oracle's, the same
+    convergence, and at every legalisation checkpoint the overlap within
+    2e-3 absolute and the legalised HPWL within 0.5 % of the oracle's."""
     nl, chip, cfg = E.workload("electro_5k_128")
     r = E.place_electro(nl, chip, cfg)
     orc = Oracle(nl, chip)
@@ -245,6 +246,13 @@ def test_full_run_matches_oracle():
     bx, by = r.bel_tile % chip.width, r.bel_tile // chip.width
     assert orc.hpwl(bx, by) == r.hpwl
     assert len(np.unique(r.bel_tile)) == nl.num_cells
+    # the trajectory, checkpoint by checkpoint
+    ours = {t["iter"]: t for t in r.trajectory}
+    common = [t for t in o["trajectory"] if t["iter"] in ours]
+    assert len(common) == len(o["trajectory"]) == len(r.trajectory)
+    d_ov = max(abs(ours[t["iter"]]["overlap"] - t["overlap"]) for t in common)
+    d_hp = max(abs(ours[t["iter"]]["hpwl"] - t["hpwl"]) / t["hpwl"] for t in common)
+    assert d_ov <= 2e-3 and d_hp <= 0.005, (d_ov, d_hp)
 
 
 def test_full_run_potential_gradient_mode():

@@ -194,3 +194,40 @@ def test_engine_without_gpu_reports_no_device():
     with pytest.raises(E.EplaceError) as ei:
         E.JobServer()
     assert ei.value.status == E._abi.EPLACE_ERR_NO_DEVICE
+
+
+@pytest.mark.parametrize("spec", [
+    E.SynthSpec(seed=1, num_cells=5000, num_nets=5500, num_pads=400, width=128, height=128, cluster_size=32),
+    E.SynthSpec(seed=9, num_cells=20000, num_nets=22000, num_pads=300, width=256, height=256, bins_x=128,
+                bins_y=128, cluster_size=64, macro_fraction=0.05),
+    E.SynthSpec(seed=4, num_cells=3, num_nets=10, num_pads=0, width=4, height=4),
+    E.SynthSpec(seed=5, num_cells=0, num_nets=3, num_pads=6, width=8, height=1),
+    E.SynthSpec(seed=6, num_cells=700, num_nets=0, num_pads=17, width=40, height=30, cluster_size=7,
+                locality=0.9, macro_fraction=0.2, macro_min=3, macro_max=5),
+])
+def test_oracle_generator_equals_product_generator(spec):
+    """The CPU reference arm generates its inputs with the oracle's copy of
+    the generator (so it never loads the product library): both copies must
+    emit the same netlist bytes."""
+    a, ca = E.synth_netlist(spec)
+    b, cb = O.synth(spec)
+    for k in ("net_offsets", "pin_cell", "fixed_x", "fixed_y", "cell_w", "cell_h"):
+        va, vb = getattr(a, k), getattr(b, k)
+        assert (va is None) == (vb is None), k
+        if va is not None:
+            assert va.dtype == vb.dtype and np.array_equal(va, vb), k
+    assert (ca.width, ca.height, ca.bins_x, ca.bins_y) == (cb.width, cb.height, cb.bins_x, cb.bins_y)
+
+
+def test_workload_table_is_plain_data():
+    """bench.py's CPU arm reads the workload table as JSON; the product's
+    WORKLOADS is built from the same file."""
+    import json
+    with open(os.path.join(ROOT, "eisenjoch_b200", "workloads.json")) as f:
+        table = {k: v for k, v in json.load(f).items() if not k.startswith("_")}
+    assert set(table) == set(E.WORKLOADS)
+    for name, w in table.items():
+        spec = E.WORKLOADS[name]["spec"]
+        for k, v in w["spec"].items():
+            assert getattr(spec, k) == v, (name, k)
+        assert E.WORKLOADS[name]["cfg"] == w["cfg"]

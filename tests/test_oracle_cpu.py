@@ -356,3 +356,29 @@ def test_job_summaries_fixture():
         d = json.load(f)
     assert not d["electro_5k_128:reference_field"]["converged"]
     assert d["electro_5k_128"]["converged"] and d["electro_200k_1024"]["converged"]
+
+
+def test_stable_wa_shift_equals_reference_where_finite():
+    """The oracle's overflow-free WA shift (per-net max / min, the shift the
+    CUDA kernel uses) gives the reference's gradient wherever the reference's
+    mean shift (wa.rs:58) stays finite, and stays finite where it does not."""
+    rng = np.random.default_rng(3)
+    n, w = 400, 64
+    off = np.cumsum([0] + [int(d) for d in rng.integers(2, 30, 60)]).astype(np.uint32)
+    pins = rng.integers(0, n, int(off[-1])).astype(np.uint32)
+    nl = O.FlatNetlist(n, off, pins, np.zeros(0, np.int32), np.zeros(0, np.int32))
+    orc = O.Oracle(nl, O.FlatChip(w, w))
+    x, y = rng.uniform(0, w - 1, n), rng.uniform(0, w - 1, n)
+    for coeff in (0.1, 0.5, 2.0):
+        a = orc.wa_gradient(x, y, coeff)
+        b = orc.wa_gradient(x, y, coeff, wa_mode=1)
+        for ga, gb in zip(a, b):
+            assert np.isfinite(ga).all()
+            np.testing.assert_allclose(gb, ga, rtol=1e-9, atol=1e-12 * np.abs(ga).max())
+    # 2048-site spans: the mean shift overflows FP64, the stable one does not
+    x2 = rng.uniform(0, 2047, n)
+    ra = orc.wa_gradient(x2, y, 1.0)[0]
+    rb = orc.wa_gradient(x2, y, 1.0, wa_mode=1)[0]
+    assert not np.isfinite(ra).all() and np.isfinite(rb).all()
+    ok = np.isfinite(ra)
+    np.testing.assert_allclose(rb[ok], ra[ok], rtol=1e-9, atol=1e-12 * np.abs(ra[ok]).max())
