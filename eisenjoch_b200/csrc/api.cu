@@ -620,7 +620,7 @@ void launch_scatter_stage(eplace_ctx *c) {
   const HostProblem &hp = c->hp;
   ScatterArgs a{c->look.p, hp.any_macro ? c->half.p : nullptr, hp.any_macro ? c->mflag.p : nullptr,
                 hp.any_macro ? c->mac_idx.p : nullptr, hp.any_macro ? c->n_mac : 0u, hp.N, hp.BX, hp.BY,
-                (float)hp.sx, (float)hp.sy, 1.0f / (float)hp.sx, 1.0f / (float)hp.sy, c->dens.p};
+                hp.sx, hp.sy, c->dens.p};
   CK(launch_scatter(a, grid_for((int)hp.N, kScatterBlock, c->num_sms * c->sc_blocks_per_sm), c->stream));
 }
 
@@ -957,10 +957,8 @@ StepArgs step_args(eplace_ctx *c) {
   a.N = hp.N;
   a.BX = hp.BX;
   a.BY = hp.BY;
-  a.sx = (float)hp.sx;
-  a.sy = (float)hp.sy;
-  a.inv_sx = 1.0f / (float)hp.sx;
-  a.inv_sy = 1.0f / (float)hp.sy;
+  a.isx = hp.sx;
+  a.isy = hp.sy;
   a.maxx = (float)(hp.W - 1);
   a.maxy = (float)(hp.H - 1);
   a.look = c->look.p;

@@ -335,32 +335,53 @@ __global__ void __launch_bounds__(kWaBlock) k_wa(const WaArgs a) {
 // ---------------------------------------------------------------------------
 // Footprint helpers shared by the scatter and the gather.  Footprint
 // [x - w/2, x + w/2] x [y - h/2, y + h/2] in sites; bin b covers
-// [b*s, (b+1)*s).  With w = h = s = 1 this is cell_bin_overlap /
-// bin_overlap_area (density.rs:20-48) in FP32.
+// [b*s, (b+1)*s) (s sites per bin, an integer).  With w = h = s = 1 this is
+// cell_bin_overlap / bin_overlap_area (density.rs:20-48).
+// The arithmetic is exact in FP32 up to the final product of the two 1-D
+// overlaps: a coordinate is split into its integer part i and fraction f
+// (both exact), every edge difference is formed as (integer - f), and the
+// bin range comes from integer floor / ceiling divisions.  Forming x + w/2
+// directly would round once the sum crosses a power of two (at 1024 sites
+// the FP32 spacing doubles to 1.2e-4), which shows up as area lost from one
+// bin.
 // ---------------------------------------------------------------------------
 struct Foot {
-  float xlo, xhi, ylo, yhi;
+  float fx, fy;   // fractional parts of the centre, in [0, 1)
+  float hw, hh;   // half extents
+  int ix, iy;     // integer parts of the centre
   int bx0, bx1, by0, by1;
 };
 
-__device__ __forceinline__ Foot make_foot(float2 p, float hw, float hh, int BX, int BY,
-                                          float inv_sx, float inv_sy) {
+__device__ __forceinline__ int floor_div(int a, int s) { return a >= 0 ? a / s : -((s - 1 - a) / s); }
+__device__ __forceinline__ int ceil_div(int a, int s) { return -floor_div(-a, s); }
+
+__device__ __forceinline__ Foot make_foot(float2 p, float hw, float hh, int BX, int BY, int sx, int sy) {
   Foot f;
-  f.xlo = p.x - hw;
-  f.xhi = p.x + hw;
-  f.ylo = p.y - hh;
-  f.yhi = p.y + hh;
-  f.bx0 = max(0, (int)floorf(f.xlo * inv_sx));
-  f.bx1 = min(BX, max(0, (int)ceilf(f.xhi * inv_sx)));
-  f.by0 = max(0, (int)floorf(f.ylo * inv_sy));
-  f.by1 = min(BY, max(0, (int)ceilf(f.yhi * inv_sy)));
+  const float flx = floorf(p.x), fly = floorf(p.y);
+  f.ix = (int)flx;
+  f.iy = (int)fly;
+  f.fx = p.x - flx;
+  f.fy = p.y - fly;
+  f.hw = hw;
+  f.hh = hh;
+  // floor(x - hw) = ix + floor(fx - hw), ceil(x + hw) = ix + ceil(fx + hw)
+  f.bx0 = max(0, floor_div(f.ix + (int)floorf(f.fx - hw), sx));
+  f.bx1 = min(BX, max(0, ceil_div(f.ix + (int)ceilf(f.fx + hw), sx)));
+  f.by0 = max(0, floor_div(f.iy + (int)floorf(f.fy - hh), sy));
+  f.by1 = min(BY, max(0, ceil_div(f.iy + (int)ceilf(f.fy + hh), sy)));
   return f;
 }
 
-__device__ __forceinline__ float overlap_1d(float lo, float hi, int b, float s) {
-  float b0 = (float)b * s;
-  return fmaxf(fminf(hi, b0 + s) - fmaxf(lo, b0), 0.0f);
+// Length of [c - h, c + h] inside [b*s, (b+1)*s), c = i + fr:
+// min(h, (b+1)s - c) - max(-h, b s - c), each difference formed exactly.
+__device__ __forceinline__ float overlap_1d(int i, float fr, float h, int b, int s) {
+  const int k0 = b * s - i;
+  const float hi = fminf(h, (float)(k0 + s) - fr);
+  const float lo = fmaxf(-h, (float)k0 - fr);
+  return fmaxf(hi - lo, 0.0f);
 }
+__device__ __forceinline__ float overlap_x(const Foot &f, int bx, int s) { return overlap_1d(f.ix, f.fx, f.hw, bx, s); }
+__device__ __forceinline__ float overlap_y(const Foot &f, int by, int s) { return overlap_1d(f.iy, f.fy, f.hh, by, s); }
 
 // Unit cells first (a 1x1 footprint covers at most 2 x 2 bins: unrolled, no
 // footprint load), then the macros from their own list, so a warp of unit
@@ -372,11 +393,11 @@ __global__ void __launch_bounds__(kScatterBlock) k_scatter(const ScatterArgs a) 
   if (a.half && !a.mflag) {
     for (uint32_t i = t0; i < a.N; i += ts) {
       const float2 hf = a.half[i];
-      const Foot f = make_foot(a.pos[i], hf.x, hf.y, a.BX, a.BY, a.inv_sx, a.inv_sy);
+      const Foot f = make_foot(a.pos[i], hf.x, hf.y, a.BX, a.BY, a.isx, a.isy);
       for (int by = f.by0; by < f.by1; ++by) {
-        const float oy = overlap_1d(f.ylo, f.yhi, by, a.sy);
+        const float oy = overlap_y(f, by, a.isy);
         for (int bx = f.bx0; bx < f.bx1; ++bx) {
-          const float ar = overlap_1d(f.xlo, f.xhi, bx, a.sx) * oy;
+          const float ar = overlap_x(f, bx, a.isx) * oy;
           if (ar > 0.0f) atomicAdd(&a.dens[(size_t)by * a.BX + bx], to_fix(ar));
         }
       }
@@ -385,23 +406,23 @@ __global__ void __launch_bounds__(kScatterBlock) k_scatter(const ScatterArgs a) 
   }
   for (uint32_t i = t0; i < a.N; i += ts) {
     if (a.mflag && a.mflag[i]) continue;
-    const Foot f = make_foot(a.pos[i], 0.5f, 0.5f, a.BX, a.BY, a.inv_sx, a.inv_sy);
+    const Foot f = make_foot(a.pos[i], 0.5f, 0.5f, a.BX, a.BY, a.isx, a.isy);
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
       const int by = f.by0 + (k >> 1), bx = f.bx0 + (k & 1);
       if (by >= f.by1 || bx >= f.bx1) continue;
-      const float ar = overlap_1d(f.xlo, f.xhi, bx, a.sx) * overlap_1d(f.ylo, f.yhi, by, a.sy);
+      const float ar = overlap_x(f, bx, a.isx) * overlap_y(f, by, a.isy);
       if (ar > 0.0f) atomicAdd(&a.dens[(size_t)by * a.BX + bx], to_fix(ar));
     }
   }
   for (uint32_t k = t0; k < a.n_mac; k += ts) {
     const uint32_t i = a.mac_idx[k];
     const float2 hf = a.half[i];
-    const Foot f = make_foot(a.pos[i], hf.x, hf.y, a.BX, a.BY, a.inv_sx, a.inv_sy);
+    const Foot f = make_foot(a.pos[i], hf.x, hf.y, a.BX, a.BY, a.isx, a.isy);
     for (int by = f.by0; by < f.by1; ++by) {
-      const float oy = overlap_1d(f.ylo, f.yhi, by, a.sy);
+      const float oy = overlap_y(f, by, a.isy);
       for (int bx = f.bx0; bx < f.bx1; ++bx) {
-        const float ar = overlap_1d(f.xlo, f.xhi, bx, a.sx) * oy;
+        const float ar = overlap_x(f, bx, a.isx) * oy;
         if (ar > 0.0f) atomicAdd(&a.dens[(size_t)by * a.BX + bx], to_fix(ar));
       }
     }
@@ -737,7 +758,7 @@ __device__ __forceinline__ float2 gather_unit_foot(const StepArgs &a, const Foot
   for (int k = 0; k < 4; ++k) {
     const int by = f.by0 + (k >> 1), bx = f.bx0 + (k & 1);
     const bool in = by < f.by1 && bx < f.bx1;
-    w[k] = in ? overlap_1d(f.xlo, f.xhi, bx, a.sx) * overlap_1d(f.ylo, f.yhi, by, a.sy) : 0.0f;
+    w[k] = in ? overlap_x(f, bx, a.isx) * overlap_y(f, by, a.isy) : 0.0f;
     id[k] = (w[k] > 0.0f) ? (size_t)by * a.BX + bx : 0;
   }
   float e[4], h[4];
@@ -763,7 +784,7 @@ __device__ __forceinline__ float2 gather_unit_foot(const StepArgs &a, const Foot
 
 // Field gather of a 1x1 cell (no footprint load).
 __device__ __forceinline__ float2 gather_unit(const StepArgs &a, float2 p) {
-  const Foot f = make_foot(p, 0.5f, 0.5f, a.BX, a.BY, a.inv_sx, a.inv_sy);
+  const Foot f = make_foot(p, 0.5f, 0.5f, a.BX, a.BY, a.isx, a.isy);
   return gather_unit_foot(a, f);
 }
 
@@ -771,7 +792,7 @@ __device__ __forceinline__ float2 gather_unit(const StepArgs &a, float2 p) {
 // (compute_density_gradient, density.rs:171-206).
 __device__ __forceinline__ float2 gather_cell(const StepArgs &a, uint32_t i, float2 p) {
   const float2 hf = a.half ? a.half[i] : make_float2(0.5f, 0.5f);
-  const Foot f = make_foot(p, hf.x, hf.y, a.BX, a.BY, a.inv_sx, a.inv_sy);
+  const Foot f = make_foot(p, hf.x, hf.y, a.BX, a.BY, a.isx, a.isy);
   float fx = 0.f, fy = 0.f, wt = 0.f;
   if (hf.x == 0.5f && hf.y == 0.5f) return gather_unit_foot(a, f);
   // Bins of a row in chunks of 8 with all field loads of a chunk issued
@@ -779,13 +800,13 @@ __device__ __forceinline__ float2 gather_cell(const StepArgs &a, uint32_t i, flo
   // costs one memory latency per row and chunk instead of one per bin; the
   // sums keep the row-major bin order.
   for (int by = f.by0; by < f.by1; ++by) {
-    const float oy = overlap_1d(f.ylo, f.yhi, by, a.sy);
+    const float oy = overlap_y(f, by, a.isy);
     for (int b0 = f.bx0; b0 < f.bx1; b0 += 8) {
       float w[8], e[8], h[8];
 #pragma unroll
       for (int k = 0; k < 8; ++k) {
         const int bx = b0 + k;
-        w[k] = (bx < f.bx1) ? overlap_1d(f.xlo, f.xhi, bx, a.sx) * oy : 0.0f;
+        w[k] = (bx < f.bx1) ? overlap_x(f, bx, a.isx) * oy : 0.0f;
         const size_t idx = (size_t)by * a.BX + (w[k] > 0.0f ? bx : 0);
         e[k] = (w[k] > 0.0f) ? a.Ex[idx] : 0.0f;
         h[k] = (w[k] > 0.0f) ? a.Ey[idx] : 0.0f;

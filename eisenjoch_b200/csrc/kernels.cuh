@@ -86,7 +86,7 @@ struct ScatterArgs {
   uint32_t n_mac;
   uint32_t N;
   int BX, BY;
-  float sx, sy, inv_sx, inv_sy;
+  int isx, isy;              // sites per bin along x / y
   unsigned long long *dens; // [BY * BX] fixed point
 };
 
@@ -123,7 +123,7 @@ struct SpectralArgs {
 struct StepArgs {
   uint32_t N;
   int BX, BY;
-  float sx, sy, inv_sx, inv_sy;
+  int isx, isy;              // sites per bin along x / y
   float maxx, maxy;
   float2 *look;             // [N] (fixed cells follow in the same buffer)
   const float2 *half;       // nullptr => unit cells

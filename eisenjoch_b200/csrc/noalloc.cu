@@ -154,9 +154,9 @@ extern "C" eplace_status eplace_density_noalloc(const float *pos_xy, const float
   if (cudaMemsetAsync(map, 0, (size_t)nb * sizeof(unsigned long long), s) != cudaSuccess ||
       cudaMemsetAsync(ticket, 0, 256, s) != cudaSuccess || cudaMemsetAsync(sc, 0, 256, s) != cudaSuccess)
     return EPLACE_ERR_CUDA;
-  const float sx = (float)(width / bins_x), sy = (float)(height / bins_y);
+  const int sx = width / bins_x, sy = height / bins_y;
   ScatterArgs a{reinterpret_cast<const float2 *>(pos_xy), reinterpret_cast<const float2 *>(half_wh), nullptr,
-                nullptr, 0u, num_cells, bins_x, bins_y, sx, sy, 1.0f / sx, 1.0f / sy, map};
+                nullptr, 0u, num_cells, bins_x, bins_y, sx, sy, map};
   if (num_cells) {
     long long g = ((long long)num_cells + kScatterBlock - 1) / kScatterBlock;
     if (g > (long long)sms * 16) g = (long long)sms * 16;

@@ -48,10 +48,11 @@ def _noalloc(torch, nl, chip, x, y, half_d, dens_d, ov_d):
     dev = dens_d.device
     pos_d = torch.from_numpy(np.ascontiguousarray(np.stack([x, y], axis=1))).to(dev)
     stream = torch.cuda.current_stream(dev)
+    bx, by = chip.bins_x or chip.width, chip.bins_y or chip.height  # 0: one bin per site
     st = L.eplace_density_noalloc(
         ctypes.c_void_p(pos_d.data_ptr() if nl.num_cells else 0),
         ctypes.c_void_p(half_d.data_ptr() if half_d is not None else 0), nl.num_cells, chip.width, chip.height,
-        chip.bins_x, chip.bins_y, ctypes.c_void_p(dens_d.data_ptr()), ctypes.c_void_p(ov_d.data_ptr()),
+        bx, by, ctypes.c_void_p(dens_d.data_ptr()), ctypes.c_void_p(ov_d.data_ptr()),
         ctypes.c_void_p(stream.cuda_stream))
     torch.cuda.synchronize(dev)
     return st, dens_d.cpu().numpy().copy(), float(ov_d.item())
@@ -64,7 +65,8 @@ def _check(torch, nl, chip, with_half):
     if with_half:
         half = np.stack([nl.cell_w.astype(np.float32) * 0.5, nl.cell_h.astype(np.float32) * 0.5], axis=1)
         half_d = torch.from_numpy(np.ascontiguousarray(half)).to(dev)
-    dens_d = torch.full((chip.bins_y, chip.bins_x), -1.0, dtype=torch.float64, device=dev)
+    dens_d = torch.full((chip.bins_y or chip.height, chip.bins_x or chip.width), -1.0, dtype=torch.float64,
+                        device=dev)
     ov_d = torch.full((1,), -1.0, dtype=torch.float64, device=dev)
     orc = Oracle(nl, chip)
     with E.PlacementContext(nl, chip) as ctx:
