@@ -34,7 +34,7 @@
 #include "eplace_internal.h"
 #include "job.h"
 #include "kernels.cuh"
-#include "legalize.cuh"
+#include "legal_par.cuh"
 
 namespace eplace {
 namespace {
@@ -233,9 +233,14 @@ struct LegalSlot {
   DBuf<int2> sites;
   DBuf<int2> loc;       // [N + F]: pin locations, fixed cells at the end
   DBuf<double> cost;
-  DBuf<uint64_t> work;  // map in global memory for chips beyond shared memory
   DBuf<LegalOut> out;
   PinBuf<LegalOut> hout;
+  // round buffers of the parallel legaliser (legal_par.cu)
+  DBuf<uint64_t> fm;
+  DBuf<int32_t> list, len, info, hmark, dmark, pick;
+  DBuf<uint8_t> dist, fresh;
+  DBuf<LpState> lst;
+  LpGraph graph;        // the whole legalisation: rounds in a device-side loop
   uint64_t gen = ~0ull;  // problem load this slot is prepared for
   cudaStream_t stream = nullptr;
   cudaEvent_t snap = nullptr, start = nullptr, done = nullptr;
@@ -337,9 +342,9 @@ struct eplace_ctx {
   // (from lbase), and the slots of legalisations in flight.
   bool lg_ready = false;
   DBuf<uint32_t> lg_order;
-  DBuf<uchar2> lg_msize;
+  DBuf<uchar2> lg_fsize;     // [N] footprint per cell (only when some cell is a macro)
   DBuf<uint64_t> lg_free0;
-  uint32_t lg_nmacro = 0;
+  bool lg_macros = false;
   std::vector<std::unique_ptr<LegalSlot>> lslots;
   int step_grid_full = 0;
   // Step as three ordinary launches instead of one cooperative launch: used
@@ -1034,23 +1039,25 @@ void upload_momentum(eplace_ctx *c, uint64_t iters) {
 }
 
 // Uploads what every device legalisation reads: the cell order (macros
-// first), the macros' footprints and the free map with the fixed cells.
+// first), the footprints and the free map with the fixed cells.
 void setup_gpu_legal(eplace_ctx *c) {
   AllocOn on_stream(c->stream);
   if (c->lg_ready) return;
   const HostProblem &hp = c->hp;
   if (!c->lbase) c->lbase.reset(new LegalBase(hp));
   const LegalBase &b = *c->lbase;
-  std::vector<uchar2> ms;
-  for (uint32_t i : b.order) {
-    if (hp.cw[i] * hp.ch[i] <= 1) break;
-    ms.push_back(make_uchar2(hp.cw[i], hp.ch[i]));
+  c->lg_macros = false;
+  std::vector<uchar2> fs(hp.N);
+  for (uint32_t i = 0; i < hp.N; ++i) {
+    fs[i] = make_uchar2(hp.cw[i], hp.ch[i]);
+    c->lg_macros |= hp.cw[i] * hp.ch[i] > 1;
   }
-  c->lg_nmacro = (uint32_t)ms.size();
   c->lg_order.ensure(std::max<size_t>(b.order.size(), 1));
   c->lg_order.upload(b.order.data(), b.order.size(), c->stream);
-  c->lg_msize.ensure(std::max<size_t>(ms.size(), 1));
-  c->lg_msize.upload(ms.data(), ms.size(), c->stream);
+  if (c->lg_macros) {
+    c->lg_fsize.ensure(std::max<size_t>(fs.size(), 1));
+    c->lg_fsize.upload(fs.data(), fs.size(), c->stream);
+  }
   c->lg_free0.ensure(b.free0.size());
   c->lg_free0.upload(b.free0.data(), b.free0.size(), c->stream);
   CK(cudaStreamSynchronize(c->stream));
@@ -1069,12 +1076,49 @@ void prepare_slot(eplace_ctx *c, LegalSlot &L) {
   L.loc.ensure((size_t)hp.N + hp.F + 1);
   L.cost.ensure(N1);
   const int WR = (hp.W + 63) / 64;
-  if (legalize_smem_bytes(WR, hp.H) > kLegalMaxSmem) L.work.ensure((size_t)WR * hp.H + hp.H);
+  const size_t sites = (size_t)hp.W * hp.H;
+  L.fm.ensure((size_t)WR * hp.H);
+  L.list.ensure((size_t)kLpMaxWindow * kLpList);
+  L.len.ensure(kLpMaxWindow);
+  L.info.ensure(kLpMaxWindow);
+  L.pick.ensure(kLpMaxWindow);
+  L.dist.ensure(kLpMaxWindow);
+  L.fresh.ensure(kLpMaxWindow);
+  L.hmark.ensure(sites);
+  L.dmark.ensure(sites);
+  L.lst.ensure(1);
   std::vector<int2> floc(hp.F);
   for (uint32_t f = 0; f < hp.F; ++f) floc[f] = make_int2(hp.fx[f], hp.fy[f]);
   if (hp.F) CK(cudaMemcpyAsync(L.loc.p + hp.N, floc.data(), sizeof(int2) * hp.F, cudaMemcpyHostToDevice, L.stream));
   g_h2d += sizeof(int2) * hp.F;
   CK(cudaStreamSynchronize(L.stream));
+  // The legalisation graph bakes in this load's buffers.
+  LpArgs a{};
+  a.pos = L.pos.p;
+  a.order = c->lg_order.p;
+  a.fsize = c->lg_macros ? c->lg_fsize.p : nullptr;
+  a.n = (uint32_t)c->lbase->order.size();
+  a.W = hp.W;
+  a.H = hp.H;
+  a.WR = WR;
+  a.free0 = c->lg_free0.p;
+  a.fm = L.fm.p;
+  a.list = L.list.p;
+  a.len = L.len.p;
+  a.info = L.info.p;
+  a.hmark = L.hmark.p;
+  a.dmark = L.dmark.p;
+  a.dist = L.dist.p;
+  a.fresh = L.fresh.p;
+  a.pick = L.pick.p;
+  a.st = L.lst.p;
+  a.sites = L.sites.p;
+  a.loc = L.loc.p;
+  a.cost = L.cost.p;
+  a.disp = &L.out.p->disp;
+  a.status = &L.out.p->status;
+  a.max_rounds = a.n + 64;
+  CK(lp_build_graph(a, L.graph, L.stream));
   L.gen = c->load_gen;
 }
 
@@ -1102,23 +1146,7 @@ void launch_gpu_legal(eplace_ctx *c, LegalSlot &L) {
   const HostProblem &hp = c->hp;
   CK(cudaMemsetAsync(L.out.p, 0, sizeof(LegalOut), L.stream));
   CK(cudaEventRecord(L.start, L.stream));
-  LegalArgs a;
-  a.pos = L.pos.p;
-  a.order = c->lg_order.p;
-  a.msize = c->lg_msize.p;
-  a.n_order = (uint32_t)c->lbase->order.size();
-  a.n_macro = c->lg_nmacro;
-  a.free0 = c->lg_free0.p;
-  a.work = L.work.p;
-  a.W = hp.W;
-  a.H = hp.H;
-  a.WR = (hp.W + 63) / 64;
-  a.sites = L.sites.p;
-  a.loc = L.loc.p;
-  a.cost = L.cost.p;
-  a.disp = &L.out.p->disp;
-  a.status = &L.out.p->status;
-  CK(launch_legalize(a, L.stream));
+  CK(cudaGraphLaunch(L.graph.exec, L.stream));
   HpwlArgs h{c->net_off.p, c->pin_cell.p, c->has_driver.p, L.loc.p, hp.NN, &L.out.p->hpwl};
   if (hp.NN) CK(launch_hpwl(h, grid_for((int)hp.NN, kHpwlBlock, c->num_sms * 2), L.stream));
   CK(cudaMemcpyAsync(L.hout.p, L.out.p, sizeof(LegalOut), cudaMemcpyDeviceToHost, L.stream));
@@ -1746,7 +1774,7 @@ struct JobState {
           const LegalOut &o = *L.hout.p;
           float lms = 0.f;
           if (cudaEventElapsedTime(&lms, L.start, L.done) == cudaSuccess) cp->secs = 1e-3 * lms;
-          cp->st = o.status == 0 ? EPLACE_OK : EPLACE_ERR_NO_BELS;
+          cp->st = o.status == 0 ? EPLACE_OK : (o.status == 1 ? EPLACE_ERR_NO_BELS : EPLACE_ERR_PLACEMENT_FAILED);
           cp->disp = o.disp;
           cp->hpwl = (int64_t)o.hpwl;
         }
@@ -2227,9 +2255,10 @@ uint64_t eplace_ctx::device_bytes() const {
   add(rho_h); add(rho_l); add(Tt_h); add(Tt_l); add(Exh_h); add(Exh_l); add(Eyh_h); add(Eyh_l);
   add(Ut_h); add(Ut_l); add(Vt_h); add(Vt_l); add(B1t_h); add(B1t_l); add(L2_h); add(L2_l);
   add(B3t_h); add(B3t_l); add(B5t_h); add(B5t_l); add(L4_h); add(L4_l); add(L6_h); add(L6_l);
-  add(B3gt_h); add(B3gt_l); add(L6g_h); add(L6g_l); add(lg_order); add(lg_msize); add(lg_free0);
+  add(B3gt_h); add(B3gt_l); add(L6g_h); add(L6g_l); add(lg_order); add(lg_fsize); add(lg_free0);
   for (const auto &l : lslots) {
-    add(l->pos); add(l->sites); add(l->loc); add(l->cost); add(l->work); add(l->out);
+    add(l->pos); add(l->sites); add(l->loc); add(l->cost); add(l->out); add(l->fm); add(l->list); add(l->len); add(l->info);
+    add(l->hmark); add(l->dmark); add(l->pick); add(l->dist); add(l->fresh); add(l->lst);
   }
   return b;
 }
@@ -2665,7 +2694,7 @@ eplace_status eplace_stage_legalize(eplace_ctx *c, const float *x, const float *
   if (!c || (c->hp.N && (!x || !y || !sx || !sy))) return EPLACE_ERR_INVALID;
   const HostProblem &hp = c->hp;
   if (!legalize_supported(hp.W, hp.H)) {
-    set_err(c, "the device legaliser supports chips up to 4096 sites wide");
+    set_err(c, "the device legaliser supports chips up to 4096 x 4096 sites");
     return EPLACE_ERR_INVALID;
   }
   try {
@@ -2688,8 +2717,8 @@ eplace_status eplace_stage_legalize(eplace_ctx *c, const float *x, const float *
     CK(cudaStreamSynchronize(L->stream));
     const LegalOut &o = *L->hout.p;
     if (o.status != 0) {
-      set_err(c, "logic");
-      return EPLACE_ERR_NO_BELS;
+      set_err(c, o.status == 1 ? "logic" : "device legaliser stopped at an internal limit");
+      return o.status == 1 ? EPLACE_ERR_NO_BELS : EPLACE_ERR_PLACEMENT_FAILED;
     }
     for (uint32_t i = 0; i < hp.N; ++i) {
       sx[i] = s[i].x;

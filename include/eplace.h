@@ -86,10 +86,12 @@ typedef enum {
 /* Where the periodic legalisations run.  Both give the same bindings, the
  * same displacement and the same HPWL (the reference's greedy choice and
  * tie-break, electro_place/mod.rs:206-255).  EPLACE_LEGAL_HOST: host
- * threads, snapshots copied to pinned memory.  EPLACE_LEGAL_GPU: one warp
- * per checkpoint on the device, concurrent with the Nesterov loop, HPWL on
- * the device; only the best checkpoint's binding is copied back.  Chips
- * wider than 4096 sites fall back to EPLACE_LEGAL_HOST. */
+ * threads, snapshots copied to pinned memory.  EPLACE_LEGAL_GPU: on the
+ * device, concurrent with the Nesterov loop, HPWL on the device; only the
+ * best checkpoint's binding is copied back.  The device legaliser places the
+ * cells in rounds (candidate lists in parallel, one serial pass over the
+ * cells whose lists interact), as one CUDA graph per checkpoint.  Chips
+ * larger than 4096 x 4096 sites fall back to EPLACE_LEGAL_HOST. */
 typedef enum {
   EPLACE_LEGAL_HOST = 0,
   EPLACE_LEGAL_GPU = 1
@@ -265,12 +267,13 @@ eplace_status eplace_profile_stages(eplace_ctx *ctx, const eplace_cfg *cfg, cons
 eplace_status eplace_legalize(eplace_ctx *ctx, const float *x, const float *y,
                               int32_t *site_x, int32_t *site_y, double *displacement);
 
-/* The same legalisation on the GPU (one warp, free-site bitmap in shared
- * memory; results identical to eplace_legalize), followed by the device
- * HPWL of the binding.  Replaces legalize_electro (electro_place/mod.rs:
- * 206-255) + total_hpwl (metrics/wirelength.rs:10-51).  Returns
- * EPLACE_ERR_NO_BELS when a cell finds no free site; EPLACE_ERR_INVALID for
- * chips wider than 4096 sites. */
+/* The same legalisation on the GPU (rounds of parallel candidate lists and a
+ * serial pass over the interacting cells; results identical to
+ * eplace_legalize), followed by the device HPWL of the binding.  Replaces
+ * legalize_electro (electro_place/mod.rs:206-255) + total_hpwl
+ * (metrics/wirelength.rs:10-51).  Returns EPLACE_ERR_NO_BELS when a cell
+ * finds no free site; EPLACE_ERR_INVALID for chips larger than 4096 x 4096
+ * sites. */
 eplace_status eplace_stage_legalize(eplace_ctx *ctx, const float *x, const float *y,
                                     int32_t *site_x, int32_t *site_y, double *displacement,
                                     int64_t *hpwl);

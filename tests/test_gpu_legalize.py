@@ -148,3 +148,22 @@ def test_run_with_device_legalizer_macros():
     assert a.hpwl == b.hpwl and a.best_iter == b.best_iter
     assert np.array_equal(a.bel_tile, b.bel_tile)
     assert a.trajectory == b.trajectory
+
+
+def test_device_legalizer_bench_geometry():
+    """The benchmark job's geometry (200k cells, 5 % macros, 1024^2 sites)
+    with the cells drawn into one central pile, as in the crowded middle of
+    a run (many cells end up ~200 sites from their target, in long chains
+    of cells that depend on each other): the device legaliser's bindings,
+    displacement and HPWL equal the host legaliser's bit for bit."""
+    nl, chip, _ = E.workload("electro_200k_1024")
+    rng = np.random.default_rng(41)
+    n, W = nl.num_cells, chip.width
+    x = np.clip(rng.normal(W / 2, W * 0.13, n), 0, W - 1).astype(np.float32)
+    y = np.clip(rng.normal(W / 2, W * 0.13, n), 0, W - 1).astype(np.float32)
+    with E.PlacementContext(nl, chip) as ctx:
+        hx, hy, hd = ctx.legalize(x, y)
+        dx, dy, dd, dh = ctx.legalize_device(x, y)
+    assert np.array_equal(dx, hx) and np.array_equal(dy, hy)
+    assert dd == hd
+    assert dh == E.hpwl_host(nl, chip, hx, hy)
