@@ -70,7 +70,7 @@ class Opts(ctypes.Structure):
         ("max_inflight", ctypes.c_int32),
         ("field_mode", ctypes.c_int32),
         ("legal_mode", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 1),
+        ("wait_limit_us", ctypes.c_int32),
     ]
 
 
@@ -211,6 +211,7 @@ PROTOTYPES = {
         [ctypes.c_void_p, ctypes.c_uint64] + [c_f32p] * 6 + [c_f32p] * 6 + [c_f64p, c_f64p, c_f32p, c_f32p],
     ),
     "eplace_stage_hpwl": (ctypes.c_int, [ctypes.c_void_p, c_i32p, c_i32p, c_i64p]),
+    "eplace_stage_barrier_timeout": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_uint32]),
     "eplace_legalize": (ctypes.c_int, [ctypes.c_void_p, c_f32p, c_f32p, c_i32p, c_i32p, c_f64p]),
     "eplace_ctx_load": (ctypes.c_int, [ctypes.c_void_p, P(Netlist), P(Chip)]),
     "eplace_stage_legalize": (ctypes.c_int, [ctypes.c_void_p, c_f32p, c_f32p, c_i32p, c_i32p, c_f64p, c_i64p]),

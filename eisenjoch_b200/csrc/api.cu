@@ -270,6 +270,7 @@ struct eplace_ctx {
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   std::string err;
   int num_sms = 0;
+  int64_t spin_cycles = 0;  // bound of the step's barrier waits for the current run (0: kernel default)
   int step_grid = 0;
   std::vector<double> pw_host;
   double total_area = 0.0;
@@ -1417,9 +1418,18 @@ static void reset_state(eplace_ctx *c, const std::vector<int32_t> &sx, const std
   sc.lam_init = 0;
   sc.iter = 0;
   sc.err = 0;
+  sc.spin_cycles = c->spin_cycles;
   c->sc.upload(&sc, 1, s);
   c->bar.zero(s);
   CK(cudaStreamSynchronize(s));
+}
+
+// SM clock cycles of a wait limit given in microseconds (0: the kernel default).
+static int64_t wait_cycles(int device, int32_t us) {
+  if (us <= 0) return 0;
+  int khz = 0;
+  if (cudaDeviceGetAttribute(&khz, cudaDevAttrClockRate, device) != cudaSuccess || khz <= 0) khz = 2000000;
+  return (int64_t)us * (int64_t)khz / 1000;
 }
 
 namespace {
@@ -1540,6 +1550,7 @@ struct JobState {
         c->split_step = want_split;
         ++c->buf_epoch;
       }
+      c->spin_cycles = wait_cycles(c->device, opts.wait_limit_us);
       reset_state(c, isx, isy, &cfg);
       autotune_launches(c, gamma, opts.field_mode, tc);
       mark("device_reset");
@@ -2646,6 +2657,49 @@ eplace_status eplace_stage_step(eplace_ctx *c, uint64_t iter, const float *look_
     out[1] = L.step_norm[1];
     out[2] = L.alpha[0];
     out[3] = L.alpha[1];
+  } catch (const CudaError &e) {
+    return cuda_fail(c, e);
+  }
+  return EPLACE_OK;
+}
+
+eplace_status eplace_stage_barrier_timeout(eplace_ctx *c, int32_t wait_limit_us, uint32_t phantom) {
+  if (!c || wait_limit_us <= 0 || phantom == 0) return EPLACE_ERR_INVALID;
+  const HostProblem &hp = c->hp;
+  if (hp.N == 0) return EPLACE_ERR_INVALID;
+  try {
+    CK(cudaSetDevice(c->device));
+    if (phantom >= (uint32_t)c->step_grid) {
+      set_err(c, "phantom arrivals must be below the step's grid size");
+      return EPLACE_ERR_INVALID;
+    }
+    eplace_cfg cfg;
+    eplace_cfg_default(&cfg);
+    std::vector<int32_t> isx, isy;
+    std::string msg;
+    const eplace_status st = initial_placement(hp, cfg.seed, isx, isy, msg);
+    if (st != EPLACE_OK) {
+      set_err(c, msg);
+      return st;
+    }
+    ensure_log(c, 2);
+    upload_momentum(c, 2);
+    const int64_t saved = c->spin_cycles;
+    c->spin_cycles = wait_cycles(c->device, wait_limit_us);
+    reset_state(c, isx, isy, &cfg);
+    c->spin_cycles = saved;
+    // the arrival count starts `phantom` ahead: the block whose ticket lands
+    // in the next multiple of the grid waits for arrivals that never come
+    const unsigned long long start = phantom;
+    CK(cudaMemcpyAsync(c->bar.p, &start, sizeof(start), cudaMemcpyHostToDevice, c->stream));
+    CK(launch_step(step_args(c), c->step_grid, c->stream));
+    DevScalars sc{};
+    CK(cudaMemcpyAsync(&sc, c->sc.p, sizeof(sc), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (sc.err) {
+      set_err(c, "a bounded device wait timed out");
+      return EPLACE_ERR_TIMEOUT;
+    }
   } catch (const CudaError &e) {
     return cuda_fail(c, e);
   }

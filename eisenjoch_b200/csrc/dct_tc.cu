@@ -16,7 +16,8 @@
 // Poisson scaling (density.rs:114-153), or the final FP32 field.
 //
 // Every mbarrier wait is bounded: on timeout the CTA records an error in
-// *err, skips the remaining work, releases its TMEM and returns.
+// *err, skips the remaining work, waits (bounded again) for the MMAs and
+// tensor loads it has in flight, releases its TMEM and returns.
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -140,6 +141,7 @@ __global__ void __launch_bounds__(128, 1)
   uint64_t *done = empty + STAGES;
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(done + 1);
   __shared__ int failed;
+  __shared__ int s_issued;  // stage loads the producer issued
 
   const int z = blockIdx.z;
   const TcOperandMaps &om = maps.op[z];
@@ -149,6 +151,7 @@ __global__ void __launch_bounds__(128, 1)
 
   if (threadIdx.x == 0) {
     failed = 0;
+    s_issued = 0;
     for (int s = 0; s < STAGES; ++s) {
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
@@ -167,12 +170,14 @@ __global__ void __launch_bounds__(128, 1)
 
   if (threadIdx.x == 0) {
     // TMA producer
+    int issued = 0;
     for (int kb = 0; kb < nk; ++kb) {
       const int s = kb % STAGES;
       if (kb >= STAGES && !mbar_wait(&empty[s], ((kb / STAGES) - 1) & 1)) {
         atomicExch(&failed, 1);
         break;
       }
+      ++issued;
       uint8_t *st = smem + s * S::STAGE_BYTES;
       mbar_expect_tx(&full[s], S::STAGE_BYTES);
       tma_load_2d(st, &om.a_hi, kb * BK, m0, &full[s]);
@@ -180,6 +185,7 @@ __global__ void __launch_bounds__(128, 1)
       tma_load_2d(st + 2 * S::A_BYTES, BN == 32 ? &om.b_hi32 : &om.b_hi, kb * BK, n0, &full[s]);
       tma_load_2d(st + 2 * S::A_BYTES + S::B_BYTES, BN == 32 ? &om.b_lo32 : &om.b_lo, kb * BK, n0, &full[s]);
     }
+    s_issued = issued;
   } else if (threadIdx.x == 32) {
     // MMA issuer: M = 128, N = BN, BF16 x BF16 -> FP32, both K-major.
     const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
@@ -206,13 +212,22 @@ __global__ void __launch_bounds__(128, 1)
       }
       mma_commit(&empty[s]);
     }
-    if (ok) mma_commit(done);
+    // Also after a timeout: `done` then tracks every MMA issued so far, so
+    // the CTA's wait on it below drains them before TMEM is released.
+    mma_commit(done);
+    (void)ok;
   }
   __syncwarp();
   // Epilogue: warp w owns accumulator rows 32w..32w+31 (TMEM lanes).
   bool ok = mbar_wait(done, 0);
   __syncthreads();
   if (failed) ok = false;
+  if (!ok && threadIdx.x == 0) {
+    // After a timeout anywhere in the CTA, the loads still in flight (at
+    // most the last STAGES issued, one per stage) land before the CTA may
+    // leave: bounded waits on their stages' full barriers.
+    for (int kb = max(0, s_issued - STAGES); kb < s_issued; ++kb) mbar_wait(&full[kb % STAGES], (kb / STAGES) & 1);
+  }
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   if (ok) {
     const int r = m0 + warp * 32 + lane;

@@ -715,19 +715,25 @@ bool sgemm_small_tile(int M, int N, int nb, int K) {
 
 // ---------------------------------------------------------------------------
 // Grid barrier for the cooperative step kernel.  Every wait is bounded: on
-// timeout the block records the error in sc->err and carries on, so the
-// kernel always terminates and the host reports EPLACE_ERR_TIMEOUT.
+// timeout the block records the error in sc->err and leaves the kernel, so
+// the kernel always terminates, no block computes on partial data, and the
+// host reports EPLACE_ERR_TIMEOUT (the next run resets the device state).
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void grid_barrier(unsigned *bar, DevScalars *sc) {
+__device__ __forceinline__ bool grid_barrier(unsigned *bar, DevScalars *sc) {
   // bar[0..1] is one 64-bit arrival count that is never reset inside a run:
   // every launch on it has the same grid and passes whole barriers, so a
   // launch starts at a multiple of gridDim.x, and barrier k of the run is
   // complete when the count reaches (k + 1) * gridDim.x.  The last block's
   // own add releases the others (no reset, no second word to publish).
-  // The host zeroes the count at every load and run start.
+  // The host zeroes the count at every load and run start.  The wait is
+  // bounded (sc->spin_cycles): a block that gives up records sc->err and
+  // returns false, and its caller leaves the kernel.
+  __shared__ int gave_up;
   __syncthreads();
   if (threadIdx.x == 0) {
+    gave_up = 0;
     unsigned long long *cnt = reinterpret_cast<unsigned long long *>(bar);
+    const long long limit = sc->spin_cycles > 0 ? sc->spin_cycles : kSpinCycles;
     __threadfence();  // this block's writes before its arrival
     const unsigned long long old = atomicAdd(cnt, 1ull);
     const unsigned long long target = old - old % gridDim.x + gridDim.x;
@@ -736,8 +742,9 @@ __device__ __forceinline__ void grid_barrier(unsigned *bar, DevScalars *sc) {
       unsigned long long v;
       asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(cnt) : "memory");
       if (v >= target) break;
-      if (clock64() - t0 > kSpinCycles) {
+      if (clock64() - t0 > limit) {
         atomicExch(&sc->err, 1);
+        gave_up = 1;
         break;
       }
       __nanosleep(32);
@@ -745,6 +752,7 @@ __device__ __forceinline__ void grid_barrier(unsigned *bar, DevScalars *sc) {
     __threadfence();
   }
   __syncthreads();
+  return !gave_up;
 }
 
 // Field gather of a 1x1 footprint: it touches at most 2 x 2 bins (bins are
@@ -961,7 +969,7 @@ __global__ void __launch_bounds__(kStepBlock, 2) k_step(const StepArgs a) {
     if (threadIdx.x == 0)
       for (int k = 0; k < 4; ++k) a.part[4 * blockIdx.x + k] = v[k];
     if (a.mode == 2) return;
-    grid_barrier(a.bar, a.sc);
+    if (!grid_barrier(a.bar, a.sc)) return;
   }
 
   // Pass-2 partials: part[] again after a barrier (cooperative), else part_b[].
@@ -977,7 +985,7 @@ __global__ void __launch_bounds__(kStepBlock, 2) k_step(const StepArgs a) {
       lam_init = true;
     }
     if (a.mode == 0 || a.mode == 3) {
-      if (coop) grid_barrier(a.bar, a.sc);  // everyone has read part[] before it is reused
+      if (coop) if (!grid_barrier(a.bar, a.sc)) return;  // everyone has read part[] before it is reused
       for (int k = 0; k < 4; ++k) v[k] = 0.0;
       for (uint32_t i = tid0; i < a.N; i += gstride) {
         const float2 g = combine(a, i, a.tmp_wl[i], a.tmp_den[i], lam, false);
@@ -993,7 +1001,7 @@ __global__ void __launch_bounds__(kStepBlock, 2) k_step(const StepArgs a) {
       if (threadIdx.x == 0)
         for (int k = 0; k < 4; ++k) part2nd[4 * blockIdx.x + k] = v[k];
       if (a.mode == 3) return;
-      grid_barrier(a.bar, a.sc);
+      if (!grid_barrier(a.bar, a.sc)) return;
     }
   } else if (a.mode == 3) {
     return;

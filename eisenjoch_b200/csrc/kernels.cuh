@@ -19,6 +19,7 @@ struct DevScalars {
   int32_t iter;        // index of the next iteration to execute
   int32_t err;         // non-zero: a bounded wait gave up
   int32_t pad_;
+  int64_t spin_cycles; // bound of every grid-barrier wait in SM clock cycles (0: the default, ~2 s)
 };
 
 // One record per executed iteration (fields of the reference log line).

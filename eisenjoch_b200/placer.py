@@ -62,6 +62,7 @@ class RunOptions:
     max_inflight: int = 3
     field_mode: int = _abi.EPLACE_FIELD_REFERENCE
     legal_mode: int = _abi.EPLACE_LEGAL_HOST
+    wait_limit_us: int = 0  # bound of each device grid-barrier wait; 0 = about 2 s
 
     def to_c(self):
         o = _abi.Opts()
@@ -73,6 +74,7 @@ class RunOptions:
         o.max_inflight = int(self.max_inflight)
         o.field_mode = int(self.field_mode)
         o.legal_mode = int(self.legal_mode)
+        o.wait_limit_us = int(self.wait_limit_us)
         return o
 
 

@@ -105,7 +105,9 @@ typedef struct {
   int32_t max_inflight;        /* intervals launched ahead of the host; default 3 */
   int32_t field_mode;          /* eplace_field_mode; default EPLACE_FIELD_REFERENCE */
   int32_t legal_mode;          /* eplace_legal_mode; default EPLACE_LEGAL_HOST */
-  int32_t reserved[1];
+  int32_t wait_limit_us;       /* bound of each grid-barrier wait of the step kernel, microseconds;
+                                  0 = about 2 s.  A wait that runs out ends the run with
+                                  EPLACE_ERR_TIMEOUT; the context stays usable. */
 } eplace_opts;
 
 void eplace_opts_default(eplace_opts *opts);
@@ -246,6 +248,17 @@ eplace_status eplace_stage_step(eplace_ctx *ctx, uint64_t iter, const float *loo
                                 float *x_prev, float *y_prev, float *gprev_x, float *gprev_y,
                                 double *scal, double *out, float *next_look_x,
                                 float *next_look_y);
+
+/* The failure path of a bounded device wait, on demand.  No counterpart in
+ * the reference.  Resets the context's solver state to the initial
+ * placement of seed 1 and runs one fused step in its cooperative form (the
+ * form with grid barriers) with `phantom` arrivals already counted on the
+ * barrier (1 <= phantom < the step's grid size), so one block's wait can
+ * never be met and must run out after wait_limit_us (> 0).  Returns
+ * EPLACE_ERR_TIMEOUT when the wait ran out, as it must; the context is then
+ * usable for the next run, which resets the device state.  Nothing faults
+ * or hangs: every wait is bounded. */
+eplace_status eplace_stage_barrier_timeout(eplace_ctx *ctx, int32_t wait_limit_us, uint32_t phantom);
 
 /* Integer HPWL of a binding (anchor sites per movable cell), replaces
  * total_hpwl (metrics/wirelength.rs:10-51). */
