@@ -30,6 +30,13 @@ FLAGS = [
 ]
 
 
+# Host-only sources compiled by the host C++ compiler: the legaliser uses x86
+# intrinsics with per-function targets, which nvcc's front end does not take.
+HOST_CXX = {"host.cpp"}
+CXX = os.environ.get("CXX", "g++")
+CXXFLAGS = ["-O3", "-std=c++17", "-fPIC", "-Wall", "-ffp-contract=off"]
+
+
 def sources():
     out = []
     for name in sorted(os.listdir(CSRC)):
@@ -63,7 +70,9 @@ def build(force=False, verbose=False):
     for src in sources():
         obj = os.path.join(objdir, os.path.basename(src) + ".o")
         cmd = [NVCC] + ARCH + FLAGS + ["-I", os.path.join(ROOT, "include"), "-c", src, "-o", obj]
-        if src.endswith(".cpp"):
+        if os.path.basename(src) in HOST_CXX:
+            cmd = [CXX] + CXXFLAGS + ["-I", os.path.join(ROOT, "include"), "-c", src, "-o", obj]
+        elif src.endswith(".cpp"):
             cmd = [NVCC, "-x", "cu"] + ARCH + FLAGS + ["-I", os.path.join(ROOT, "include"), "-c", src, "-o", obj]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:

@@ -80,6 +80,7 @@ struct Legalizer {
   const LegalBase &base_;
   std::vector<uint64_t> free_, sum_;
   std::vector<int32_t> lc_, rc_;  // per-row candidate cache of the unit-cell search
+  bool simd_ = false;             // AVX2 available: the search takes four rows per step
 };
 
 // total_hpwl (metrics/wirelength.rs:10-51) on the host.

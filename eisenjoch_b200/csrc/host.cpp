@@ -1,6 +1,8 @@
 // host.cpp -- host-side parts of the ElectroPlace path: problem validation,
 // the reference's initial placement and pin weights, the exact greedy
 // legaliser, integer HPWL and the synthetic netlist generator.
+#include <immintrin.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -212,6 +214,8 @@ LegalBase::LegalBase(const HostProblem &hp) : W(hp.W), H(hp.H) {
 }
 
 Legalizer::Legalizer(const HostProblem &hp, const LegalBase &base) : hp_(hp), base_(base) {
+  __builtin_cpu_init();
+  simd_ = __builtin_cpu_supports("avx2");
   free_.resize(base.free0.size());
   sum_.resize(base.sum0.size());
   lc_.resize(std::max(base.H, 0));
@@ -293,6 +297,178 @@ inline int nearest_ints(double t, int32_t n, int32_t (&out)[2]) {
     if (out[i] >= 0 && out[i] < n) out[m++] = out[i];
   return m;
 }
+
+// One unit cell's search over the rows (see Legalizer::run).
+struct RowSearch {
+  const uint64_t *fm;
+  const uint64_t *sm;
+  int32_t *lc, *rc;
+  int32_t W, H, WR;
+  double tx, ty;
+  int32_t fx0;
+  bool cacheable;
+  double best;
+  int64_t best_t;
+};
+
+// The row's two candidates: from the cache when its entry covers fx0, else
+// from the bitmap (and then cached).
+inline void row_candidates(RowSearch &s, int32_t row, int32_t &l, int32_t &rr) {
+  if (s.cacheable && s.lc[row] <= s.fx0 && s.fx0 < s.rc[row]) {
+    l = s.lc[row];
+    rr = s.rc[row] < s.W ? s.rc[row] : -1;
+    return;
+  }
+  const uint64_t *r = s.fm + (size_t)row * s.WR;
+  const uint64_t *rs = s.sm ? s.sm + row : nullptr;
+  l = free_at_or_left(r, rs, std::min(s.fx0, s.W - 1));
+  rr = free_at_or_right(r, rs, s.fx0 + 1, s.W, s.WR);
+  if (s.cacheable) {
+    s.lc[row] = l;
+    s.rc[row] = rr >= 0 ? rr : s.W;
+  }
+}
+
+inline void consider(RowSearch &s, double cost, int64_t t) {
+  if (cost < s.best || (cost == s.best && t < s.best_t)) {
+    s.best = cost;
+    s.best_t = t;
+  }
+}
+
+inline void scan_row(RowSearch &s, int32_t row) {
+  const double dy = (double)row - s.ty;
+  const double dy2 = dy * dy;
+  int32_t l, rr;
+  row_candidates(s, row, l, rr);
+  if (l >= 0) {
+    const double dx = (double)l - s.tx;
+    consider(s, dx * dx + dy2, (int64_t)row * s.W + l);
+  }
+  if (rr >= 0) {
+    const double dx = (double)rr - s.tx;
+    consider(s, dx * dx + dy2, (int64_t)row * s.W + rr);
+  }
+}
+
+// Whether a side whose next row is `row` is finished: off the grid, or
+// dy^2 above the best cost (no row beyond can win or tie).
+inline bool side_done(const RowSearch &s, int32_t row) {
+  if (row < 0 || row >= s.H) return true;
+  const double dy = (double)row - s.ty;
+  return s.best_t >= 0 && dy * dy > s.best;
+}
+
+// Rows outward from cy, one at a time.
+void search_rows(RowSearch &s, int32_t cy) {
+  scan_row(s, cy);
+  bool up = true, down = true;
+  for (int32_t d = 1; up || down; ++d) {
+    if (down) {
+      if (side_done(s, cy - d)) down = false;
+      else scan_row(s, cy - d);
+    }
+    if (up) {
+      if (side_done(s, cy + d)) up = false;
+      else scan_row(s, cy + d);
+    }
+  }
+}
+
+// The same search, four consecutive rows per step where they are all on the
+// grid (AVX2).  The caches of the four rows are checked together and
+// refreshed one by one only where stale; then the eight candidates' costs
+// are formed with 256-bit doubles as the scalar code forms them (separate
+// multiply and add; the target has no FMA, so nothing is contracted), and
+// only when one of them can improve on or tie the best does the block go
+// through the scalar comparison with its tile tie-break.  Rows beyond a
+// side's stopping row cannot win or tie, so visiting them changes nothing:
+// the result is the minimum over all rows, as in the one-row search.
+__attribute__((target("avx2"))) inline void rows4(RowSearch &s, int32_t r0) {
+  const __m128i fxv = _mm_set1_epi32(s.fx0);
+  __m128i l = _mm_loadu_si128(reinterpret_cast<const __m128i *>(s.lc + r0));
+  __m128i r = _mm_loadu_si128(reinterpret_cast<const __m128i *>(s.rc + r0));
+  // stale: lc > fx0 or rc <= fx0
+  const __m128i stale =
+      _mm_or_si128(_mm_cmpgt_epi32(l, fxv), _mm_cmpgt_epi32(_mm_add_epi32(fxv, _mm_set1_epi32(1)), r));
+  if (_mm_movemask_epi8(stale)) {
+    // Refresh only the rows still within reach; a row whose dy^2 exceeds
+    // the best cost cannot win or tie, so it leaves the block instead.
+    alignas(16) int32_t la[4], ra[4];
+    for (int32_t k = 0; k < 4; ++k) {
+      const int32_t row = r0 + k;
+      const double d = (double)row - s.ty;
+      if (s.best_t >= 0 && d * d > s.best) {
+        la[k] = -1;
+        ra[k] = s.W;
+      } else {
+        int32_t a, b;
+        row_candidates(s, row, a, b);
+        la[k] = a;
+        ra[k] = b >= 0 ? b : s.W;
+      }
+    }
+    l = _mm_load_si128(reinterpret_cast<const __m128i *>(la));
+    r = _mm_load_si128(reinterpret_cast<const __m128i *>(ra));
+  }
+  const __m256d txv = _mm256_set1_pd(s.tx);
+  const __m256d dy = _mm256_sub_pd(_mm256_cvtepi32_pd(_mm_add_epi32(_mm_set1_epi32(r0), _mm_setr_epi32(0, 1, 2, 3))),
+                                   _mm256_set1_pd(s.ty));
+  const __m256d dy2 = _mm256_mul_pd(dy, dy);
+  const __m256d dxl = _mm256_sub_pd(_mm256_cvtepi32_pd(l), txv);
+  const __m256d dxr = _mm256_sub_pd(_mm256_cvtepi32_pd(r), txv);
+  const __m256d cl = _mm256_add_pd(_mm256_mul_pd(dxl, dxl), dy2);
+  const __m256d cr = _mm256_add_pd(_mm256_mul_pd(dxr, dxr), dy2);
+  const __m256d okl = _mm256_castsi256_pd(_mm256_cvtepi32_epi64(_mm_cmpgt_epi32(l, _mm_set1_epi32(-1))));
+  const __m256d okr = _mm256_castsi256_pd(_mm256_cvtepi32_epi64(_mm_cmplt_epi32(r, _mm_set1_epi32(s.W))));
+  const __m256d bv = _mm256_set1_pd(s.best);
+  const __m256d le = _mm256_or_pd(_mm256_and_pd(okl, _mm256_cmp_pd(cl, bv, _CMP_LE_OQ)),
+                                  _mm256_and_pd(okr, _mm256_cmp_pd(cr, bv, _CMP_LE_OQ)));
+  if (!_mm256_movemask_pd(le)) return;
+  alignas(32) double al[4], ar[4];
+  _mm256_store_pd(al, cl);
+  _mm256_store_pd(ar, cr);
+  alignas(16) int32_t li[4], ri[4];
+  _mm_store_si128(reinterpret_cast<__m128i *>(li), l);
+  _mm_store_si128(reinterpret_cast<__m128i *>(ri), r);
+  for (int32_t k = 0; k < 4; ++k) {
+    const int64_t row = r0 + k;
+    if (li[k] >= 0) consider(s, al[k], row * s.W + li[k]);
+    if (ri[k] < s.W) consider(s, ar[k], row * s.W + ri[k]);
+  }
+}
+
+__attribute__((target("avx2"))) void search_rows4(RowSearch &s, int32_t cy) {
+  scan_row(s, cy);
+  bool up = true, down = true;
+  int32_t dd = 1, du = 1;
+  while (up || down) {
+    if (down) {
+      const int32_t row = cy - dd;
+      if (side_done(s, row)) {
+        down = false;
+      } else if (row >= 3) {
+        rows4(s, row - 3);
+        dd += 4;
+      } else {
+        scan_row(s, row);
+        dd += 1;
+      }
+    }
+    if (up) {
+      const int32_t row = cy + du;
+      if (side_done(s, row)) {
+        up = false;
+      } else if (row + 3 < s.H) {
+        rows4(s, row);
+        du += 4;
+      } else {
+        scan_row(s, row);
+        du += 1;
+      }
+    }
+  }
+}
 }  // namespace
 
 eplace_status Legalizer::run(const float *x, const float *y, size_t stride, int32_t *site_x, int32_t *site_y,
@@ -334,65 +510,11 @@ eplace_status Legalizer::run(const float *x, const float *y, size_t stride, int3
         // cell of a crowded region (whose neighbours in the order target the
         // same region) reads them instead of searching the bitmap.  A row's
         // entry dies when one of its two sites is taken.
-        const bool cacheable = fx0 >= 0 && fx0 <= W - 1;
-        auto scan_row = [&](int32_t row) {
-          const double dy = (double)row - ty;
-          const double dy2 = dy * dy;
-          int32_t l, rr;
-          if (cacheable && lc[row] <= fx0 && fx0 < rc[row]) {
-            l = lc[row];
-            rr = rc[row] < W ? rc[row] : -1;
-          } else {
-            const uint64_t *r = fm + (size_t)row * WR;
-            const uint64_t *rs = sm ? sm + row : nullptr;
-            l = free_at_or_left(r, rs, std::min(fx0, W - 1));
-            rr = free_at_or_right(r, rs, fx0 + 1, W, WR);
-            if (cacheable) {
-              lc[row] = l;
-              rc[row] = rr >= 0 ? rr : W;
-            }
-          }
-          if (l >= 0) {
-            const double dx = (double)l - tx, cost = dx * dx + dy2;
-            const int64_t t = (int64_t)row * W + l;
-            if (cost < best || (cost == best && t < best_t)) {
-              best = cost;
-              best_t = t;
-            }
-          }
-          if (rr >= 0) {
-            const double dx = (double)rr - tx, cost = dx * dx + dy2;
-            const int64_t t = (int64_t)row * W + rr;
-            if (cost < best || (cost == best && t < best_t)) {
-              best = cost;
-              best_t = t;
-            }
-          }
-        };
-        scan_row(cy);
-        bool up = true, down = true;
-        for (int32_t d = 1; up || down; ++d) {
-          if (down) {
-            const int32_t row = cy - d;
-            if (row < 0) {
-              down = false;
-            } else {
-              const double dy = (double)row - ty;
-              if (best_t >= 0 && dy * dy > best) down = false;
-              else scan_row(row);
-            }
-          }
-          if (up) {
-            const int32_t row = cy + d;
-            if (row >= H) {
-              up = false;
-            } else {
-              const double dy = (double)row - ty;
-              if (best_t >= 0 && dy * dy > best) up = false;
-              else scan_row(row);
-            }
-          }
-        }
+        RowSearch rs{fm, sm, lc, rc, W, H, WR, tx, ty, fx0, fx0 >= 0 && fx0 <= W - 1, best, best_t};
+        if (simd_ && rs.cacheable) search_rows4(rs, cy);
+        else search_rows(rs, cy);
+        best = rs.best;
+        best_t = rs.best_t;
       }
     } else {
       // Macro: anchor rows outward from the target anchor row.  In anchor

@@ -231,3 +231,24 @@ def test_workload_table_is_plain_data():
         for k, v in w["spec"].items():
             assert getattr(spec, k) == v, (name, k)
         assert E.WORKLOADS[name]["cfg"] == w["cfg"]
+
+
+def test_host_legalizer_dense_pile_equals_oracle():
+    """A central pile (cells up to ~60 sites from their nearest free site,
+    long row searches: the four-rows-per-step path on CPUs with AVX2) with
+    5 % macros: the product's host legaliser equals the oracle's ring search
+    (the reference's choice and tie-break) site for site, and the FP64
+    displacement bit for bit."""
+    nl, chip = E.synth_netlist(E.SynthSpec(seed=12, num_cells=20000, num_nets=22000, num_pads=300, width=256,
+                                           height=256, cluster_size=64, macro_fraction=0.05))
+    rng = np.random.default_rng(4)
+    n = nl.num_cells
+    x = np.clip(rng.normal(128, 28, n), 0, 255).astype(np.float32)
+    y = np.clip(rng.normal(128, 28, n), 0, 255).astype(np.float32)
+    sx, sy, disp = E.legalize_host(nl, chip, x, y)
+    st, ox, oy, odisp = O.Oracle(nl, chip).legalize(x, y, 1)
+    assert st == 0
+    assert np.array_equal(sx, ox) and np.array_equal(sy, oy)
+    assert disp == odisp
+    far = (sx - x) ** 2 + (sy - y) ** 2 > 400
+    assert far.sum() > 1000  # the pile is real: many long searches
