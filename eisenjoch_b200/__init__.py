@@ -4,6 +4,7 @@ The computation lives in libeplace.so (CUDA kernels + C ABI, include/eplace.h);
 this package is the host-side mirror of the reference placer interface.
 """
 
+from . import frontend  # noqa: F401
 from ._abi import LIB_PATH, lib  # noqa: F401
 from .placer import (  # noqa: F401
     WORKLOADS,
