@@ -779,7 +779,7 @@ def ours(args, dist):
             "dct": {"fp32": "fp32 simt gemm", "bf16x3": "tcgen05 bf16 3-term split, fp32 accumulate"}[args.dct],
             "field_mode": args.field_mode + ("" if args.field_mode == "reference" else
                                              " (extension: the reference field does not spread cells; on this "
-                                             "workload the reference FP64 loop reaches NaN near iteration 47)"),
+                                             "workload the reference FP64 loop reaches a non-finite gradient at iteration 50)"),
         },
         "job": {
             "iters": r0.iters, "converged": r0.converged, "overlap": r0.overlap, "hpwl": r0.hpwl,

@@ -352,7 +352,12 @@ struct Foot {
   int bx0, bx1, by0, by1;
 };
 
-__device__ __forceinline__ int floor_div(int a, int s) { return a >= 0 ? a / s : -((s - 1 - a) / s); }
+// floor(a / s) for s > 0; a shift when s is a power of two (arithmetic
+// shifts floor negative values too), which is the usual bin size.
+__device__ __forceinline__ int floor_div(int a, int s) {
+  if ((s & (s - 1)) == 0) return a >> (__ffs(s) - 1);
+  return a >= 0 ? a / s : -((s - 1 - a) / s);
+}
 __device__ __forceinline__ int ceil_div(int a, int s) { return -floor_div(-a, s); }
 
 __device__ __forceinline__ Foot make_foot(float2 p, float hw, float hh, int BX, int BY, int sx, int sy) {
