@@ -1189,6 +1189,7 @@ void load_into(eplace_ctx *c, HostProblem &&hp_in, const uint64_t *ip_seed = nul
   std::thread t_pw([&] {
     pin_weights(hp, c->pw_host);
     grad_k = grad_scale_log2(hp);
+    build_hpwl_table(c->hp);  // its own members only; the others read the rest
   });
   std::thread t_ip;
   if (ip_seed)
@@ -1444,6 +1445,7 @@ struct Checkpoint {
   double disp = 0.0;
   int64_t hpwl = 0;
   double secs = 0.0;  // time of its legalisation + HPWL (host clock, or device events)
+  double began = 0.0;  // host legaliser: its start, seconds from the run's start
   eplace_status st = EPLACE_OK;
   std::atomic<bool> done{false};
 };
@@ -1961,9 +1963,11 @@ struct JobState {
         outstanding.fetch_add(1, std::memory_order_acq_rel);
         eplace_ctx *cc = c;
         std::atomic<int> *out = &outstanding;
-        pool->submit([raw, cc, out](int tid) {
+        const auto ts = t_start;
+        pool->submit([raw, cc, out, ts](int tid) {
           const HostProblem &php = cc->hp;
           const auto t0 = std::chrono::steady_clock::now();
+          raw->began = std::chrono::duration<double>(t0 - ts).count();
           HostSnap &h = *raw->hs;
           h.sx.resize(php.N);
           h.sy.resize(php.N);
@@ -2081,6 +2085,9 @@ struct JobState {
       std::fprintf(stderr, "eplace_run legalisations: %zu (%s), mean %.2f ms, max %.2f ms, threads %d\n", cps.size(),
                    gpu_legal ? "device" : "host", cps.empty() ? 0.0 : 1e3 * sum / cps.size(), 1e3 * mx,
                    pool ? pool->size() : 0);
+      std::fprintf(stderr, "eplace_run checkpoints (iteration: start + length, ms):");
+      for (auto &cp : cps) std::fprintf(stderr, " %d:%.1f+%.1f", cp->iter, cp->began * 1e3, cp->secs * 1e3);
+      std::fprintf(stderr, "\n");
     }
     res->h2d_bytes = g_h2d - h2d0;
     res->d2h_bytes = g_d2h - d2h0;
@@ -2813,6 +2820,7 @@ eplace_status eplace_hpwl_host(const eplace_netlist *nl, const eplace_chip *chip
     return st;
   }
   if (!hpwl || (hp.N && (!sx || !sy))) return EPLACE_ERR_INVALID;
+  build_hpwl_table(hp);
   *hpwl = hpwl_host(hp, sx, sy);
   return EPLACE_OK;
 }

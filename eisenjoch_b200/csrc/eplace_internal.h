@@ -38,6 +38,13 @@ struct HostProblem {
   std::vector<uint8_t> has_driver;
   bool any_macro = false;
   uint32_t max_degree = 0;
+  // The nets that count toward the HPWL (a driver and two pins or more),
+  // grouped by degree: their pins back to back in hpwl_pins, and one
+  // (degree, nets) pair per group in hpwl_runs.  Until build_hpwl_table
+  // sets hpwl_table, hpwl_host walks the plain CSR.
+  std::vector<uint32_t> hpwl_pins;
+  std::vector<std::pair<uint32_t, uint32_t>> hpwl_runs;
+  bool hpwl_table = false;
 };
 
 // Validates the C structs and copies them.  Returns EPLACE_OK or
@@ -81,10 +88,13 @@ struct Legalizer {
   std::vector<uint64_t> free_, sum_;
   std::vector<int32_t> lc_, rc_;  // per-row candidate cache of the unit-cell search
   bool simd_ = false;             // AVX2 available: the search takes four rows per step
+  bool simd512_ = false;          // AVX-512F available: eight rows per step
 };
 
 // total_hpwl (metrics/wirelength.rs:10-51) on the host.
 int64_t hpwl_host(const HostProblem &hp, const int32_t *site_x, const int32_t *site_y);
+// Fills hp.hpwl_pins / hp.hpwl_runs (counting sort by degree, O(pins)).
+void build_hpwl_table(HostProblem &hp);
 
 // Synthetic generator (no reference counterpart).
 eplace_status synth(const eplace_synth_spec &spec, eplace_synth_info *info, uint8_t *cw,

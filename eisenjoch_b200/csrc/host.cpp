@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 
 #include "eplace_internal.h"
@@ -215,7 +216,12 @@ LegalBase::LegalBase(const HostProblem &hp) : W(hp.W), H(hp.H) {
 
 Legalizer::Legalizer(const HostProblem &hp, const LegalBase &base) : hp_(hp), base_(base) {
   __builtin_cpu_init();
-  simd_ = __builtin_cpu_supports("avx2");
+  // EPLACE_LEGAL_SIMD=0/1 caps the search at the scalar / AVX2 form (all
+  // forms give the same bindings; tests compare each with the oracle).
+  const char *cap = std::getenv("EPLACE_LEGAL_SIMD");
+  const int level = cap ? std::atoi(cap) : 2;
+  simd_ = level >= 1 && __builtin_cpu_supports("avx2");
+  simd512_ = simd_ && level >= 2 && __builtin_cpu_supports("avx512f");
   free_.resize(base.free0.size());
   sum_.resize(base.sum0.size());
   lc_.resize(std::max(base.H, 0));
@@ -298,6 +304,86 @@ inline int nearest_ints(double t, int32_t n, int32_t (&out)[2]) {
   return m;
 }
 
+// The 3 x 3 block of sites around the unique nearest site (cx, cy) of the
+// target.  Every site outside the block is more than 1.5 away from the
+// target along one axis, so its cost is at least 2.25 (exact differences,
+// monotone rounding); a free site of the block that costs less than that is
+// the minimum over the grid.  Visited in tile order with a strict <, so the
+// lowest tile wins a tie, as in the reference's scan.  Leaves best / best_t
+// at the block's best free site (or unchanged when all nine are taken).
+inline void probe3(const uint64_t *fm, int32_t WR, int32_t W, int32_t H, int32_t cx, int32_t cy, double tx, double ty,
+                   double &best, int64_t &best_t, int32_t &bx, int32_t &by) {
+  double dx2[3], dy2[3];
+  for (int k = 0; k < 3; ++k) {
+    const double dx = (double)(cx - 1 + k) - tx, dy = (double)(cy - 1 + k) - ty;
+    dx2[k] = dx * dx;
+    dy2[k] = dy * dy;
+  }
+  for (int a = 0; a < 3; ++a) {
+    const int32_t y = cy - 1 + a;
+    if (y < 0 || y >= H) continue;
+    const uint64_t *row = fm + (size_t)y * WR;
+    uint32_t m = 0;
+    for (int k = 0; k < 3; ++k) {
+      const int32_t x = cx - 1 + k;
+      if (x >= 0 && x < W) m |= (uint32_t)((row[x >> 6] >> (x & 63)) & 1) << k;
+    }
+    while (m) {
+      const int k = __builtin_ctz(m);
+      m &= m - 1;
+      const double cost = dx2[k] + dy2[a];
+      if (cost < best) {
+        best = cost;
+        best_t = (int64_t)y * W + cx - 1 + k;
+        bx = cx - 1 + k;
+        by = y;
+      }
+    }
+  }
+}
+
+// Bits of columns x0 .. x0 + n - 1 of a row (n <= 57), 0 for columns off
+// the grid (the map's bits past W are 0 already).
+inline uint64_t window_bits(const uint64_t *row, int32_t x0, int n, int32_t WR) {
+  uint64_t m;
+  if (x0 >= 0) {
+    const int32_t w = x0 >> 6, sh = x0 & 63;
+    m = row[w] >> sh;
+    if (sh && w + 1 < WR) m |= row[w + 1] << (64 - sh);
+  } else {
+    m = row[0] << (-x0);
+  }
+  return m & ((1ull << n) - 1);
+}
+
+// The (2k+1)^2 block around the unique nearest site (cx, cy): in each of
+// its rows the nearest free site of the block left of or at floor(tx) and
+// right of it (the rest of the row's part in the block costs more).  A site
+// outside the block costs at least (k + 1/2)^2; the caller trusts the
+// result only below that.  Keeps the lower (cost, tile).
+inline void probe_window(const uint64_t *fm, int32_t WR, int32_t W, int32_t H, int32_t cx, int32_t cy, int32_t fx0,
+                         int k, double tx, double ty, double &best, int64_t &best_t) {
+  const int32_t x0 = cx - k, n = 2 * k + 1, off = fx0 - x0;  // off in [k - 1, k]
+  const uint64_t lmask = (2ull << off) - 1;
+  for (int32_t y = std::max(cy - k, 0); y <= std::min(cy + k, H - 1); ++y) {
+    const uint64_t m = window_bits(fm + (size_t)y * WR, x0, n, WR);
+    const double dy = (double)y - ty, dy2 = dy * dy;
+    const uint64_t ml = m & lmask, mr = m & ~lmask;
+    if (ml) {
+      const int32_t x = x0 + 63 - __builtin_clzll(ml);
+      const double dx = (double)x - tx, c = dx * dx + dy2;
+      const int64_t t = (int64_t)y * W + x;
+      if (c < best || (c == best && t < best_t)) { best = c; best_t = t; }
+    }
+    if (mr) {
+      const int32_t x = x0 + __builtin_ctzll(mr);
+      const double dx = (double)x - tx, c = dx * dx + dy2;
+      const int64_t t = (int64_t)y * W + x;
+      if (c < best || (c == best && t < best_t)) { best = c; best_t = t; }
+    }
+  }
+}
+
 // One unit cell's search over the rows (see Legalizer::run).
 struct RowSearch {
   const uint64_t *fm;
@@ -360,7 +446,7 @@ inline bool side_done(const RowSearch &s, int32_t row) {
 }
 
 // Rows outward from cy, one at a time.
-void search_rows(RowSearch &s, int32_t cy) {
+__attribute__((noinline)) void search_rows(RowSearch &s, int32_t cy) {
   scan_row(s, cy);
   bool up = true, down = true;
   for (int32_t d = 1; up || down; ++d) {
@@ -438,7 +524,7 @@ __attribute__((target("avx2"))) inline void rows4(RowSearch &s, int32_t r0) {
   }
 }
 
-__attribute__((target("avx2"))) void search_rows4(RowSearch &s, int32_t cy) {
+__attribute__((target("avx2"), noinline)) void search_rows4(RowSearch &s, int32_t cy) {
   scan_row(s, cy);
   bool up = true, down = true;
   int32_t dd = 1, du = 1;
@@ -469,6 +555,112 @@ __attribute__((target("avx2"))) void search_rows4(RowSearch &s, int32_t cy) {
     }
   }
 }
+// The same search with AVX-512, eight consecutive rows per step and no
+// branch on the candidates: each of the eight lanes keeps the best
+// (cost, tile) of the candidates it has seen, updated with the scalar
+// code's comparison (lower cost, then lower tile), and the lanes are merged
+// at the end.  Costs are formed as in the scalar code (separate multiply and
+// add).  A side stops once dy^2 exceeds the best cost found so far, which
+// only ever shrinks, so every row that could win or tie is visited.
+struct Lanes8 {
+  __m512d bc;   // best cost per lane
+  __m512i bt;   // its tile (INT64_MAX: none)
+  __m512i kw;   // k * W for lane k
+  double best;  // minimum over the lanes and the scalar rows
+};
+
+__attribute__((target("avx512f,avx2"))) inline void lane_update(Lanes8 &L, __m512d c, __m512i t, __mmask8 ok) {
+  const __mmask8 lt = _mm512_cmp_pd_mask(c, L.bc, _CMP_LT_OQ);
+  const __mmask8 eq = _mm512_cmp_pd_mask(c, L.bc, _CMP_EQ_OQ) & _mm512_cmplt_epi64_mask(t, L.bt);
+  const __mmask8 u = ok & (lt | eq);
+  L.bc = _mm512_mask_blend_pd(u, L.bc, c);
+  L.bt = _mm512_mask_blend_epi64(u, L.bt, t);
+}
+
+__attribute__((target("avx512f,avx2"))) inline void rows8(RowSearch &s, Lanes8 &L, int32_t r0) {
+  __m256i l = _mm256_loadu_si256(reinterpret_cast<const __m256i *>(s.lc + r0));
+  __m256i r = _mm256_loadu_si256(reinterpret_cast<const __m256i *>(s.rc + r0));
+  const __m256i fxv = _mm256_set1_epi32(s.fx0);
+  const __m256i stale = _mm256_or_si256(_mm256_cmpgt_epi32(l, fxv),
+                                        _mm256_cmpgt_epi32(_mm256_add_epi32(fxv, _mm256_set1_epi32(1)), r));
+  if (_mm256_movemask_epi8(stale)) {
+    // Refresh only the rows still within reach (as in rows4).
+    alignas(32) int32_t la[8], ra[8];
+    for (int32_t k = 0; k < 8; ++k) {
+      const int32_t row = r0 + k;
+      const double d = (double)row - s.ty;
+      if (d * d > L.best) {
+        la[k] = -1;
+        ra[k] = s.W;
+      } else {
+        int32_t a, b;
+        row_candidates(s, row, a, b);
+        la[k] = a;
+        ra[k] = b >= 0 ? b : s.W;
+      }
+    }
+    l = _mm256_load_si256(reinterpret_cast<const __m256i *>(la));
+    r = _mm256_load_si256(reinterpret_cast<const __m256i *>(ra));
+  }
+  const __m512d txv = _mm512_set1_pd(s.tx);
+  const __m256i rows = _mm256_add_epi32(_mm256_set1_epi32(r0), _mm256_setr_epi32(0, 1, 2, 3, 4, 5, 6, 7));
+  const __m512d dy = _mm512_sub_pd(_mm512_cvtepi32_pd(rows), _mm512_set1_pd(s.ty));
+  const __m512d dy2 = _mm512_mul_pd(dy, dy);
+  const __m512i base = _mm512_add_epi64(_mm512_set1_epi64((int64_t)r0 * s.W), L.kw);
+  const __mmask8 okl = (__mmask8)_mm256_movemask_ps(_mm256_castsi256_ps(_mm256_cmpgt_epi32(l, _mm256_set1_epi32(-1))));
+  const __m512d dxl = _mm512_sub_pd(_mm512_cvtepi32_pd(l), txv);
+  lane_update(L, _mm512_add_pd(_mm512_mul_pd(dxl, dxl), dy2), _mm512_add_epi64(base, _mm512_cvtepi32_epi64(l)), okl);
+  const __mmask8 okr =
+      (__mmask8)_mm256_movemask_ps(_mm256_castsi256_ps(_mm256_cmpgt_epi32(_mm256_set1_epi32(s.W), r)));
+  const __m512d dxr = _mm512_sub_pd(_mm512_cvtepi32_pd(r), txv);
+  lane_update(L, _mm512_add_pd(_mm512_mul_pd(dxr, dxr), dy2), _mm512_add_epi64(base, _mm512_cvtepi32_epi64(r)), okr);
+  L.best = std::min(L.best, _mm512_reduce_min_pd(L.bc));
+}
+
+__attribute__((target("avx512f,avx2"), noinline)) void search_rows8(RowSearch &s, int32_t cy) {
+  scan_row(s, cy);
+  const int64_t W = s.W;
+  Lanes8 L{_mm512_set1_pd(INFINITY), _mm512_set1_epi64(INT64_MAX),
+           _mm512_setr_epi64(0, W, 2 * W, 3 * W, 4 * W, 5 * W, 6 * W, 7 * W), s.best};
+  bool up = true, down = true;
+  int32_t dd = 1, du = 1;
+  while (up || down) {
+    if (down) {
+      const int32_t row = cy - dd;
+      const double d = (double)row - s.ty;
+      if (row < 0 || d * d > L.best) {
+        down = false;
+      } else if (row >= 7) {
+        rows8(s, L, row - 7);
+        dd += 8;
+      } else {
+        scan_row(s, row);
+        L.best = std::min(L.best, s.best);
+        dd += 1;
+      }
+    }
+    if (up) {
+      const int32_t row = cy + du;
+      const double d = (double)row - s.ty;
+      if (row >= s.H || d * d > L.best) {
+        up = false;
+      } else if (row + 7 < s.H) {
+        rows8(s, L, row);
+        du += 8;
+      } else {
+        scan_row(s, row);
+        L.best = std::min(L.best, s.best);
+        du += 1;
+      }
+    }
+  }
+  alignas(64) double cs[8];
+  alignas(64) int64_t ts[8];
+  _mm512_store_pd(cs, L.bc);
+  _mm512_store_si512(reinterpret_cast<__m512i *>(ts), L.bt);
+  for (int k = 0; k < 8; ++k)
+    if (ts[k] != INT64_MAX) consider(s, cs[k], ts[k]);
+}
 }  // namespace
 
 eplace_status Legalizer::run(const float *x, const float *y, size_t stride, int32_t *site_x, int32_t *site_y,
@@ -486,20 +678,52 @@ eplace_status Legalizer::run(const float *x, const float *y, size_t stride, int3
     const int w = hp_.cw[i], h = hp_.ch[i];
     double best = INFINITY;
     int64_t best_t = -1;
+    int32_t bx = -1, by = -1;  // best_t's site when known without a division
     if (w == 1 && h == 1) {
-      // fast path: a free site of minimum cost over the whole grid
-      int32_t xs[2], ys[2];
-      const int nx = (tx >= 0.0 && tx <= (double)(W - 1)) ? nearest_ints(tx, W, xs) : 0;
-      const int ny = (ty >= 0.0 && ty <= (double)(H - 1)) ? nearest_ints(ty, H, ys) : 0;
-      for (int a = 0; a < ny && best_t < 0; ++a)
-        for (int b = 0; b < nx; ++b)
-          if (is_free(fm, WR, xs[b], ys[a])) {
-            const double dx = (double)xs[b] - tx, dy = (double)ys[a] - ty;
-            best = dx * dx + dy * dy;
-            best_t = (int64_t)ys[a] * W + xs[b];
-            break;
+      // fast path: a free site of minimum cost over the whole grid.  With
+      // both fractions away from 1/2 the nearest site is unique; otherwise
+      // the tied nearest sites are tried in tile order.
+      const double flx = floor_exact(tx), fly = floor_exact(ty);
+      const double frx = tx - flx, fry = ty - fly;
+      const bool inside = tx >= 0.0 && tx <= (double)(W - 1) && ty >= 0.0 && ty <= (double)(H - 1);
+      bool resolved = false;
+      // The block probes: 3 x 3, then the (2 kWin + 1)^2 block.
+      constexpr int kWin = 4;
+      if (inside && frx != 0.5 && fry != 0.5) {
+        const int32_t nx = (int32_t)flx + (frx > 0.5 ? 1 : 0), ny = (int32_t)fly + (fry > 0.5 ? 1 : 0);
+        if (is_free(fm, WR, nx, ny)) {
+          const double dx = (double)nx - tx, dy = (double)ny - ty;
+          best = dx * dx + dy * dy;
+          best_t = (int64_t)ny * W + nx;
+          bx = nx;
+          by = ny;
+          resolved = true;
+        } else {
+          probe3(fm, WR, W, H, nx, ny, tx, ty, best, best_t, bx, by);
+          resolved = best < 2.25;
+          if (!resolved) {
+            probe_window(fm, WR, W, H, nx, ny, (int32_t)flx, kWin, tx, ty, best, best_t);
+            bx = -1;
+            resolved = best < (kWin + 0.5) * (kWin + 0.5);  // exact product
           }
-      if (best_t < 0) {
+        }
+      } else {
+        int32_t xs[2], ys[2];
+        const int nx = (tx >= 0.0 && tx <= (double)(W - 1)) ? nearest_ints(tx, W, xs) : 0;
+        const int ny = (ty >= 0.0 && ty <= (double)(H - 1)) ? nearest_ints(ty, H, ys) : 0;
+        for (int a = 0; a < ny && best_t < 0; ++a)
+          for (int b = 0; b < nx; ++b)
+            if (is_free(fm, WR, xs[b], ys[a])) {
+              const double dx = (double)xs[b] - tx, dy = (double)ys[a] - ty;
+              best = dx * dx + dy * dy;
+              best_t = (int64_t)ys[a] * W + xs[b];
+              bx = xs[b];
+              by = ys[a];
+              break;
+            }
+        resolved = best_t >= 0;
+      }
+      if (!resolved) {
         int32_t cy = (int32_t)floor_exact(ty + 0.5);
         cy = std::min(std::max(cy, 0), H - 1);
         const int32_t fx0 = (int32_t)floor_exact(tx);
@@ -511,10 +735,12 @@ eplace_status Legalizer::run(const float *x, const float *y, size_t stride, int3
         // same region) reads them instead of searching the bitmap.  A row's
         // entry dies when one of its two sites is taken.
         RowSearch rs{fm, sm, lc, rc, W, H, WR, tx, ty, fx0, fx0 >= 0 && fx0 <= W - 1, best, best_t};
-        if (simd_ && rs.cacheable) search_rows4(rs, cy);
+        if (simd512_ && rs.cacheable) search_rows8(rs, cy);
+        else if (simd_ && rs.cacheable) search_rows4(rs, cy);
         else search_rows(rs, cy);
         best = rs.best;
         best_t = rs.best_t;
+        bx = -1;
       }
     } else {
       // Macro: anchor rows outward from the target anchor row.  In anchor
@@ -605,7 +831,10 @@ eplace_status Legalizer::run(const float *x, const float *y, size_t stride, int3
       }
     }
     if (best_t < 0) return EPLACE_ERR_NO_BELS;
-    const int32_t bx = (int32_t)(best_t % W), by = (int32_t)(best_t / W);
+    if (bx < 0) {
+      bx = (int32_t)(best_t % W);
+      by = (int32_t)(best_t / W);
+    }
     for (int dy = 0; dy < h; ++dy)
       for (int dx = 0; dx < w; ++dx) {
         const int32_t xx = bx + dx;
@@ -625,28 +854,102 @@ eplace_status Legalizer::run(const float *x, const float *y, size_t stride, int3
 // total_hpwl (metrics/wirelength.rs:10-51): integer bbox of driver + users;
 // nets without a driver or without users contribute 0.  A macro's pins sit
 // at anchor + (w-1)/2 (integer), which is the BEL itself for a unit cell.
+// Pin locations packed per cell, x | y << 16 (the grid fits 16 bits): one
+// 4-byte gather per pin from a table that stays in the core's cache.
+static const uint32_t *packed_locations(const HostProblem &hp, const int32_t *sx, const int32_t *sy) {
+  thread_local std::vector<uint32_t> loc;
+  loc.resize((size_t)hp.N + hp.F);
+  for (uint32_t c = 0; c < hp.N; ++c)
+    loc[c] = (uint32_t)(sx[c] + (hp.cw[c] - 1) / 2) | ((uint32_t)(sy[c] + (hp.ch[c] - 1) / 2) << 16);
+  for (uint32_t f = 0; f < hp.F; ++f) loc[hp.N + f] = (uint32_t)hp.fx[f] | ((uint32_t)hp.fy[f] << 16);
+  return loc.data();
+}
+
+void build_hpwl_table(HostProblem &hp) {
+  std::vector<uint32_t> count((size_t)hp.max_degree + 1, 0);
+  size_t pins = 0;
+  for (uint32_t n = 0; n < hp.NN; ++n) {
+    const uint32_t d = hp.net_off[n + 1] - hp.net_off[n];
+    if (hp.has_driver[n] && d >= 2) {
+      ++count[d];
+      pins += d;
+    }
+  }
+  std::vector<size_t> at(count.size(), 0);
+  hp.hpwl_runs.clear();
+  for (size_t d = 2, k = 0; d < count.size(); ++d) {
+    at[d] = k;
+    k += count[d] * d;
+    if (count[d]) hp.hpwl_runs.emplace_back((uint32_t)d, count[d]);
+  }
+  hp.hpwl_pins.resize(pins);
+  for (uint32_t n = 0; n < hp.NN; ++n) {
+    const uint32_t b = hp.net_off[n], d = hp.net_off[n + 1] - b;
+    if (!hp.has_driver[n] || d < 2) continue;
+    std::copy(hp.pin_cell.begin() + b, hp.pin_cell.begin() + b + d, hp.hpwl_pins.begin() + at[d]);
+    at[d] += d;
+  }
+  hp.hpwl_table = true;
+}
+
 int64_t hpwl_host(const HostProblem &hp, const int32_t *sx, const int32_t *sy) {
   int64_t total = 0;
-  for (uint32_t n = 0; n < hp.NN; ++n) {
-    uint32_t b = hp.net_off[n], e = hp.net_off[n + 1];
-    if (!hp.has_driver[n] || e - b < 2) continue;
-    int32_t x0 = INT32_MAX, x1 = INT32_MIN, y0 = INT32_MAX, y1 = INT32_MIN;
-    for (uint32_t q = b; q < e; ++q) {
-      uint32_t c = hp.pin_cell[q];
-      int32_t lx, ly;
-      if (c < hp.N) {
-        lx = sx[c] + (hp.cw[c] - 1) / 2;
-        ly = sy[c] + (hp.ch[c] - 1) / 2;
-      } else {
-        lx = hp.fx[c - hp.N];
-        ly = hp.fy[c - hp.N];
+  if (hp.W > 65536 || hp.H > 65536) {
+    // Wide grids: the footprint and binding arrays directly.
+    for (uint32_t n = 0; n < hp.NN; ++n) {
+      uint32_t b = hp.net_off[n], e = hp.net_off[n + 1];
+      if (!hp.has_driver[n] || e - b < 2) continue;
+      int32_t x0 = INT32_MAX, x1 = INT32_MIN, y0 = INT32_MAX, y1 = INT32_MIN;
+      for (uint32_t q = b; q < e; ++q) {
+        uint32_t c = hp.pin_cell[q];
+        int32_t lx, ly;
+        if (c < hp.N) {
+          lx = sx[c] + (hp.cw[c] - 1) / 2;
+          ly = sy[c] + (hp.ch[c] - 1) / 2;
+        } else {
+          lx = hp.fx[c - hp.N];
+          ly = hp.fy[c - hp.N];
+        }
+        x0 = std::min(x0, lx);
+        x1 = std::max(x1, lx);
+        y0 = std::min(y0, ly);
+        y1 = std::max(y1, ly);
       }
-      x0 = std::min(x0, lx);
-      x1 = std::max(x1, lx);
-      y0 = std::min(y0, ly);
-      y1 = std::max(y1, ly);
+      total += (int64_t)(x1 - x0) + (int64_t)(y1 - y0);
     }
-    total += (int64_t)(x1 - x0) + (int64_t)(y1 - y0);
+    return total;
+  }
+  const uint32_t *L = packed_locations(hp, sx, sy);
+  // bounding box of the d pins at p (d >= 2)
+  auto box = [L](const uint32_t *p, uint32_t d) -> int64_t {
+    if (d == 2) {
+      const uint32_t v0 = L[p[0]], v1 = L[p[1]];
+      const int32_t dx = (int32_t)(v0 & 0xffffu) - (int32_t)(v1 & 0xffffu);
+      const int32_t dy = (int32_t)(v0 >> 16) - (int32_t)(v1 >> 16);
+      return (int64_t)std::abs(dx) + std::abs(dy);
+    }
+    uint32_t x0 = 0xffffu, x1 = 0, y0 = 0xffffu, y1 = 0;
+    for (uint32_t q = 0; q < d; ++q) {
+      const uint32_t v = L[p[q]];
+      x0 = std::min(x0, v & 0xffffu);
+      x1 = std::max(x1, v & 0xffffu);
+      y0 = std::min(y0, v >> 16);
+      y1 = std::max(y1, v >> 16);
+    }
+    return (int64_t)(x1 - x0) + (int64_t)(y1 - y0);
+  };
+  if (hp.hpwl_table) {
+    // Nets grouped by degree: the inner trip count repeats from net to net.
+    const uint32_t *p = hp.hpwl_pins.data();
+    for (const auto &run : hp.hpwl_runs) {
+      const uint32_t d = run.first;
+      for (uint32_t k = 0; k < run.second; ++k, p += d) total += box(p, d);
+    }
+    return total;
+  }
+  for (uint32_t n = 0; n < hp.NN; ++n) {
+    const uint32_t b = hp.net_off[n], d = hp.net_off[n + 1] - b;
+    if (hp.has_driver[n] && d >= 2) total += box(hp.pin_cell.data() + b, d);
   }
   return total;
 }

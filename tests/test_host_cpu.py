@@ -233,12 +233,15 @@ def test_workload_table_is_plain_data():
         assert E.WORKLOADS[name]["cfg"] == w["cfg"]
 
 
-def test_host_legalizer_dense_pile_equals_oracle():
+@pytest.mark.parametrize("simd", ["0", "1", "2"])
+def test_host_legalizer_dense_pile_equals_oracle(simd, monkeypatch):
     """A central pile (cells up to ~60 sites from their nearest free site,
-    long row searches: the four-rows-per-step path on CPUs with AVX2) with
-    5 % macros: the product's host legaliser equals the oracle's ring search
-    (the reference's choice and tie-break) site for site, and the FP64
-    displacement bit for bit."""
+    long row searches) with 5 % macros: the product's host legaliser equals
+    the oracle's ring search (the reference's choice and tie-break) site for
+    site, and the FP64 displacement bit for bit, in each of its search forms
+    (EPLACE_LEGAL_SIMD: 0 scalar, 1 four rows per step with AVX2, 2 eight
+    rows per step with AVX-512 where the CPU has them)."""
+    monkeypatch.setenv("EPLACE_LEGAL_SIMD", simd)
     nl, chip = E.synth_netlist(E.SynthSpec(seed=12, num_cells=20000, num_nets=22000, num_pads=300, width=256,
                                            height=256, cluster_size=64, macro_fraction=0.05))
     rng = np.random.default_rng(4)
@@ -252,3 +255,24 @@ def test_host_legalizer_dense_pile_equals_oracle():
     assert disp == odisp
     far = (sx - x) ** 2 + (sy - y) ** 2 > 400
     assert far.sum() > 1000  # the pile is real: many long searches
+
+
+@pytest.mark.parametrize("simd", ["0", "1", "2"])
+def test_host_legalizer_ties_equal_oracle(simd, monkeypatch):
+    """Targets on the integer and half-integer lattice (ties between sites
+    of equal cost everywhere: the nearest-site fast path, the 3 x 3 block
+    around it and the row search all break them by lowest tile) in a pile
+    with an off-centre second pile near the chip edge, unit cells only."""
+    monkeypatch.setenv("EPLACE_LEGAL_SIMD", simd)
+    nl, chip = E.synth_netlist(E.SynthSpec(seed=13, num_cells=12000, num_nets=12000, num_pads=100, width=160,
+                                           height=160, cluster_size=32))
+    rng = np.random.default_rng(5)
+    n = nl.num_cells
+    centre = np.where(rng.random(n) < 0.7, 80.0, 8.0)
+    x = np.clip(np.round(rng.normal(centre, 20, n) * 2) / 2, 0, 159).astype(np.float32)
+    y = np.clip(np.round(rng.normal(centre, 20, n) * 2) / 2, 0, 159).astype(np.float32)
+    sx, sy, disp = E.legalize_host(nl, chip, x, y)
+    st, ox, oy, odisp = O.Oracle(nl, chip).legalize(x, y, 1)
+    assert st == 0
+    assert np.array_equal(sx, ox) and np.array_equal(sy, oy)
+    assert disp == odisp
