@@ -701,8 +701,13 @@ eplace_status Legalizer::run(const float *x, const float *y, size_t stride, int3
         } else {
           probe3(fm, WR, W, H, nx, ny, tx, ty, best, best_t, bx, by);
           resolved = best < 2.25;
-          if (!resolved) {
-            probe_window(fm, WR, W, H, nx, ny, (int32_t)flx, kWin, tx, ty, best, best_t);
+          // Skip the larger block when the cell's own row is known to have
+          // no free site within it (a cell deep in a pile): the row search
+          // follows either way.
+          const int32_t fx = (int32_t)flx;
+          const bool deep = lc[ny] <= fx && fx < rc[ny] && fx - lc[ny] > kWin && rc[ny] - fx > kWin;
+          if (!resolved && !deep) {
+            probe_window(fm, WR, W, H, nx, ny, fx, kWin, tx, ty, best, best_t);
             bx = -1;
             resolved = best < (kWin + 0.5) * (kWin + 0.5);  // exact product
           }
