@@ -409,51 +409,74 @@ eplace_status cuda_fail(eplace_ctx *c, const CudaError &e) {
   return EPLACE_ERR_CUDA;
 }
 
-// The WA kernel works on a copy of the CSR with the nets ordered by pin
-// count (stable), so nets of one degree class are contiguous.  Net order
-// does not change the result: the gradient accumulates in fixed point.
-void degree_sorted_csr(const HostProblem &hp, std::vector<uint32_t> &off, std::vector<uint32_t> &pins) {
+// The WA kernel sees the nets ordered by pin count (stable), so nets of one
+// degree class are contiguous: order[i] is the i-th net of that order and
+// off[] its offsets (a CSR over the sorted nets).  Net order does not
+// change the result: the gradient accumulates in fixed point.
+void degree_order(const HostProblem &hp, std::vector<uint32_t> &order, std::vector<uint32_t> &off) {
   // Counting sort by degree (stable: nets of one degree keep their order).
   std::vector<uint32_t> start((size_t)hp.max_degree + 2, 0);
   for (uint32_t n = 0; n < hp.NN; ++n) ++start[hp.net_off[n + 1] - hp.net_off[n] + 1];
   for (size_t d = 1; d < start.size(); ++d) start[d] += start[d - 1];
-  std::vector<uint32_t> order(hp.NN);
+  order.resize(hp.NN);
   for (uint32_t n = 0; n < hp.NN; ++n) order[start[hp.net_off[n + 1] - hp.net_off[n]]++] = n;
-  off.assign(hp.NN + 1, 0);
-  pins.resize(hp.P);
-  uint32_t k = 0;
-  for (uint32_t i = 0; i < hp.NN; ++i) {
+  off.resize((size_t)hp.NN + 1);
+  off[0] = 0;
+  for (uint32_t i = 0; i < hp.NN; ++i) off[i + 1] = off[i] + (hp.net_off[order[i] + 1] - hp.net_off[order[i]]);
+}
+
+// The pins of sorted nets [n0, n1), in sorted-CSR order starting at off[n0]
+// (the device reads the sorted CSR only for the last class: nets of more
+// than 224 pins).
+void sorted_pins(const HostProblem &hp, const std::vector<uint32_t> &order, const std::vector<uint32_t> &off,
+                 uint32_t n0, uint32_t n1, std::vector<uint32_t> &pins) {
+  pins.resize(off[n1] - off[n0]);
+  for (uint32_t i = n0; i < n1; ++i) {
     const uint32_t n = order[i];
-    for (uint32_t q = hp.net_off[n]; q < hp.net_off[n + 1]; ++q) pins[k++] = hp.pin_cell[q];
-    off[i + 1] = k;
+    std::copy(hp.pin_cell.begin() + hp.net_off[n], hp.pin_cell.begin() + hp.net_off[n + 1],
+              pins.begin() + (off[i] - off[n0]));
   }
 }
 
 // The padded pin table of the degree classes: net idx of class j takes
 // G * S slots (G = kWaGroup[j], S = kWaSlots[j]) from the class base (a
 // multiple of 4 slots, for 16-byte loads); pin q of the net goes to lane
-// q % G, slot q / G of that lane.  Sets each class's slot_base.
-std::vector<uint32_t> build_wa_slots(const std::vector<uint32_t> &off, const std::vector<uint32_t> &pins,
+// q % G, slot q / G of that lane.  Sets each class's slot_base.  Three
+// threads fill disjoint runs of classes of about equal size.
+std::vector<uint32_t> build_wa_slots(const HostProblem &hp, const std::vector<uint32_t> &order,
                                      WaClass (&cls)[kWaClasses]) {
   size_t total = 0;
+  size_t upto[kWaClasses + 1] = {0};
   for (int j = 0; j < kWaClasses; ++j) {
     total = (total + 3) & ~(size_t)3;
     cls[j].slot_base = (long long)total;
     total += (size_t)cls[j].nets * kWaGroup[j] * kWaSlots[j];
+    upto[j + 1] = total;
   }
   std::vector<uint32_t> t(std::max<size_t>(total, 4), 0xffffffffu);
-  for (int j = 0; j < kWaClasses; ++j) {
-    const int G = kWaGroup[j], S = kWaSlots[j];
-    if (S == 0) continue;
-    for (int idx = 0; idx < cls[j].nets; ++idx) {
-      const uint32_t n = (uint32_t)(cls[j].first_net + idx);
-      const size_t base = (size_t)cls[j].slot_base + (size_t)idx * G * S;
-      for (uint32_t q = off[n]; q < off[n + 1]; ++q) {
-        const uint32_t r = q - off[n];
-        t[base + (size_t)(r % G) * S + r / G] = pins[q];
+  auto fill = [&](int j0, int j1) {
+    for (int j = j0; j < j1; ++j) {
+      const int G = kWaGroup[j], S = kWaSlots[j];
+      if (S == 0) continue;
+      const int gs = __builtin_ctz(G);  // G is a power of two
+      for (int idx = 0; idx < cls[j].nets; ++idx) {
+        const uint32_t n = order[(uint32_t)(cls[j].first_net + idx)];
+        const size_t base = (size_t)cls[j].slot_base + (size_t)idx * G * S;
+        const uint32_t b = hp.net_off[n], d = hp.net_off[n + 1] - b;
+        for (uint32_t r = 0; r < d; ++r) t[base + (size_t)(r & (G - 1)) * S + (r >> gs)] = hp.pin_cell[b + r];
       }
     }
+  };
+  int cut[4] = {0, 0, 0, kWaClasses};
+  for (int k = 1; k < 3; ++k) {
+    cut[k] = cut[k - 1];
+    while (cut[k] < kWaClasses && upto[cut[k]] * 3 < total * k) ++cut[k];
   }
+  std::thread t1([&] { fill(cut[1], cut[2]); });
+  std::thread t2([&] { fill(cut[2], cut[3]); });
+  fill(cut[0], cut[1]);
+  t1.join();
+  t2.join();
   return t;
 }
 
@@ -1176,18 +1199,19 @@ void load_into(eplace_ctx *c, HostProblem &&hp_in, const uint64_t *ip_seed = nul
   ++c->buf_epoch;
   // Host-side derived arrays are built on two helper threads while this
   // thread uploads the netlist; all CUDA calls stay on this thread.
-  std::vector<uint32_t> soff, spins, slots;
+  std::vector<uint32_t> sorder, soff, spins, slots;
   WaClass cls[kWaClasses];
   int wa_warps = 0;
   std::thread t_wa([&] {
-    degree_sorted_csr(hp, soff, spins);
+    degree_order(hp, sorder, soff);
     wa_warps = build_wa_classes(soff, cls);
-    slots = build_wa_slots(soff, spins, cls);
+    sorted_pins(hp, sorder, soff, (uint32_t)cls[kWaClasses - 1].first_net, hp.NN, spins);
+    slots = build_wa_slots(hp, sorder, cls);
   });
   int grad_k = 24;
   c->pre_ip = false;
-  std::thread t_pw([&] {
-    pin_weights(hp, c->pw_host);
+  std::thread t_pw([&] { pin_weights(hp, c->pw_host); });
+  std::thread t_hp([&] {
     grad_k = grad_scale_log2(hp);
     build_hpwl_table(c->hp);  // its own members only; the others read the rest
   });
@@ -1198,13 +1222,12 @@ void load_into(eplace_ctx *c, HostProblem &&hp_in, const uint64_t *ip_seed = nul
       c->pre_seed = *ip_seed;
     });
   struct Joiner {  // joins the helpers on every exit, an upload error included
-    std::thread &a, &b, &d;
+    std::thread &a, &b, &d, &e;
     ~Joiner() {
-      if (a.joinable()) a.join();
-      if (b.joinable()) b.join();
-      if (d.joinable()) d.join();
+      for (std::thread *t : {&a, &b, &d, &e})
+        if (t->joinable()) t->join();
     }
-  } joiner{t_wa, t_pw, t_ip};
+  } joiner{t_wa, t_pw, t_ip, t_hp};
   c->net_off.ensure(hp.net_off.size());
   c->net_off.upload(hp.net_off.data(), hp.net_off.size(), s);
   c->pin_cell.ensure(std::max<size_t>(hp.P, 1));
@@ -1219,8 +1242,14 @@ void load_into(eplace_ctx *c, HostProblem &&hp_in, const uint64_t *ip_seed = nul
     // than 224 pins); the others read the padded table.
     c->wa_off.ensure(soff.size());
     c->wa_off.upload(soff.data(), soff.size(), s);
-    c->wa_pins.ensure(std::max<size_t>(spins.size(), 1));
-    if (c->wa_cls[kWaClasses - 1].nets > 0) c->wa_pins.upload(spins.data(), spins.size(), s);
+    // Only the last class's part of the sorted pin list is uploaded, at its
+    // sorted-CSR place; no other class reads it.
+    c->wa_pins.ensure(std::max<size_t>(hp.P, 1));
+    if (c->wa_cls[kWaClasses - 1].nets > 0 && !spins.empty()) {
+      const size_t at = soff[c->wa_cls[kWaClasses - 1].first_net];
+      CK(cudaMemcpyAsync(c->wa_pins.p + at, spins.data(), sizeof(uint32_t) * spins.size(), cudaMemcpyHostToDevice, s));
+      g_h2d += sizeof(uint32_t) * spins.size();
+    }
     c->wa_slots.ensure(slots.size());
     c->wa_slots.upload(slots.data(), slots.size(), s);
   }
@@ -1264,7 +1293,6 @@ void load_into(eplace_ctx *c, HostProblem &&hp_in, const uint64_t *ip_seed = nul
   for (auto *b : {&c->x, &c->xp, &c->g, &c->gprev, &c->tmp_wl, &c->tmp_den}) b->ensure(N1);
   c->acc.ensure(N1);
   c->acc.zero(s);
-  c->grad_k = grad_k;
   const size_t nb = (size_t)hp.BX * hp.BY;
   c->dens.ensure(nb);
   c->dens.zero(s);
@@ -1289,6 +1317,8 @@ void load_into(eplace_ctx *c, HostProblem &&hp_in, const uint64_t *ip_seed = nul
   for (uint32_t f = 0; f < hp.F; ++f) floc[f] = make_int2(hp.fx[f], hp.fy[f]);
   if (hp.F) CK(cudaMemcpyAsync(c->loc.p + hp.N, floc.data(), sizeof(int2) * hp.F, cudaMemcpyHostToDevice, s));
   g_h2d += sizeof(int2) * hp.F;
+  t_hp.join();
+  c->grad_k = grad_k;
   if (t_ip.joinable()) {
     t_ip.join();
     c->pre_ip = true;

@@ -38,13 +38,20 @@ eplace_status load_problem(const eplace_netlist *nl, const eplace_chip *chip, Ho
   if (hp.NN && nl->net_offsets[0] != 0) { msg = "net_offsets[0] must be 0"; return EPLACE_ERR_INVALID; }
   hp.net_off.assign(nl->net_offsets, nl->net_offsets + (hp.NN ? hp.NN + 1 : 0));
   if (hp.NN == 0) hp.net_off.assign(1, 0);
+  // Branch-free scans (they vectorise): monotone offsets, largest degree,
+  // largest pin cell.
+  uint32_t drop = 0, maxdeg = 0;
   for (uint32_t n = 0; n < hp.NN; ++n) {
-    if (hp.net_off[n + 1] < hp.net_off[n]) { msg = "net_offsets not monotone"; return EPLACE_ERR_INVALID; }
-    hp.max_degree = std::max(hp.max_degree, hp.net_off[n + 1] - hp.net_off[n]);
+    const uint32_t a = hp.net_off[n], b = hp.net_off[n + 1];
+    drop |= (uint32_t)(b < a);
+    maxdeg = std::max(maxdeg, b - a);
   }
+  if (drop) { msg = "net_offsets not monotone"; return EPLACE_ERR_INVALID; }
+  hp.max_degree = maxdeg;
   hp.pin_cell.assign(nl->pin_cell, nl->pin_cell + hp.P);
-  for (uint32_t p = 0; p < hp.P; ++p)
-    if (hp.pin_cell[p] >= hp.N + hp.F) { msg = "pin_cell out of range"; return EPLACE_ERR_INVALID; }
+  uint32_t maxcell = 0;
+  for (uint32_t p = 0; p < hp.P; ++p) maxcell = std::max(maxcell, hp.pin_cell[p]);
+  if (hp.P && maxcell >= hp.N + hp.F) { msg = "pin_cell out of range"; return EPLACE_ERR_INVALID; }
   hp.cw.assign(hp.N, 1);
   hp.ch.assign(hp.N, 1);
   if (nl->cell_w) std::copy(nl->cell_w, nl->cell_w + hp.N, hp.cw.begin());
