@@ -26,6 +26,7 @@ from .placer import (  # noqa: F401
     batched_specs,
     footprint,
     hpwl_host,
+    pin_weights,
     initial_placement_host,
     legalize_host,
     lock_others,

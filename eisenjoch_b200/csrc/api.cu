@@ -2855,6 +2855,21 @@ eplace_status eplace_hpwl_host(const eplace_netlist *nl, const eplace_chip *chip
   return EPLACE_OK;
 }
 
+eplace_status eplace_pin_weights(const eplace_netlist *nl, const eplace_chip *chip, double *weights) {
+  HostProblem hp;
+  std::string msg;
+  eplace_status st = load_problem(nl, chip, hp, msg);
+  if (st != EPLACE_OK) {
+    set_err(nullptr, msg);
+    return st;
+  }
+  if (hp.N && !weights) return EPLACE_ERR_INVALID;
+  std::vector<double> w;
+  pin_weights(hp, w);
+  std::copy(w.begin(), w.end(), weights);
+  return EPLACE_OK;
+}
+
 eplace_status eplace_initial_placement_host(const eplace_netlist *nl, const eplace_chip *chip, uint64_t seed,
                                             int32_t *sx, int32_t *sy) {
   HostProblem hp;

@@ -600,6 +600,16 @@ def hpwl_host(netlist: Netlist, chip: Chip, site_x, site_y):
     return int(v.value)
 
 
+def pin_weights(netlist: Netlist, chip: Chip):
+    """compute_pin_weights (placer/common.rs:381-407) without a context: the
+    per-cell weights the optimal-transport placer also takes
+    (opt_trans_place/mod.rs:110)."""
+    w = np.zeros(netlist.num_cells, np.float64)
+    nl_c, chip_c = netlist.to_c(), chip.to_c()
+    check(_abi.lib().eplace_pin_weights(ctypes.byref(nl_c), ctypes.byref(chip_c), _abi.ptr(w, ctypes.c_double)))
+    return w
+
+
 def initial_placement_host(netlist: Netlist, chip: Chip, seed: int):
     """initial_placement (placer/common.rs:27-117) without a context."""
     n = netlist.num_cells

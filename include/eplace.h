@@ -302,6 +302,13 @@ eplace_status eplace_hpwl_host(const eplace_netlist *nl, const eplace_chip *chip
  * Fisher-Yates over the free logic BELs), host only. */
 eplace_status eplace_initial_placement_host(const eplace_netlist *nl, const eplace_chip *chip,
                                             uint64_t seed, int32_t *site_x, int32_t *site_y);
+/* compute_pin_weights (placer/common.rs:381-407) without a context: for each
+ * movable cell the sum of 1 / degree (f64, nets in order) over its nets of
+ * two pins or more; pads take no weight.  The optimal-transport placer
+ * computes the same weights for its preconditioner
+ * (opt_trans_place/mod.rs:110), so a port of that placer takes them from
+ * here.  weights: [num_cells].  Host only. */
+eplace_status eplace_pin_weights(const eplace_netlist *nl, const eplace_chip *chip, double *weights);
 
 /* Density map + overlap without any allocation.  No counterpart in the
  * reference: it is the density stage (eplace_stage_density) for callers

@@ -276,3 +276,24 @@ def test_host_legalizer_ties_equal_oracle(simd, monkeypatch):
     assert st == 0
     assert np.array_equal(sx, ox) and np.array_equal(sy, oy)
     assert disp == odisp
+
+
+def test_pin_weights_equal_oracle():
+    """compute_pin_weights (placer/common.rs:381-407), the weights the
+    optimal-transport placer shares (opt_trans_place/mod.rs:110): per cell
+    the sum of 1/degree over its nets of two pins or more, pads excluded,
+    a net without a driver counted by its users; bit for bit against the
+    oracle, plus a hand-checked case."""
+    nl, chip = E.synth_netlist(E.SynthSpec(seed=21, num_cells=3000, num_nets=3300, num_pads=120, width=64,
+                                           height=64, cluster_size=32))
+    drv = np.ones(nl.num_nets, np.uint8)
+    drv[::7] = 0
+    nl.net_has_driver = drv
+    w = E.pin_weights(nl, chip)
+    assert np.array_equal(w, O.Oracle(nl, chip).pin_weights())
+    # three cells, one pad (cell 3): nets {0,1}, {0,1,2}, {2,3}, {1}
+    small = E.Netlist(num_cells=3, net_offsets=np.array([0, 2, 5, 7, 8], np.uint32),
+                      pin_cell=np.array([0, 1, 0, 1, 2, 2, 3, 1], np.uint32),
+                      fixed_x=np.array([0], np.int32), fixed_y=np.array([0], np.int32))
+    w = E.pin_weights(small, E.Chip(4, 4))
+    assert np.array_equal(w, np.array([1 / 2 + 1 / 3, 1 / 2 + 1 / 3, 1 / 3 + 1 / 2]))
