@@ -220,6 +220,7 @@ PROTOTYPES = {
     "eplace_hpwl_host": (ctypes.c_int, [P(Netlist), P(Chip), c_i32p, c_i32p, c_i64p]),
     "eplace_initial_placement_host": (ctypes.c_int, [P(Netlist), P(Chip), ctypes.c_uint64, c_i32p, c_i32p]),
     "eplace_pin_weights": (ctypes.c_int, [P(Netlist), P(Chip), ctypes.POINTER(ctypes.c_double)]),
+    "eplace_stage_initial_placement": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, c_i32p, c_i32p, c_i32p]),
     "eplace_density_noalloc": (
         ctypes.c_int,
         [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,

@@ -32,6 +32,7 @@
 
 #include "dct_tc.cuh"
 #include "eplace_internal.h"
+#include "init_place.cuh"
 #include "job.h"
 #include "kernels.cuh"
 #include "legal_par.cuh"
@@ -360,14 +361,13 @@ struct eplace_ctx {
   // of any result): grid caps of the WA and scatter kernels in blocks per
   // SM, and the SIMT GEMM tile of each of the four transform GEMMs.
   int wa_blocks_per_sm = 16, sc_blocks_per_sm = 16;
-  // Initial placement computed during a load for the seed the caller will
-  // run with (one-shot eplace_place); the next run with that seed takes it
-  // and clears it, every other run computes its own.
-  bool pre_ip = false;
-  uint64_t pre_seed = 0;
-  std::vector<int32_t> pre_isx, pre_isy;
-  eplace_status pre_st = EPLACE_OK;
-  std::string pre_msg;
+  // Device initial placement (init_place.cu): scratch of the shuffle, the
+  // taken sites, the handed-out BELs, and the jump maps (uploaded once).
+  DBuf<uint32_t> ip_j, ip_cnt, ip_start, ip_entries, ip_block, ip_occ;
+  DBuf<uint64_t> ip_jump;
+  DBuf<int2> ip_site;
+  std::vector<uint32_t> ip_occ_host;  // sorted taken sites of the pending device placement
+  uint64_t ip_n = 0;                  // free logic BELs of the pending device placement
   int gemm_tile[4] = {0, 0, 0, 0};
   WaClass wa_cls[kWaClasses] = {};  // degree classes of the sorted CSR
   int wa_warps = 0;
@@ -1182,7 +1182,7 @@ void launch_gpu_legal(eplace_ctx *c, LegalSlot &L) {
 // (capacity reuse: no frees, which would synchronise the device); the DCT
 // matrices and the tensor-core operands are rebuilt only when the bin grid
 // changes; every captured graph is invalidated.
-void load_into(eplace_ctx *c, HostProblem &&hp_in, const uint64_t *ip_seed = nullptr) {
+void load_into(eplace_ctx *c, HostProblem &&hp_in) {
   AllocOn on_stream(c->stream);
   const bool same_bins = c->mat_bx == hp_in.BX && c->mat_by == hp_in.BY;
   c->hp = std::move(hp_in);
@@ -1209,25 +1209,18 @@ void load_into(eplace_ctx *c, HostProblem &&hp_in, const uint64_t *ip_seed = nul
     slots = build_wa_slots(hp, sorder, cls);
   });
   int grad_k = 24;
-  c->pre_ip = false;
   std::thread t_pw([&] { pin_weights(hp, c->pw_host); });
   std::thread t_hp([&] {
     grad_k = grad_scale_log2(hp);
     build_hpwl_table(c->hp);  // its own members only; the others read the rest
   });
-  std::thread t_ip;
-  if (ip_seed)
-    t_ip = std::thread([&] {
-      c->pre_st = initial_placement(hp, *ip_seed, c->pre_isx, c->pre_isy, c->pre_msg);
-      c->pre_seed = *ip_seed;
-    });
   struct Joiner {  // joins the helpers on every exit, an upload error included
-    std::thread &a, &b, &d, &e;
+    std::thread &a, &b, &d;
     ~Joiner() {
-      for (std::thread *t : {&a, &b, &d, &e})
+      for (std::thread *t : {&a, &b, &d})
         if (t->joinable()) t->join();
     }
-  } joiner{t_wa, t_pw, t_ip, t_hp};
+  } joiner{t_wa, t_pw, t_hp};
   c->net_off.ensure(hp.net_off.size());
   c->net_off.upload(hp.net_off.data(), hp.net_off.size(), s);
   c->pin_cell.ensure(std::max<size_t>(hp.P, 1));
@@ -1319,10 +1312,6 @@ void load_into(eplace_ctx *c, HostProblem &&hp_in, const uint64_t *ip_seed = nul
   g_h2d += sizeof(int2) * hp.F;
   t_hp.join();
   c->grad_k = grad_k;
-  if (t_ip.joinable()) {
-    t_ip.join();
-    c->pre_ip = true;
-  }
 }
 
 }  // namespace
@@ -1428,16 +1417,70 @@ static eplace_status check_modes(eplace_ctx *c, const eplace_opts &o) {
 }
 
 // Resets the loop state on the device for a new run from positions (sx, sy).
+// Host half of the device initial placement (placer/common.rs:27-117): the
+// taken sites and the count check of the host form, without the shuffle.
+// Returns false when the device form does not apply (a pre-bound cell, or a
+// grid beyond 32-bit site indices): the host form runs instead.
+static bool ip_device_prepare(eplace_ctx *c, eplace_status &st, std::string &msg) {
+  const HostProblem &hp = c->hp;
+  st = EPLACE_OK;
+  if ((uint64_t)hp.W * hp.H >= (1ull << 31)) return false;
+  for (uint32_t i = 0; i < hp.N; ++i)
+    if (hp.init_x[i] >= 0) return false;
+  std::vector<uint32_t> &occ = c->ip_occ_host;
+  occ.clear();
+  for (uint32_t f = 0; f < hp.F; ++f)
+    if (hp.f_logic[f]) occ.push_back((uint32_t)hp.fy[f] * (uint32_t)hp.W + (uint32_t)hp.fx[f]);
+  std::sort(occ.begin(), occ.end());
+  occ.erase(std::unique(occ.begin(), occ.end()), occ.end());
+  c->ip_n = (uint64_t)hp.W * hp.H - occ.size();
+  if (hp.N > c->ip_n) {
+    msg = "logic (need " + std::to_string(hp.N) + " BELs but only " + std::to_string(c->ip_n) + " available)";
+    st = EPLACE_ERR_NO_BELS;
+  }
+  return true;
+}
+
+// Device half: the shuffle and the hand-out on the context's stream, writing
+// x, x_prev and the look-ahead positions (and the integer sites).
+static void ip_device_launch(eplace_ctx *c, uint64_t seed) {
+  const HostProblem &hp = c->hp;
+  cudaStream_t s = c->stream;
+  const size_t n = c->ip_n;
+  if (!c->ip_jump.p) {
+    const std::vector<uint64_t> &m = ip_jump_maps();
+    c->ip_jump.ensure(m.size());
+    c->ip_jump.upload(m.data(), m.size(), s);
+  }
+  c->ip_j.ensure(std::max<size_t>(n, 1));
+  c->ip_cnt.ensure(n + 1);
+  c->ip_start.ensure(n + 1);
+  c->ip_entries.ensure(std::max<size_t>(n, 1));
+  c->ip_block.ensure((n + 1) / 1024 + 2);
+  c->ip_occ.ensure(std::max<size_t>(c->ip_occ_host.size(), 1));
+  c->ip_occ.upload(c->ip_occ_host.data(), c->ip_occ_host.size(), s);
+  c->ip_site.ensure(std::max<size_t>(hp.N, 1));
+  IpBuffers b{c->ip_j.p, c->ip_cnt.p, c->ip_start.p, c->ip_entries.p, c->ip_block.p, c->ip_jump.p,
+              c->ip_occ.p, (uint32_t)c->ip_occ_host.size(), nullptr, hp.N, hp.W, c->ip_site.p,
+              c->x.p, c->xp.p, c->look.p};
+  CK(launch_initial_placement(b, seed ? seed : 1, (uint32_t)n, s));
+}
+
+// sx / sy empty: the positions come from the device initial placement.
 static void reset_state(eplace_ctx *c, const std::vector<int32_t> &sx, const std::vector<int32_t> &sy,
                         const eplace_cfg *cfg) {
   const HostProblem &hp = c->hp;
   cudaStream_t s = c->stream;
-  std::vector<float2> p(hp.N);
-  for (uint32_t i = 0; i < hp.N; ++i) p[i] = make_float2((float)sx[i], (float)sy[i]);
-  c->x.upload(p.data(), hp.N, s);
-  c->xp.upload(p.data(), hp.N, s);
-  CK(cudaMemcpyAsync(c->look.p, p.data(), sizeof(float2) * hp.N, cudaMemcpyHostToDevice, s));
-  g_h2d += sizeof(float2) * hp.N;
+  if (sx.empty() && hp.N) {
+    ip_device_launch(c, cfg->seed);
+  } else {
+    std::vector<float2> p(hp.N);
+    for (uint32_t i = 0; i < hp.N; ++i) p[i] = make_float2((float)sx[i], (float)sy[i]);
+    c->x.upload(p.data(), hp.N, s);
+    c->xp.upload(p.data(), hp.N, s);
+    CK(cudaMemcpyAsync(c->look.p, p.data(), sizeof(float2) * hp.N, cudaMemcpyHostToDevice, s));
+    g_h2d += sizeof(float2) * hp.N;
+  }
   c->gprev.zero(s);
   c->g.zero(s);
   c->acc.zero(s);
@@ -1553,15 +1596,9 @@ struct JobState {
     if (!res->bel_tile && hp.N) return final_st = EPLACE_ERR_INVALID;
     std::string msg;
     eplace_status st;
-    if (c->pre_ip && c->pre_seed == cfg.seed) {  // computed during the load, used once
-      st = c->pre_st;
-      msg = c->pre_msg;
-      isx = std::move(c->pre_isx);
-      isy = std::move(c->pre_isy);
-      c->pre_ip = false;
-    } else {
+    if (!ip_device_prepare(c, st, msg)) {
       st = initial_placement(hp, cfg.seed, isx, isy, msg);
-    }
+    }  // else: isx / isy stay empty, the placement is made on the device in reset_state
     mark("initial_placement");
     if (st != EPLACE_OK) {
       set_err(c, msg);
@@ -2076,6 +2113,17 @@ struct JobState {
           }
           res->best_iter = best->iter;
         } else {
+          if (isx.empty()) {  // the device made the initial placement
+            std::vector<int2> site(hp.N);
+            CK(cudaMemcpy(site.data(), c->ip_site.p, sizeof(int2) * hp.N, cudaMemcpyDeviceToHost));
+            g_d2h += sizeof(int2) * hp.N;
+            isx.resize(hp.N);
+            isy.resize(hp.N);
+            for (uint32_t i = 0; i < hp.N; ++i) {
+              isx[i] = site[i].x;
+              isy[i] = site[i].y;
+            }
+          }
           for (uint32_t i = 0; i < hp.N; ++i) {
             bx[i] = (float)isx[i];
             by[i] = (float)isy[i];
@@ -2273,13 +2321,13 @@ eplace_ctx *ctx_new(int32_t device, eplace_status *st) {
   return c.release();
 }
 
-eplace_status ctx_load_problem(eplace_ctx *c, HostProblem &&hp, const uint64_t *ip_seed) {
+eplace_status ctx_load_problem(eplace_ctx *c, HostProblem &&hp) {
   try {
     CK(cudaSetDevice(c->device));
     CK(cudaStreamSynchronize(c->stream));
     for (auto &l : c->lslots)
       if (l && l->stream) CK(cudaStreamSynchronize(l->stream));
-    load_into(c, std::move(hp), ip_seed);
+    load_into(c, std::move(hp));
     CK(cudaStreamSynchronize(c->stream));
   } catch (const CudaError &e) {
     return cuda_fail(c, e);
@@ -2348,8 +2396,7 @@ eplace_status eplace_place(const eplace_netlist *nl, const eplace_chip *chip, co
     c = ctx_new(device, &st);
     if (!c) return st;
   }
-  const uint64_t ip_seed = cfg ? cfg->seed : 1;
-  st = ctx_load_problem(c, std::move(hp), &ip_seed);
+  st = ctx_load_problem(c, std::move(hp));
   if (st != EPLACE_OK) {
     g_thread_error = c->err;
     eplace_ctx_destroy(c);
@@ -2741,6 +2788,40 @@ eplace_status eplace_stage_barrier_timeout(eplace_ctx *c, int32_t wait_limit_us,
     return cuda_fail(c, e);
   }
   return EPLACE_OK;
+}
+
+eplace_status eplace_stage_initial_placement(eplace_ctx *c, uint64_t seed, int32_t *sx, int32_t *sy,
+                                             int32_t *on_device) {
+  if (!c || (c->hp.N && (!sx || !sy))) return EPLACE_ERR_INVALID;
+  try {
+    CK(cudaSetDevice(c->device));
+    const HostProblem &hp = c->hp;
+    eplace_status st;
+    std::string msg;
+    const bool dev = ip_device_prepare(c, st, msg);
+    if (on_device) *on_device = dev ? 1 : 0;
+    if (!dev) {
+      std::vector<int32_t> hx, hy;
+      st = initial_placement(hp, seed, hx, hy, msg);
+      if (st == EPLACE_OK) {
+        std::copy(hx.begin(), hx.end(), sx);
+        std::copy(hy.begin(), hy.end(), sy);
+      }
+    } else if (st == EPLACE_OK && hp.N) {
+      ip_device_launch(c, seed);
+      std::vector<int2> site(hp.N);
+      CK(cudaMemcpyAsync(site.data(), c->ip_site.p, sizeof(int2) * hp.N, cudaMemcpyDeviceToHost, c->stream));
+      CK(cudaStreamSynchronize(c->stream));
+      for (uint32_t i = 0; i < hp.N; ++i) {
+        sx[i] = site[i].x;
+        sy[i] = site[i].y;
+      }
+    }
+    if (st != EPLACE_OK) set_err(c, msg);
+    return st;
+  } catch (const CudaError &e) {
+    return cuda_fail(c, e);
+  }
 }
 
 eplace_status eplace_stage_hpwl(eplace_ctx *c, const int32_t *sx, const int32_t *sy, int64_t *hpwl) {

@@ -41,9 +41,7 @@ eplace_ctx *ctx_new(int32_t device, eplace_status *st);
 eplace_ctx *take_kept_context(int32_t device, int bx, int by);
 void keep_context(eplace_ctx *c);
 // Loads a validated problem into a context (buffers reused, only grow).
-// ip_seed (optional): also compute the initial placement for that seed
-// during the load, for the next run with the same seed.
-eplace_status ctx_load_problem(eplace_ctx *c, HostProblem &&hp, const uint64_t *ip_seed = nullptr);
+eplace_status ctx_load_problem(eplace_ctx *c, HostProblem &&hp);
 // Whether the tensor-core transform supports the problem's bin grid.
 bool problem_tc_supported(const HostProblem &hp);
 // Sets the calling thread's last error (eplace_last_error with ctx NULL).

@@ -524,6 +524,17 @@ class PlacementContext:
         scal[:] = list(sc)
         return out[0], out[1], out[2], out[3], nlx, nly
 
+    def initial_placement(self, seed: int):
+        """initial_placement (placer/common.rs:27-117) as eplace_run makes it:
+        on the device unless a cell is pre-bound.  Returns (site_x, site_y,
+        on_device)."""
+        n = self.netlist.num_cells
+        sx, sy = np.zeros(n, np.int32), np.zeros(n, np.int32)
+        dev = ctypes.c_int32(0)
+        self._check(self._lib.eplace_stage_initial_placement(self.handle, seed, _abi.ptr(sx, ctypes.c_int32),
+                                                             _abi.ptr(sy, ctypes.c_int32), ctypes.byref(dev)))
+        return sx, sy, bool(dev.value)
+
     def hpwl(self, site_x, site_y):
         v = ctypes.c_int64()
         sx, sy = np.ascontiguousarray(site_x, np.int32), np.ascontiguousarray(site_y, np.int32)

@@ -262,6 +262,15 @@ eplace_status eplace_stage_barrier_timeout(eplace_ctx *ctx, int32_t wait_limit_u
 
 /* Integer HPWL of a binding (anchor sites per movable cell), replaces
  * total_hpwl (metrics/wirelength.rs:10-51). */
+/* The initial placement (placer/common.rs:27-117) for `seed` on the
+ * context's device, as eplace_run makes it: the reference's xorshift64
+ * Fisher-Yates shuffle of the free logic BELs, reformulated so that each
+ * handed-out BEL is found independently (same permutation, bit for bit, as
+ * eplace_initial_placement_host).  Problems with pre-bound cells take the
+ * host form; *on_device (optional) tells which ran.  Writes the context's
+ * positions (the next run resets them). */
+eplace_status eplace_stage_initial_placement(eplace_ctx *ctx, uint64_t seed, int32_t *site_x, int32_t *site_y,
+                                             int32_t *on_device);
 eplace_status eplace_stage_hpwl(eplace_ctx *ctx, const int32_t *site_x,
                                 const int32_t *site_y, int64_t *hpwl);
 
