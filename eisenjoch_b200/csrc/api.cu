@@ -1227,25 +1227,6 @@ void load_into(eplace_ctx *c, HostProblem &&hp_in) {
   c->pin_cell.upload(hp.pin_cell.data(), hp.P, s);
   c->has_driver.ensure(std::max<size_t>(hp.NN, 1));
   c->has_driver.upload(hp.has_driver.data(), hp.NN, s);
-  t_wa.join();
-  {
-    std::copy(cls, cls + kWaClasses, c->wa_cls);
-    c->wa_warps = wa_warps;
-    // The sorted CSR itself is read only by the last class (nets of more
-    // than 224 pins); the others read the padded table.
-    c->wa_off.ensure(soff.size());
-    c->wa_off.upload(soff.data(), soff.size(), s);
-    // Only the last class's part of the sorted pin list is uploaded, at its
-    // sorted-CSR place; no other class reads it.
-    c->wa_pins.ensure(std::max<size_t>(hp.P, 1));
-    if (c->wa_cls[kWaClasses - 1].nets > 0 && !spins.empty()) {
-      const size_t at = soff[c->wa_cls[kWaClasses - 1].first_net];
-      CK(cudaMemcpyAsync(c->wa_pins.p + at, spins.data(), sizeof(uint32_t) * spins.size(), cudaMemcpyHostToDevice, s));
-      g_h2d += sizeof(uint32_t) * spins.size();
-    }
-    c->wa_slots.ensure(slots.size());
-    c->wa_slots.upload(slots.data(), slots.size(), s);
-  }
   const size_t N1 = std::max<size_t>(hp.N, 1);
   std::vector<float2> half(hp.N);
   std::vector<float> area(hp.N);
@@ -1274,10 +1255,6 @@ void load_into(eplace_ctx *c, HostProblem &&hp_in) {
     c->mac_idx.ensure(std::max<size_t>(mi.size(), 1));
     c->mac_idx.upload(mi.data(), mi.size(), s);
   }
-  t_pw.join();
-  std::vector<float> pwf(c->pw_host.begin(), c->pw_host.end());
-  c->pw.ensure(N1);
-  c->pw.upload(pwf.data(), hp.N, s);
   c->look.ensure((size_t)hp.N + hp.F + 1);
   std::vector<float2> fixed(hp.F);
   for (uint32_t f = 0; f < hp.F; ++f) fixed[f] = make_float2((float)hp.fx[f], (float)hp.fy[f]);
@@ -1310,6 +1287,30 @@ void load_into(eplace_ctx *c, HostProblem &&hp_in) {
   for (uint32_t f = 0; f < hp.F; ++f) floc[f] = make_int2(hp.fx[f], hp.fy[f]);
   if (hp.F) CK(cudaMemcpyAsync(c->loc.p + hp.N, floc.data(), sizeof(int2) * hp.F, cudaMemcpyHostToDevice, s));
   g_h2d += sizeof(int2) * hp.F;
+  // The helpers' results last: the work above did not need them.
+  t_wa.join();
+  {
+    std::copy(cls, cls + kWaClasses, c->wa_cls);
+    c->wa_warps = wa_warps;
+    // The sorted CSR itself is read only by the last class (nets of more
+    // than 224 pins); the others read the padded table.
+    c->wa_off.ensure(soff.size());
+    c->wa_off.upload(soff.data(), soff.size(), s);
+    // Only the last class's part of the sorted pin list is uploaded, at its
+    // sorted-CSR place; no other class reads it.
+    c->wa_pins.ensure(std::max<size_t>(hp.P, 1));
+    if (c->wa_cls[kWaClasses - 1].nets > 0 && !spins.empty()) {
+      const size_t at = soff[c->wa_cls[kWaClasses - 1].first_net];
+      CK(cudaMemcpyAsync(c->wa_pins.p + at, spins.data(), sizeof(uint32_t) * spins.size(), cudaMemcpyHostToDevice, s));
+      g_h2d += sizeof(uint32_t) * spins.size();
+    }
+    c->wa_slots.ensure(slots.size());
+    c->wa_slots.upload(slots.data(), slots.size(), s);
+  }
+  t_pw.join();
+  std::vector<float> pwf(c->pw_host.begin(), c->pw_host.end());
+  c->pw.ensure(N1);
+  c->pw.upload(pwf.data(), hp.N, s);
   t_hp.join();
   c->grad_k = grad_k;
 }
