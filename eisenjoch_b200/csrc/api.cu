@@ -1443,8 +1443,9 @@ static bool ip_device_prepare(eplace_ctx *c, eplace_status &st, std::string &msg
 }
 
 // Device half: the shuffle and the hand-out on the context's stream, writing
-// x, x_prev and the look-ahead positions (and the integer sites).
-static void ip_device_launch(eplace_ctx *c, uint64_t seed) {
+// x, x_prev and the look-ahead positions (and the integer sites).  Returns
+// the kernels it launched.
+static int ip_device_launch(eplace_ctx *c, uint64_t seed) {
   const HostProblem &hp = c->hp;
   cudaStream_t s = c->stream;
   const size_t n = c->ip_n;
@@ -1465,15 +1466,18 @@ static void ip_device_launch(eplace_ctx *c, uint64_t seed) {
               c->ip_occ.p, (uint32_t)c->ip_occ_host.size(), nullptr, hp.N, hp.W, c->ip_site.p,
               c->x.p, c->xp.p, c->look.p};
   CK(launch_initial_placement(b, seed ? seed : 1, (uint32_t)n, s));
+  return n > 1 ? 7 : 4;
 }
 
 // sx / sy empty: the positions come from the device initial placement.
-static void reset_state(eplace_ctx *c, const std::vector<int32_t> &sx, const std::vector<int32_t> &sy,
-                        const eplace_cfg *cfg) {
+// Returns the kernels launched.
+static int reset_state(eplace_ctx *c, const std::vector<int32_t> &sx, const std::vector<int32_t> &sy,
+                       const eplace_cfg *cfg) {
   const HostProblem &hp = c->hp;
   cudaStream_t s = c->stream;
+  int launches = 0;
   if (sx.empty() && hp.N) {
-    ip_device_launch(c, cfg->seed);
+    launches = ip_device_launch(c, cfg->seed);
   } else {
     std::vector<float2> p(hp.N);
     for (uint32_t i = 0; i < hp.N; ++i) p[i] = make_float2((float)sx[i], (float)sy[i]);
@@ -1497,6 +1501,7 @@ static void reset_state(eplace_ctx *c, const std::vector<int32_t> &sx, const std
   c->sc.upload(&sc, 1, s);
   c->bar.zero(s);
   CK(cudaStreamSynchronize(s));
+  return launches;
 }
 
 // SM clock cycles of a wait limit given in microseconds (0: the kernel default).
@@ -1621,7 +1626,7 @@ struct JobState {
         ++c->buf_epoch;
       }
       c->spin_cycles = wait_cycles(c->device, opts.wait_limit_us);
-      reset_state(c, isx, isy, &cfg);
+      ip_launches = reset_state(c, isx, isy, &cfg);
       autotune_launches(c, gamma, opts.field_mode, tc);
       mark("device_reset");
       // Host resources persist in the context across runs.
@@ -2064,7 +2069,7 @@ struct JobState {
       CK(cudaEventElapsedTime(&ms, ev0, ev1));
       res->gpu_seconds = ms * 1e-3;
       res->gpu_launches = (uint64_t)(kLaunchesPerIter + (c->split_step ? 2 : 0)) * launched_iters +
-                          (gpu_legal ? 2 * cps.size() : 0);
+                          (gpu_legal ? 2 * cps.size() : 0) + (uint64_t)ip_launches;
       res->iters = (uint32_t)iters_done;
       res->converged = converged_chunk < chunks.size() ? 1 : 0;
       res->overlap = last_overlap;
@@ -2187,6 +2192,7 @@ struct JobState {
   uint64_t max_iters = 0, interval = 1;
   float gamma = 0.f;
   std::vector<int32_t> isx, isy;
+  int ip_launches = 0;  // kernels of the device initial placement
   std::vector<std::pair<const char *, double>> marks;
   std::vector<Chunk> chunks;
   int inflight = 1;
