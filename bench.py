@@ -66,7 +66,7 @@ def parse():
     ap.add_argument("--batched-jobs", type=int, default=64)
     ap.add_argument("--served-jobs", type=int, default=2000,
                     help="jobs of the served stream (the configuration's 2,000; fewer for a subsample)")
-    ap.add_argument("--served-rate", type=float, default=250.0,
+    ap.add_argument("--served-rate", type=float, default=600.0,
                     help="offered rate of the served stream, jobs/s (above both forms' capacity, so the "
                          "throughput of each is measured)")
     ap.add_argument("--served-rate-2", type=float, default=0.0,

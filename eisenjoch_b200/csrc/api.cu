@@ -1448,6 +1448,7 @@ static bool ip_device_prepare(eplace_ctx *c, eplace_status &st, std::string &msg
 static int ip_device_launch(eplace_ctx *c, uint64_t seed) {
   const HostProblem &hp = c->hp;
   cudaStream_t s = c->stream;
+  AllocOn on_stream(s);  // scratch that grows is allocated in stream order
   const size_t n = c->ip_n;
   if (!c->ip_jump.p) {
     const std::vector<uint64_t> &m = ip_jump_maps();
@@ -1470,22 +1471,14 @@ static int ip_device_launch(eplace_ctx *c, uint64_t seed) {
 }
 
 // sx / sy empty: the positions come from the device initial placement.
-// Returns the kernels launched.
+// Returns the kernels launched.  Nothing here waits for the device: the
+// scalars leave first (a copy from pageable memory waits for the stream's
+// earlier work, so it goes before the placement kernels, not after them),
+// and every later use of the state is ordered on the same stream.
 static int reset_state(eplace_ctx *c, const std::vector<int32_t> &sx, const std::vector<int32_t> &sy,
                        const eplace_cfg *cfg) {
   const HostProblem &hp = c->hp;
   cudaStream_t s = c->stream;
-  int launches = 0;
-  if (sx.empty() && hp.N) {
-    launches = ip_device_launch(c, cfg->seed);
-  } else {
-    std::vector<float2> p(hp.N);
-    for (uint32_t i = 0; i < hp.N; ++i) p[i] = make_float2((float)sx[i], (float)sy[i]);
-    c->x.upload(p.data(), hp.N, s);
-    c->xp.upload(p.data(), hp.N, s);
-    CK(cudaMemcpyAsync(c->look.p, p.data(), sizeof(float2) * hp.N, cudaMemcpyHostToDevice, s));
-    g_h2d += sizeof(float2) * hp.N;
-  }
   c->gprev.zero(s);
   c->g.zero(s);
   c->acc.zero(s);
@@ -1500,7 +1493,17 @@ static int reset_state(eplace_ctx *c, const std::vector<int32_t> &sx, const std:
   sc.spin_cycles = c->spin_cycles;
   c->sc.upload(&sc, 1, s);
   c->bar.zero(s);
-  CK(cudaStreamSynchronize(s));
+  int launches = 0;
+  if (sx.empty() && hp.N) {
+    launches = ip_device_launch(c, cfg->seed);
+  } else {
+    std::vector<float2> p(hp.N);
+    for (uint32_t i = 0; i < hp.N; ++i) p[i] = make_float2((float)sx[i], (float)sy[i]);
+    c->x.upload(p.data(), hp.N, s);
+    c->xp.upload(p.data(), hp.N, s);
+    CK(cudaMemcpyAsync(c->look.p, p.data(), sizeof(float2) * hp.N, cudaMemcpyHostToDevice, s));
+    g_h2d += sizeof(float2) * hp.N;
+  }
   return launches;
 }
 
