@@ -8,8 +8,10 @@
 // read finished intervals, fold finished legalisations) and completes the
 // finished ones.  A job runs on a context of its own; contexts are kept
 // after their job and re-loaded for the next one (their device buffers only
-// grow, a context whose bin grid matches is preferred so the DCT matrices
-// stay), so a steady stream of jobs allocates and frees nothing.  All jobs
+// grow, a context whose bin grid matches is preferred so the DCT matrices,
+// tensor maps and interval graph stay, and twice max_jobs contexts are made
+// at start so that each grid of a mixed stream finds one), so a steady
+// stream of jobs allocates and frees nothing.  All jobs
 // share one host legaliser pool.  Every job's arithmetic is its own (its
 // own buffers, streams and deterministic reductions), so its result equals
 // a single eplace_run of it.
@@ -139,12 +141,24 @@ struct eplace_server {
   // stay), else any idle one, else a new one.
   eplace_ctx *take_context(const JobRec &r, eplace_status *st) {
     *st = EPLACE_OK;
-    size_t pick = idle.size();
-    for (size_t k = 0; k < idle.size(); ++k)
+    // An idle context with this bin grid keeps its DCT matrices, tensor
+    // maps and interval graph; else one never loaded (the server creates
+    // twice max_jobs of them at start, so a mixed stream's grids each find
+    // one) while the memory the contexts hold leaves room; else any.
+    size_t pick = idle.size(), fresh = idle.size();
+    for (size_t k = 0; k < idle.size(); ++k) {
       if (ctx_bins_x(idle[k]) == r.hp.BX && ctx_bins_y(idle[k]) == r.hp.BY) {
         pick = k;
         break;
       }
+      if (ctx_bins_x(idle[k]) <= 0 && fresh == idle.size()) fresh = k;
+    }
+    uint64_t held;
+    {
+      std::lock_guard<std::mutex> g(m);
+      held = device_bytes;
+    }
+    if (pick == idle.size() && fresh < idle.size() && held + r.footprint <= budget) pick = fresh;
     if (pick == idle.size() && !idle.empty()) pick = idle.size() - 1;
     if (pick < idle.size()) {
       eplace_ctx *c = idle[pick];
@@ -325,6 +339,15 @@ eplace_status eplace_server_create(const eplace_server_cfg *cfg, eplace_server *
   const int nt = s->cfg.legal_threads > 0 ? s->cfg.legal_threads : (int)std::max(1u, std::thread::hardware_concurrency());
   s->pool.reset(new Pool(std::min(nt, 64), 5));
   s->loaders.reset(new Pool(4));
+  // Contexts made up front (streams, events, a few scalars each): made
+  // while jobs run, their set-up would stall the other jobs' streams.
+  for (int k = 0; k < 2 * s->cfg.max_jobs; ++k) {
+    eplace_status st = EPLACE_OK;
+    eplace_ctx *c = ctx_new(s->cfg.device, &st);
+    if (!c) return st;
+    s->idle.push_back(c);
+    ++s->contexts;
+  }
   eplace_server *raw = s.get();
   s->sched = std::thread([raw] { raw->loop(); });
   *out = s.release();

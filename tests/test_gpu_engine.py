@@ -54,7 +54,8 @@ def test_results_in_the_mix_equal_alone(designs, max_jobs):
             assert info.latency_seconds >= info.run_seconds > 0
         st = srv.stats()
         assert st["finished"] == len(designs) and st["running"] == 0 and st["queued"] == 0
-        assert st["contexts"] <= max_jobs
+        # at most twice max_jobs contexts are kept (one per bin grid of the mix)
+        assert st["contexts"] <= 2 * max_jobs
 
 
 def test_context_reloaded_across_bin_grids_equals_fresh(designs):
