@@ -211,7 +211,7 @@ def algorithmic(nl, chip):
     }
 
 
-def precision_form_roofline(E, args, hbm, bf16, workload="electro_800k_2048"):
+def precision_form_roofline(E, args, hbm, bf16, peak_src, workload="electro_800k_2048"):
     """Per-kernel CUDA-event times (one graph-replayed iteration) and their
     fractions of the measured peaks on the 800k-cell precision form."""
     w = E.WORKLOADS[workload]
@@ -221,8 +221,9 @@ def precision_form_roofline(E, args, hbm, bf16, workload="electro_800k_2048"):
     with E.PlacementContext(nl, chip) as ctx:
         ms = ctx.profile_stages(cfg, reps=args.profile_reps, opts=opts)
     algo = algorithmic(nl, chip)
-    out = {"workload": workload, "dct": "bf16x3 tcgen05", "peak_source": "measured (MEASURED_PEAKS.json)",
-           "stages": {}}
+    out = {"workload": workload, "dct": "bf16x3 tcgen05",
+           "peak_source": "measured (MEASURED_PEAKS.json)" if peak_src == "measured" else
+           "fallback (%.0f GB/s, %.0f TFLOP/s)" % (hbm, bf16), "stages": {}}
     for k, t in ms.items():
         kd, am = algo[k]
         d = {"ms": t}
@@ -711,7 +712,7 @@ def ours(args, dist):
     # BF16x3 transform): the configuration whose bytes exceed L2 ---
     prec = prec_report = None
     if not args.no_precision_form and dist.rank == 0:
-        prec = precision_form_roofline(E, args, hbm, bf16)
+        prec = precision_form_roofline(E, args, hbm, bf16, peak_src)
         prec_report = precision_report(E, dev)
 
     mixed_cfg = E.ElectroPlaceCfg(max_iters=500)
