@@ -295,6 +295,15 @@ struct eplace_ctx {
   DBuf<float> mB3g, mL6g;                   // potential-gradient field (extension)
   DBuf<float> wx, gx2, wy, gy2;
   DBuf<GemmOp> ops;                         // 0: GEMM1, 1: GEMM2, 2-3: GEMM3, 4-5: GEMM4
+  // Folded FP32 transform (grids with bins_x, bins_y multiples of 8): the
+  // half matrices (even / odd frequencies of the first or second half of
+  // the spatial index), the E / O products of GEMMs 3 and 4, their op
+  // tables (12 per field mode) and butterflies (2 + 2 per field mode).
+  bool fold = false;
+  DBuf<float> hB1e, hB1o, hL2e, hL2o, hB3e, hB3o, hB5e, hB5o, hB3ge, hB3go, hL4e, hL4o, hL6e, hL6o, hL6ge, hL6go;
+  DBuf<float> f3, f4;
+  DBuf<GemmOp> hops;
+  DBuf<FlyOp> fops;
   DBuf<double> mom, part, part2, part_b;
   DBuf<DevScalars> sc;
   DBuf<IterLog> log;
@@ -515,7 +524,54 @@ int build_wa_classes(const std::vector<uint32_t> &off, WaClass (&cls)[kWaClasses
 // once per process and kept; uploading a kept set costs only the copy.
 struct HostMats {
   std::vector<float> B1, B3, B5, L2, L4, L6, B3g, L6g, wx, gx2, wy, gy2;
+  // folded halves (bins_x, bins_y multiples of 8), see fold_matrices
+  std::vector<float> B1e, B1o, L2e, L2o, B3e, B3o, B5e, B5o, B3ge, B3go, L4e, L4o, L6e, L6o, L6ge, L6go;
 };
+
+// The transform's matrices fold about the middle of their spatial index:
+// with theta = pi k (n + 1/2) / N, theta(N - 1 - n) = pi k - theta(n), so
+// cos and sin of theta (and of the DST-III's pi (k + 1)(n + 1/2) / N) at
+// n and N - 1 - n agree up to the sign s (-1)^k, s = +1 except for the
+// potential-gradient field's -sin(theta), where s = -1.  A product over the
+// spatial index then splits into the even-k half applied to x(n) + x(N-1-n)
+// and the odd-k half applied to x(n) - x(N-1-n), each (N/2) x (N/2); a
+// product over k gives E = sum over even k and O = sum over odd k, and the
+// outputs n, N - 1 - n are E + O and s (E - O).  Half the multiply-adds.
+// Halves kept here (row-major):
+//   B1e/o  [x < W/2][m]   = B1[x][2m(+1)]      L2e/o [m][y < H/2]  = L2[2m(+1)][y]
+//   B3e/o, B5e/o, B3ge/o  [m][x < W/2] = B[2m(+1)][x]
+//   L4e/o, L6e/o, L6ge/o  [y < H/2][m] = L[y][2m(+1)]
+void fold_matrices(int W, int H, HostMats &m) {
+  const int hw = W / 2, hh = H / 2;
+  auto cols = [](const std::vector<float> &M, int n, int rows, int par, std::vector<float> &out) {
+    out.resize((size_t)rows * (n / 2));
+    for (int r = 0; r < rows; ++r)
+      for (int c = 0; c < n / 2; ++c) out[(size_t)r * (n / 2) + c] = M[(size_t)r * n + 2 * c + par];
+  };  // rows 0..rows-1, every other column from par
+  auto rowsel = [](const std::vector<float> &M, int n, int cols, int par, std::vector<float> &out) {
+    out.resize((size_t)(n / 2) * cols);
+    for (int r = 0; r < n / 2; ++r)
+      for (int c = 0; c < cols; ++c) out[(size_t)r * cols + c] = M[(size_t)(2 * r + par) * n + c];
+  };  // every other row from par, columns 0..cols-1
+  cols(m.B1, W, hw, 0, m.B1e);
+  cols(m.B1, W, hw, 1, m.B1o);
+  rowsel(m.L2, H, hh, 0, m.L2e);
+  rowsel(m.L2, H, hh, 1, m.L2o);
+  rowsel(m.B3, W, hw, 0, m.B3e);
+  rowsel(m.B3, W, hw, 1, m.B3o);
+  rowsel(m.B5, W, hw, 0, m.B5e);
+  rowsel(m.B5, W, hw, 1, m.B5o);
+  rowsel(m.B3g, W, hw, 0, m.B3ge);
+  rowsel(m.B3g, W, hw, 1, m.B3go);
+  cols(m.L4, H, hh, 0, m.L4e);
+  cols(m.L4, H, hh, 1, m.L4o);
+  cols(m.L6, H, hh, 0, m.L6e);
+  cols(m.L6, H, hh, 1, m.L6o);
+  cols(m.L6g, H, hh, 0, m.L6ge);
+  cols(m.L6g, H, hh, 1, m.L6go);
+}
+
+bool fold_ok(int W, int H) { return W % 8 == 0 && H % 8 == 0 && W >= 16 && H >= 16; }
 
 void compute_host_mats(int W, int H, HostMats &m) {
   const double pi = 3.14159265358979323846;
@@ -569,6 +625,7 @@ const HostMats &host_mats(int W, int H) {
   if (!slot) {
     slot.reset(new HostMats());
     compute_host_mats(W, H, *slot);
+    if (fold_ok(W, H)) fold_matrices(W, H, *slot);
   }
   return *slot;
 }
@@ -608,8 +665,83 @@ void build_matrices(eplace_ctx *c) {
       {c->mL4.p, c->U.p, c->Ex.p, nullptr},
       {c->mL6g.p, c->V.p, c->Ey.p, nullptr},
   };
+  for (auto &o : ops) {  // plain row-major operands, nothing folded
+    o.a_mir = o.a_full = o.b_mir = o.b_full = o.col_split = 0;
+    o.row_par = -1;
+  }
+  // leading dimensions: A is M x K, B is K x N, C is M x N
+  const int ld[6][3] = {{W, W, W}, {H, W, W}, {W, W, W}, {W, W, W}, {H, W, W}, {H, W, W}};
+  for (int k = 0; k < 12; ++k) {
+    ops[k].lda = ld[k % 6][0];
+    ops[k].ldb = ld[k % 6][1];
+    ops[k].ldc = ld[k % 6][2];
+  }
   c->ops.ensure(12);
   c->ops.upload(ops, 12, s);
+  c->fold = fold_ok(W, H);
+  if (c->fold) {
+    const int hw = W / 2, hh = H / 2;
+    const size_t q = (size_t)H * hw;  // one E or O of GEMM 3 ([H][W/2]); GEMM 4's are [H/2][W], the same size
+    DBuf<float> *hb[16] = {&c->hB1e, &c->hB1o, &c->hL2e, &c->hL2o, &c->hB3e, &c->hB3o, &c->hB5e, &c->hB5o,
+                           &c->hB3ge, &c->hB3go, &c->hL4e, &c->hL4o, &c->hL6e, &c->hL6o, &c->hL6ge, &c->hL6go};
+    const std::vector<float> *hv[16] = {&hm.B1e, &hm.B1o, &hm.L2e, &hm.L2o, &hm.B3e, &hm.B3o, &hm.B5e, &hm.B5o,
+                                        &hm.B3ge, &hm.B3go, &hm.L4e, &hm.L4o, &hm.L6e, &hm.L6o, &hm.L6ge, &hm.L6go};
+    for (int k = 0; k < 16; ++k) {
+      hb[k]->ensure(hv[k]->size());
+      hb[k]->upload(hv[k]->data(), hv[k]->size(), s);
+    }
+    c->f3.ensure(4 * q);
+    c->f4.ensure(4 * q);
+    float *f3 = c->f3.p, *f4 = c->f4.p;
+    auto op = [](const float *A, int lda, const float *B, int ldb, float *C, float *C2, int ldc) {
+      GemmOp o{A, B, C, C2, lda, ldb, ldc, 0, 0, 0, 0, -1, 0};
+      return o;
+    };
+    GemmOp h[24];
+    for (int fm = 0; fm < 2; ++fm) {
+      GemmOp *g = h + 12 * fm;
+      // GEMM 1: T = rho B1, columns of rho folded; T's columns even kx first
+      g[0] = op(c->rho.p, W, c->hB1e.p, hw, c->T.p, nullptr, W);
+      g[0].a_mir = 1;
+      g[0].a_full = W;
+      g[1] = op(c->rho.p, W, c->hB1o.p, hw, c->T.p + hw, nullptr, W);
+      g[1].a_mir = -1;
+      g[1].a_full = W;
+      // GEMM 2: L2 T + spectral epilogue, rows of T folded; Ex^, Ey^ rows even ky first
+      g[2] = op(c->hL2e.p, hh, c->T.p, W, c->Exh.p, c->Eyh.p, W);
+      g[2].b_mir = 1;
+      g[2].b_full = H;
+      g[2].row_par = 0;
+      g[2].col_split = 1;
+      g[3] = op(c->hL2o.p, hh, c->T.p, W, c->Exh.p + (size_t)hh * W, c->Eyh.p + (size_t)hh * W, W);
+      g[3].b_mir = -1;
+      g[3].b_full = H;
+      g[3].row_par = 1;
+      g[3].col_split = 1;
+      // GEMM 3: E / O of U = Ex^ B3 (B3g) and V = Ey^ B5
+      g[4] = op(c->Exh.p, W, fm ? c->hB3ge.p : c->hB3e.p, hw, f3, nullptr, hw);
+      g[5] = op(c->Exh.p + hw, W, fm ? c->hB3go.p : c->hB3o.p, hw, f3 + q, nullptr, hw);
+      g[6] = op(c->Eyh.p, W, c->hB5e.p, hw, f3 + 2 * q, nullptr, hw);
+      g[7] = op(c->Eyh.p + hw, W, c->hB5o.p, hw, f3 + 3 * q, nullptr, hw);
+      // GEMM 4: E / O of Ex = L4 U and Ey = L6 (L6g) V (U, V rows even ky first)
+      g[8] = op(c->hL4e.p, hh, c->U.p, W, f4, nullptr, W);
+      g[9] = op(c->hL4o.p, hh, c->U.p + (size_t)hh * W, W, f4 + q, nullptr, W);
+      g[10] = op(fm ? c->hL6ge.p : c->hL6e.p, hh, c->V.p, W, f4 + 2 * q, nullptr, W);
+      g[11] = op(fm ? c->hL6go.p : c->hL6o.p, hh, c->V.p + (size_t)hh * W, W, f4 + 3 * q, nullptr, W);
+    }
+    c->hops.ensure(24);
+    c->hops.upload(h, 24, s);
+    FlyOp fl[8];
+    for (int fm = 0; fm < 2; ++fm) {
+      FlyOp *f = fl + 4 * fm;
+      f[0] = FlyOp{f3, f3 + q, c->U.p, fm ? -1.0f : 1.0f};
+      f[1] = FlyOp{f3 + 2 * q, f3 + 3 * q, c->V.p, 1.0f};
+      f[2] = FlyOp{f4, f4 + q, c->Ex.p, 1.0f};
+      f[3] = FlyOp{f4 + 2 * q, f4 + 3 * q, c->Ey.p, fm ? -1.0f : 1.0f};
+    }
+    c->fops.ensure(8);
+    c->fops.upload(fl, 8, s);
+  }
   CK(cudaStreamSynchronize(s));
 }
 
@@ -843,6 +975,30 @@ void launch_field_gemm(eplace_ctx *c, int g, float *phi, int field_mode, bool tc
     }
     return;
   }
+  if (c->fold) {
+    const GemmOp *h = c->hops.p + 12 * fm;
+    const FlyOp *f = c->fops.p + 4 * fm;
+    const int hw = W / 2, hh = H / 2;
+    switch (g) {
+      case 0:
+        CK(launch_sgemm(h + 0, 2, H, hw, hw, c->stream, c->gemm_tile[0]));
+        break;
+      case 1: {
+        SpectralArgs sp{c->wx.p, c->gx2.p, c->wy.p, c->gy2.p, (float)(4.0 / ((double)W * H)), phi};
+        CK(launch_sgemm_spectral(h + 2, 2, hh, W, hh, sp, c->stream, c->gemm_tile[1]));
+        break;
+      }
+      case 2:
+        CK(launch_sgemm(h + 4, 4, H, hw, hw, c->stream, c->gemm_tile[2]));
+        CK(launch_fly_cols(f, 2, H, W, c->stream));
+        break;
+      default:
+        CK(launch_sgemm(h + 8, 4, hh, W, hh, c->stream, c->gemm_tile[3]));
+        CK(launch_fly_rows(f + 2, 2, H, W, c->stream));
+        break;
+    }
+    return;
+  }
   const GemmOp *ops = c->ops.p + (fm ? 6 : 0);
   switch (g) {
     case 0:
@@ -850,7 +1006,7 @@ void launch_field_gemm(eplace_ctx *c, int g, float *phi, int field_mode, bool tc
       break;
     case 1: {
       SpectralArgs sp{c->wx.p, c->gx2.p, c->wy.p, c->gy2.p, (float)(4.0 / ((double)W * H)), phi};
-      CK(launch_sgemm_spectral(ops + 1, H, W, H, sp, c->stream, c->gemm_tile[1]));
+      CK(launch_sgemm_spectral(ops + 1, 1, H, W, H, sp, c->stream, c->gemm_tile[1]));
       break;
     }
     case 2:
@@ -2071,7 +2227,8 @@ struct JobState {
       float ms = 0.f;
       CK(cudaEventElapsedTime(&ms, ev0, ev1));
       res->gpu_seconds = ms * 1e-3;
-      res->gpu_launches = (uint64_t)(kLaunchesPerIter + (c->split_step ? 2 : 0)) * launched_iters +
+      res->gpu_launches = (uint64_t)(kLaunchesPerIter + (c->split_step ? 2 : 0) + (c->fold && !tc ? 2 : 0)) *
+                              launched_iters +
                           (gpu_legal ? 2 * cps.size() : 0) + (uint64_t)ip_launches;
       res->iters = (uint32_t)iters_done;
       res->converged = converged_chunk < chunks.size() ? 1 : 0;

@@ -528,6 +528,34 @@ constexpr int GK = 16;
 // TM/S-row slice of the tile in rank order ((p0 + p1) + p2) + ... through
 // distributed shared memory, then runs the epilogue on that slice.  The
 // order is the same for both tile sizes, so they still give the same bits.
+// One output of a SIMT GEMM.  With SPECTRAL: density.rs:114-153, scale
+// 4/(WH), x1/2 on the kx = 0 and ky = 0 lines, phi = a / (2(1-cos wx) +
+// 2(1-cos wy)), E = phi * w, at the frequencies (ky, kx) the op's layout
+// gives the output (row, column); phi is written at its natural place.
+template <bool SPECTRAL>
+__device__ __forceinline__ void gemm_store(const GemmOp &op, const SpectralArgs &sp, int r, int c, int N, float v) {
+  const size_t o = (size_t)r * op.ldc + c;
+  if (SPECTRAL) {
+    const int ky = op.row_par < 0 ? r : 2 * r + op.row_par;
+    const int kx = op.col_split ? (c < N / 2 ? 2 * c : 2 * (c - N / 2) + 1) : c;
+    float s = sp.scale;
+    if (kx == 0) s *= 0.5f;
+    if (ky == 0) s *= 0.5f;
+    const float den = sp.gx2[kx] + sp.gy2[ky];
+    float phi = 0.0f, ex = 0.0f, ey = 0.0f;
+    if (!(den < 1e-30f)) {
+      phi = v * s / den;
+      ex = phi * sp.wx[kx];
+      ey = phi * sp.wy[ky];
+    }
+    op.C[o] = ex;
+    op.C2[o] = ey;
+    if (sp.phi) sp.phi[(size_t)ky * N + kx] = phi;
+  } else {
+    op.C[o] = v;
+  }
+}
+
 template <bool SPECTRAL, int TM, int TN, int S>
 __global__ void __launch_bounds__((TM / 4) * (TN / 4)) k_sgemm(const GemmOp *ops, int M, int N, int K,
                                                                SpectralArgs sp) {
@@ -541,31 +569,52 @@ __global__ void __launch_bounds__((TM / 4) * (TN / 4)) k_sgemm(const GemmOp *ops
   auto Bs = reinterpret_cast<float(*)[GK][TN + 4]>(smem + 2 * GK * (TM + 4));
   const int tid = threadIdx.x, tx = tid % (TN / 4), ty = tid / (TN / 4);
   const int bm = blockIdx.y * TM, bn = blockIdx.x * TN;
-  const bool vec = ((K & 3) == 0) && ((N & 3) == 0);
+  const bool vec = ((K & 3) == 0) && ((N & 3) == 0) && ((op.lda & 3) == 0) && ((op.ldb & 3) == 0) &&
+                   ((op.a_full & 3) == 0);
+  const float am = (float)op.a_mir, bmir = (float)op.b_mir;
   float ra[LA][4], rb[LB][4];
   auto load = [&](int k0) {
 #pragma unroll
     for (int l = 0; l < LA; ++l) {
       const int f = tid + l * T;
       const int gr = bm + f / (GK / 4), gk = k0 + (f % (GK / 4)) * 4;
+      const float *arow = op.A + (size_t)gr * op.lda;
       if (vec && gr < M && gk + 3 < K) {
-        const float4 t = *reinterpret_cast<const float4 *>(op.A + (size_t)gr * K + gk);
+        float4 t = *reinterpret_cast<const float4 *>(arow + gk);
+        if (op.a_mir) {  // columns a_full-1-gk-j, j = 0..3: the block below, reversed
+          const float4 u = *reinterpret_cast<const float4 *>(arow + (op.a_full - 4 - gk));
+          t.x += am * u.w; t.y += am * u.z; t.z += am * u.y; t.w += am * u.x;
+        }
         ra[l][0] = t.x; ra[l][1] = t.y; ra[l][2] = t.z; ra[l][3] = t.w;
       } else {
 #pragma unroll
-        for (int j = 0; j < 4; ++j) ra[l][j] = (gr < M && gk + j < K) ? op.A[(size_t)gr * K + gk + j] : 0.0f;
+        for (int j = 0; j < 4; ++j) {
+          float v = (gr < M && gk + j < K) ? arow[gk + j] : 0.0f;
+          if (op.a_mir && gr < M && gk + j < K) v += am * arow[op.a_full - 1 - (gk + j)];
+          ra[l][j] = v;
+        }
       }
     }
 #pragma unroll
     for (int l = 0; l < LB; ++l) {
       const int f = tid + l * T;
       const int gk = k0 + f / (TN / 4), gc = bn + (f % (TN / 4)) * 4;
+      const float *brow = op.B + (size_t)gk * op.ldb;
+      const float *bmrow = op.b_mir ? op.B + (size_t)(op.b_full - 1 - gk) * op.ldb : brow;
       if (vec && gk < K && gc + 3 < N) {
-        const float4 t = *reinterpret_cast<const float4 *>(op.B + (size_t)gk * N + gc);
+        float4 t = *reinterpret_cast<const float4 *>(brow + gc);
+        if (op.b_mir) {
+          const float4 u = *reinterpret_cast<const float4 *>(bmrow + gc);
+          t.x += bmir * u.x; t.y += bmir * u.y; t.z += bmir * u.z; t.w += bmir * u.w;
+        }
         rb[l][0] = t.x; rb[l][1] = t.y; rb[l][2] = t.z; rb[l][3] = t.w;
       } else {
 #pragma unroll
-        for (int j = 0; j < 4; ++j) rb[l][j] = (gk < K && gc + j < N) ? op.B[(size_t)gk * N + gc + j] : 0.0f;
+        for (int j = 0; j < 4; ++j) {
+          float v = (gk < K && gc + j < N) ? brow[gc + j] : 0.0f;
+          if (op.b_mir && gk < K && gc + j < N) v += bmir * bmrow[gc + j];
+          rb[l][j] = v;
+        }
       }
     }
   };
@@ -642,24 +691,7 @@ __global__ void __launch_bounds__((TM / 4) * (TN / 4)) k_sgemm(const GemmOp *ops
       for (int j = 0; j < 4; ++j) {
         const int cidx = bn + lc + j;
         if (cidx >= N) continue;
-        const size_t o = (size_t)r * N + cidx;
-        if (SPECTRAL) {
-          float s = sp.scale;
-          if (cidx == 0) s *= 0.5f;
-          if (r == 0) s *= 0.5f;
-          const float den = sp.gx2[cidx] + sp.gy2[r];
-          float phi = 0.0f, ex = 0.0f, ey = 0.0f;
-          if (!(den < 1e-30f)) {
-            phi = vv[j] * s / den;
-            ex = phi * sp.wx[cidx];
-            ey = phi * sp.wy[r];
-          }
-          op.C[o] = ex;
-          op.C2[o] = ey;
-          if (sp.phi) sp.phi[o] = phi;
-        } else {
-          op.C[o] = vv[j];
-        }
+        gemm_store<SPECTRAL>(op, sp, r, cidx, N, vv[j]);
       }
     }
     cluster.sync();  // no CTA leaves while another reads its partial tile
@@ -673,26 +705,7 @@ __global__ void __launch_bounds__((TM / 4) * (TN / 4)) k_sgemm(const GemmOp *ops
     for (int j = 0; j < 4; ++j) {
       const int cidx = bn + tx * 4 + j;
       if (cidx >= N) continue;
-      const size_t o = (size_t)r * N + cidx;
-      if (SPECTRAL) {
-        // density.rs:114-153: scale 4/(WH), x1/2 on the kx = 0 and ky = 0
-        // lines, phi = a / (2(1-cos wx) + 2(1-cos wy)), E = phi * w.
-        float s = sp.scale;
-        if (cidx == 0) s *= 0.5f;
-        if (r == 0) s *= 0.5f;
-        const float den = sp.gx2[cidx] + sp.gy2[r];
-        float phi = 0.0f, ex = 0.0f, ey = 0.0f;
-        if (!(den < 1e-30f)) {
-          phi = acc[i][j] * s / den;
-          ex = phi * sp.wx[cidx];
-          ey = phi * sp.wy[r];
-        }
-        op.C[o] = ex;
-        op.C2[o] = ey;
-        if (sp.phi) sp.phi[o] = phi;
-      } else {
-        op.C[o] = acc[i][j];
-      }
+      gemm_store<SPECTRAL>(op, sp, r, cidx, N, acc[i][j]);
     }
   }
 }
@@ -1151,11 +1164,40 @@ cudaError_t launch_sgemm(const GemmOp *ops, int nb, int M, int N, int K, cudaStr
   return sgemm_launch<false, 64, 64>(ops, nb, M, N, K, SpectralArgs{}, s);
 }
 
-cudaError_t launch_sgemm_spectral(const GemmOp *ops, int M, int N, int K, const SpectralArgs &sp,
+cudaError_t launch_sgemm_spectral(const GemmOp *ops, int nb, int M, int N, int K, const SpectralArgs &sp,
                                   cudaStream_t s, int tile) {
-  if (tile == 32 || (tile == 0 && sgemm_small_tile(M, N, 1, K)))
-    return sgemm_launch<true, 32, 32>(ops, 1, M, N, K, sp, s);
-  return sgemm_launch<true, 64, 64>(ops, 1, M, N, K, sp, s);
+  if (tile == 32 || (tile == 0 && sgemm_small_tile(M, N, nb, K)))
+    return sgemm_launch<true, 32, 32>(ops, nb, M, N, K, sp, s);
+  return sgemm_launch<true, 64, 64>(ops, nb, M, N, K, sp, s);
+}
+
+namespace {
+__global__ void k_fly_cols(const FlyOp *ops, int H, int W) {
+  const FlyOp op = ops[blockIdx.z];
+  const int hw = W / 2;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x, r = blockIdx.y;
+  if (x >= hw || r >= H) return;
+  const float e = op.E[(size_t)r * hw + x], o = op.O[(size_t)r * hw + x];
+  op.out[(size_t)r * W + x] = e + o;
+  op.out[(size_t)r * W + (W - 1 - x)] = op.sig * (e - o);
+}
+__global__ void k_fly_rows(const FlyOp *ops, int H, int W) {
+  const FlyOp op = ops[blockIdx.z];
+  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+  if (x >= W || y >= H / 2) return;
+  const float e = op.E[(size_t)y * W + x], o = op.O[(size_t)y * W + x];
+  op.out[(size_t)y * W + x] = e + o;
+  op.out[(size_t)(H - 1 - y) * W + x] = op.sig * (e - o);
+}
+}  // namespace
+
+cudaError_t launch_fly_cols(const FlyOp *ops, int nb, int H, int W, cudaStream_t s) {
+  k_fly_cols<<<dim3((W / 2 + 127) / 128, H, nb), 128, 0, s>>>(ops, H, W);
+  return cudaGetLastError();
+}
+cudaError_t launch_fly_rows(const FlyOp *ops, int nb, int H, int W, cudaStream_t s) {
+  k_fly_rows<<<dim3((W + 127) / 128, H / 2, nb), 128, 0, s>>>(ops, H, W);
+  return cudaGetLastError();
 }
 
 int step_max_grid(int device) {

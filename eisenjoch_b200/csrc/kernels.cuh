@@ -107,11 +107,21 @@ struct FinalArgs {
   IterLog *log;
 };
 
+// C = A B with leading dimensions lda / ldb / ldc.  a_mir = +1 / -1 reads
+// A(r, k) as A(r, k) +/- A(r, a_full - 1 - k) (columns folded about the
+// middle of a_full); b_mir likewise folds B's rows about the middle of
+// b_full.  The spectral epilogue takes output row r as frequency
+// ky = 2 r + row_par (row_par < 0: ky = r) and, with col_split, column c as
+// kx = 2 c (c < N/2) or 2 (c - N/2) + 1 (even frequencies first).
 struct GemmOp {
   const float *A;
   const float *B;
   float *C;
   float *C2;
+  int lda, ldb, ldc;
+  int a_mir, a_full;
+  int b_mir, b_full;
+  int row_par, col_split;
 };
 
 struct SpectralArgs {
@@ -169,8 +179,20 @@ cudaError_t launch_density_final(const FinalArgs &a, int grid, cudaStream_t s);
 // same order, so the tile never changes the bits.
 cudaError_t launch_sgemm(const GemmOp *ops_dev, int nb, int M, int N, int K, cudaStream_t s, int tile = 0);
 // As above with the spectral epilogue: C = Ex_hat, C2 = Ey_hat.
-cudaError_t launch_sgemm_spectral(const GemmOp *ops_dev, int M, int N, int K,
+cudaError_t launch_sgemm_spectral(const GemmOp *ops_dev, int nb, int M, int N, int K,
                                   const SpectralArgs &sp, cudaStream_t s, int tile = 0);
+// The butterflies that complete a folded transform (see api.cu):
+// cols: out[r][x] = E[r][x] + O[r][x], out[r][W-1-x] = sig (E - O), x < W/2,
+//       E / O: [H][W/2]; nb products (blockIdx.z), each its own E, O, out, sig.
+// rows: out[y][x] = E[y][x] + O[y][x], out[H-1-y][x] = sig (E - O), y < H/2,
+//       E / O: [H/2][W].
+struct FlyOp {
+  const float *E, *O;
+  float *out;
+  float sig;
+};
+cudaError_t launch_fly_cols(const FlyOp *ops_dev, int nb, int H, int W, cudaStream_t s);
+cudaError_t launch_fly_rows(const FlyOp *ops_dev, int nb, int H, int W, cudaStream_t s);
 cudaError_t launch_step(const StepArgs &a, int grid, cudaStream_t s);
 // The same step as three ordinary launches (modes 2, 3, 4): no grid barrier,
 // safe beside long-running kernels of other streams.
