@@ -25,9 +25,12 @@ CASES = {
     # macros 2..8 and 2x2 sites per bin (the extension)
     "macro_256_bins128": E.SynthSpec(seed=5, num_cells=12000, num_nets=13200, num_pads=600, width=256, height=256,
                                      bins_x=128, bins_y=128, cluster_size=64, macro_fraction=0.05),
-    # odd sizes: non-power-of-two, non-square bin grid
+    # odd sizes: non-power-of-two, non-square bin grid (the unfolded FP32 transform)
     "odd_90x60": E.SynthSpec(seed=7, num_cells=1500, num_nets=1650, num_pads=100, width=90, height=60,
                              cluster_size=32),
+    # non-square grid with sides multiples of 8 (the folded FP32 transform, K not split)
+    "fold_96x48": E.SynthSpec(seed=9, num_cells=2000, num_nets=2200, num_pads=120, width=96, height=48,
+                              cluster_size=32),
 }
 
 
