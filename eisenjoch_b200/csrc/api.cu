@@ -902,6 +902,8 @@ void setup_tc(eplace_ctx *c) {
     m.b_lo = make_map(bl.p, nrows, k, kTcBN);
     m.b_hi32 = make_map(bh.p, nrows, k, 32);
     m.b_lo32 = make_map(bl.p, nrows, k, 32);
+    m.b_hi128 = nrows >= 128 ? make_map(bh.p, nrows, k, 128) : m.b_hi;  // used only when N % 128 == 0
+    m.b_lo128 = nrows >= 128 ? make_map(bl.p, nrows, k, 128) : m.b_lo;
     return m;
   };
   // GEMM1  T   = rho * B1          A = rho (H x W),  B^T = B1t (W x W)

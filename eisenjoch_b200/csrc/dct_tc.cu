@@ -182,8 +182,10 @@ __global__ void __launch_bounds__(128, 1)
       mbar_expect_tx(&full[s], S::STAGE_BYTES);
       tma_load_2d(st, &om.a_hi, kb * BK, m0, &full[s]);
       tma_load_2d(st + S::A_BYTES, &om.a_lo, kb * BK, m0, &full[s]);
-      tma_load_2d(st + 2 * S::A_BYTES, BN == 32 ? &om.b_hi32 : &om.b_hi, kb * BK, n0, &full[s]);
-      tma_load_2d(st + 2 * S::A_BYTES + S::B_BYTES, BN == 32 ? &om.b_lo32 : &om.b_lo, kb * BK, n0, &full[s]);
+      const CUtensorMap *bh = BN == 32 ? &om.b_hi32 : (BN == 128 ? &om.b_hi128 : &om.b_hi);
+      const CUtensorMap *bl = BN == 32 ? &om.b_lo32 : (BN == 128 ? &om.b_lo128 : &om.b_lo);
+      tma_load_2d(st + 2 * S::A_BYTES, bh, kb * BK, n0, &full[s]);
+      tma_load_2d(st + 2 * S::A_BYTES + S::B_BYTES, bl, kb * BK, n0, &full[s]);
     }
     s_issued = issued;
   } else if (threadIdx.x == 32) {
@@ -321,9 +323,10 @@ cudaError_t launch_cfg(const TcGemmMaps &maps, const TcGemmEpi &epi, int nbatch,
 
 // Tile shape by grid size (measured on 512^2 and 1024^2 bin grids): a grid
 // of 128 x 64 tiles that covers at most half the SMs takes 128 x 32 tiles
-// (twice the CTAs); one that would need a second wave takes two smaller
-// rings (2 stages, 97 KB) so that two CTAs share an SM and one's epilogue
-// overlaps the other's main loop; in between, 128 x 64 with a 4-deep ring.
+// (twice the CTAs); one that would need a second wave takes 128 x 128 tiles
+// with a 3-deep ring when those fit one wave, else two smaller rings (2
+// stages, 97 KB) so that two CTAs share an SM and one's epilogue overlaps
+// the other's main loop; in between, 128 x 64 with a 4-deep ring.
 // Each output sums its K steps in the same order whatever the tile.
 cudaError_t launch_tc_gemm(const TcGemmMaps &maps, const TcGemmEpi &epi, int nbatch, int M, int N, int K,
                            cudaStream_t s) {
@@ -331,6 +334,10 @@ cudaError_t launch_tc_gemm(const TcGemmMaps &maps, const TcGemmEpi &epi, int nba
   if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const long ctas = (long)(N / kTcBN) * (M / BM) * nbatch;
   if (2 * ctas <= sms) return launch_cfg<32, 4>(maps, epi, nbatch, M, N, K, s);
+  // A grid that 128 x 64 tiles would spread over two waves fits one wave of
+  // 128 x 128 tiles: each A tile is loaded half as often (the operand
+  // traffic from L2 sets these GEMMs' time), one CTA per SM.
+  if (ctas > sms && N % 128 == 0 && ctas / 2 <= sms) return launch_cfg<128, 3>(maps, epi, nbatch, M, N, K, s);
   if (ctas > sms) return launch_cfg<64, 2>(maps, epi, nbatch, M, N, K, s);
   return launch_cfg<64, 4>(maps, epi, nbatch, M, N, K, s);
 }

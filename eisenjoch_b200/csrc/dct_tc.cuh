@@ -10,9 +10,9 @@ namespace eplace {
 constexpr int kTcBN = 64;  // widest CTA tile N (M is 128); N must be a multiple of it
 
 // TMA maps of one GEMM's operands: A (M x K) and B^T (N x K), hi and lo; the
-// B maps twice, for the 64- and the 32-column tile.
+// B maps three times, for the 64-, 32- and 128-column tiles.
 struct TcOperandMaps {
-  CUtensorMap a_hi, a_lo, b_hi, b_lo, b_hi32, b_lo32;
+  CUtensorMap a_hi, a_lo, b_hi, b_lo, b_hi32, b_lo32, b_hi128, b_lo128;
 };
 
 // Up to two GEMMs of the same shape in one launch (blockIdx.z).
