@@ -52,8 +52,9 @@ def parse():
     ap.add_argument("--workload", default="electro_200k_1024")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-reps", type=int, default=30)
-    ap.add_argument("--dct", default="fp32", choices=["fp32", "bf16x3"],
-                    help="fp32: FP32 SIMT DCT GEMMs (the plain form); bf16x3: tcgen05 three-term split")
+    ap.add_argument("--dct", default="fp32", choices=["fp32", "bf16x3", "fft"],
+                    help="fp32: FP32 SIMT DCT GEMMs (the plain form); bf16x3: tcgen05 three-term split; "
+                         "fft: FP32 FFTs (power-of-two bin grids)")
     ap.add_argument("--profile-only", action="store_true",
                     help="only run the per-kernel stage profiler (for ncu captures)")
     ap.add_argument("--field-mode", default="potential_gradient", choices=["reference", "potential_gradient"],
@@ -652,8 +653,9 @@ def ours(args, dist):
     cfg = E.ElectroPlaceCfg(**w["cfg"])
     hbm, bf16, peak_src = peaks()
 
+    dct_modes = {"fp32": 0, "bf16x3": 1, "fft": 2}
     opts = E.RunOptions(field_mode=1 if args.field_mode == "potential_gradient" else 0,
-                        dct_mode=1 if args.dct == "bf16x3" else 0)
+                        dct_mode=dct_modes[args.dct])
     ctx = E.PlacementContext(nl, chip, device=dev)
     # --- per-kernel device times (CUDA events on the library's stream) ---
     stage_ms = ctx.profile_stages(cfg, reps=args.profile_reps, opts=opts)
@@ -662,7 +664,9 @@ def ours(args, dist):
             print(json.dumps({"workload": args.workload, "dct": args.dct, "stage_ms": stage_ms}), flush=True)
         ctx.close()
         return
-    alt_opts = E.RunOptions(field_mode=opts.field_mode, dct_mode=1 - opts.dct_mode)
+    # the other transform beside it: the FP32 GEMMs for the FFT and BF16x3
+    # forms, BF16x3 for the FP32 GEMMs
+    alt_opts = E.RunOptions(field_mode=opts.field_mode, dct_mode=1 if opts.dct_mode == 0 else 0)
     try:
         alt_stage_ms = ctx.profile_stages(cfg, reps=args.profile_reps, opts=alt_opts)
     except E.EplaceError as e:
@@ -767,7 +771,7 @@ def ours(args, dist):
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f32 (FP64 global reductions)" if args.dct == "fp32" else "bf16x3->f32 (FP64 global reductions)",
+        "dtype": "bf16x3->f32 (FP64 global reductions)" if args.dct == "bf16x3" else "f32 (FP64 global reductions)",
         "data": "synthetic (seeded generator, benchmark shapes); replica r uses seed + 7919 r",
         "config": {
             "workload": args.workload,
@@ -777,7 +781,8 @@ def ours(args, dist):
             "parallelism": "replicas x%d" % dist.world,
             "l2": "per-iteration working set is L2-resident at this size; no flush between jobs "
                   "(each job runs hundreds of iterations)",
-            "dct": {"fp32": "fp32 simt gemm", "bf16x3": "tcgen05 bf16 3-term split, fp32 accumulate"}[args.dct],
+            "dct": {"fp32": "fp32 simt gemm", "bf16x3": "tcgen05 bf16 3-term split, fp32 accumulate",
+                    "fft": "fp32 fft (one N-point FFT per line)"}[args.dct],
             "field_mode": args.field_mode + ("" if args.field_mode == "reference" else
                                              " (extension: the reference field does not spread cells; on this "
                                              "workload the reference FP64 loop reaches a non-finite gradient at iteration 50)"),

@@ -32,6 +32,7 @@ EPLACE_PENDING = 9
 
 EPLACE_DCT_FP32_SIMT = 0
 EPLACE_DCT_BF16X3_TC = 1
+EPLACE_DCT_FP32_FFT = 2
 
 EPLACE_FIELD_REFERENCE = 0
 EPLACE_FIELD_POTENTIAL_GRADIENT = 1

@@ -32,6 +32,7 @@
 
 #include "dct_tc.cuh"
 #include "eplace_internal.h"
+#include "fft.cuh"
 #include "init_place.cuh"
 #include "job.h"
 #include "kernels.cuh"
@@ -300,6 +301,10 @@ struct eplace_ctx {
   // the spatial index), the E / O products of GEMMs 3 and 4, their op
   // tables (12 per field mode) and butterflies (2 + 2 per field mode).
   bool fold = false;
+  // FFT form of the transforms (EPLACE_DCT_FP32_FFT on a power-of-two grid):
+  // set by every entry that launches the transform; twiddles of length W / H.
+  bool fft = false;
+  DBuf<float2> fft_twx, fft_tqx, fft_twy, fft_tqy;
   DBuf<float> hB1e, hB1o, hL2e, hL2o, hB3e, hB3o, hB5e, hB5o, hB3ge, hB3go, hL4e, hL4o, hL6e, hL6o, hL6ge, hL6go;
   DBuf<float> f3, f4;
   DBuf<GemmOp> hops;
@@ -339,6 +344,7 @@ struct eplace_ctx {
   int g_field = -1;
   int g_bx = -1, g_by = -1;  // bin grid gexec was instantiated for
   bool g_tc = false;
+  bool g_fft = false;
   float g_gamma = 0.f;
 
   // Tensor-core (BF16x3) transform: operands as hi/lo BF16 planes, all
@@ -678,6 +684,15 @@ void build_matrices(eplace_ctx *c) {
   }
   c->ops.ensure(12);
   c->ops.upload(ops, 12, s);
+  if (fft_supported(W, H)) {
+    std::vector<float2> tw(W / 2), tq(W), uw(H / 2), uq(H);
+    fft_tables_host(W, tw.data(), tq.data());
+    fft_tables_host(H, uw.data(), uq.data());
+    c->fft_twx.ensure(tw.size()); c->fft_twx.upload(tw.data(), tw.size(), s);
+    c->fft_tqx.ensure(tq.size()); c->fft_tqx.upload(tq.data(), tq.size(), s);
+    c->fft_twy.ensure(uw.size()); c->fft_twy.upload(uw.data(), uw.size(), s);
+    c->fft_tqy.ensure(uq.size()); c->fft_tqy.upload(uq.data(), uq.size(), s);
+  }
   c->fold = fold_ok(W, H);
   if (c->fold) {
     const int hw = W / 2, hh = H / 2;
@@ -977,6 +992,49 @@ void launch_field_gemm(eplace_ctx *c, int g, float *phi, int field_mode, bool tc
     }
     return;
   }
+  if (c->fft) {
+    FftStageArgs a{};
+    a.W = W;
+    a.H = H;
+    a.tx = FftTables{c->fft_twx.p, c->fft_tqx.p};
+    a.ty = FftTables{c->fft_twy.p, c->fft_tqy.p};
+    const int sx = fm ? FFT_SG : FFT_S3;  // the x field's transform along x, the y field's along y
+    switch (g) {
+      case 0:
+        a.in_a = c->rho.p;
+        a.out_a = c->T.p;
+        break;
+      case 1:
+        a.in_a = c->T.p;
+        a.out_a = c->Exh.p;
+        a.out_b = c->Eyh.p;
+        a.wx = c->wx.p;
+        a.gx2 = c->gx2.p;
+        a.wy = c->wy.p;
+        a.gy2 = c->gy2.p;
+        a.scale = (float)(4.0 / ((double)W * H));
+        a.phi = phi;
+        break;
+      case 2:
+        a.in_a = c->Exh.p;
+        a.in_b = c->Eyh.p;
+        a.out_a = c->U.p;
+        a.out_b = c->V.p;
+        a.kind_a = sx;
+        a.kind_b = FFT_C3;
+        break;
+      default:
+        a.in_a = c->U.p;
+        a.in_b = c->V.p;
+        a.out_a = c->Ex.p;
+        a.out_b = c->Ey.p;
+        a.kind_a = FFT_C3;
+        a.kind_b = sx;
+        break;
+    }
+    CK(launch_fft_stage(g, a, c->stream));
+    return;
+  }
   if (c->fold) {
     const GemmOp *h = c->hops.p + 12 * fm;
     const FlyOp *f = c->fops.p + 4 * fm;
@@ -1108,7 +1166,7 @@ void autotune_launches(eplace_ctx *c, float gamma, int field_mode, bool tc) {
         v.sc = m;
       }
     }
-    if (!tc) {
+    if (!tc && !c->fft) {
       for (int g = 0; g < 4; ++g) {
         float bt = 1e30f;
         for (int tile : {64, 32}) {
@@ -1560,7 +1618,7 @@ void eplace_ctx_destroy(eplace_ctx *ctx) {
 
 // Validates the run options against this context.
 static eplace_status check_modes(eplace_ctx *c, const eplace_opts &o) {
-  if (o.dct_mode != EPLACE_DCT_FP32_SIMT && o.dct_mode != EPLACE_DCT_BF16X3_TC) {
+  if (o.dct_mode != EPLACE_DCT_FP32_SIMT && o.dct_mode != EPLACE_DCT_BF16X3_TC && o.dct_mode != EPLACE_DCT_FP32_FFT) {
     set_err(c, "unknown dct_mode");
     return EPLACE_ERR_INVALID;
   }
@@ -1759,6 +1817,7 @@ struct JobState {
     eplace_status mst = check_modes(c, opts);
     if (mst != EPLACE_OK) return final_st = mst;
     tc = opts.dct_mode == EPLACE_DCT_BF16X3_TC;
+    c->fft = opts.dct_mode == EPLACE_DCT_FP32_FFT && fft_supported(hp.BX, hp.BY);
     gpu_legal = opts.legal_mode == EPLACE_LEGAL_GPU && legalize_supported(hp.W, hp.H);
     if (!res->bel_tile && hp.N) return final_st = EPLACE_ERR_INVALID;
     std::string msg;
@@ -1869,7 +1928,7 @@ struct JobState {
       // thread pumping the loop only launches it.
       use_graph = opts.use_graphs != 0 && interval > 1;
       if (c->gexec && (c->g_epoch != c->buf_epoch || c->g_interval != interval || c->g_field != opts.field_mode ||
-                       c->g_tc != tc || c->g_gamma != gamma))
+                       c->g_tc != tc || c->g_fft != c->fft || c->g_gamma != gamma))
         c->g_valid = false;
       if (use_graph && interval < max_iters) ensure_graph();
       converged_chunk = chunks.size();
@@ -1916,7 +1975,7 @@ struct JobState {
     // those decide which transform kernels run and how they launch (a
     // split-K GEMM is a cluster launch, whose cluster shape an in-place
     // update does not carry), so any other grid gets a new instantiation.
-    if (c->gexec && (c->g_bx != c->hp.BX || c->g_by != c->hp.BY || c->g_tc != tc)) {
+    if (c->gexec && (c->g_bx != c->hp.BX || c->g_by != c->hp.BY || c->g_tc != tc || c->g_fft != c->fft)) {
       cudaGraphExecDestroy(c->gexec);
       c->gexec = nullptr;
     }
@@ -1948,6 +2007,7 @@ struct JobState {
     c->g_interval = interval;
     c->g_field = opts.field_mode;
     c->g_tc = tc;
+    c->g_fft = c->fft;
     c->g_gamma = gamma;
     c->g_bx = c->hp.BX;
     c->g_by = c->hp.BY;
@@ -2229,7 +2289,7 @@ struct JobState {
       float ms = 0.f;
       CK(cudaEventElapsedTime(&ms, ev0, ev1));
       res->gpu_seconds = ms * 1e-3;
-      res->gpu_launches = (uint64_t)(kLaunchesPerIter + (c->split_step ? 2 : 0) + (c->fold && !tc ? 2 : 0)) *
+      res->gpu_launches = (uint64_t)(kLaunchesPerIter + (c->split_step ? 2 : 0) + (c->fold && !tc && !c->fft ? 2 : 0)) *
                               launched_iters +
                           (gpu_legal ? 2 * cps.size() : 0) + (uint64_t)ip_launches;
       res->iters = (uint32_t)iters_done;
@@ -2601,6 +2661,7 @@ eplace_status eplace_profile_stages(eplace_ctx *c, const eplace_cfg *cfg, const 
   const bool tc = opts.dct_mode == EPLACE_DCT_BF16X3_TC;
   const HostProblem &hp = c->hp;
   if (hp.N == 0) return EPLACE_ERR_INVALID;
+  c->fft = opts.dct_mode == EPLACE_DCT_FP32_FFT && fft_supported(hp.BX, hp.BY);
   std::vector<cudaEvent_t> ev(9, nullptr);
   eplace_status st = EPLACE_OK;
   try {
@@ -2764,6 +2825,7 @@ eplace_status eplace_stage_field(eplace_ctx *c, const double *density, int32_t d
   eplace_status mst = check_modes(c, o);
   if (mst != EPLACE_OK) return mst;
   const bool tc = dct_mode == EPLACE_DCT_BF16X3_TC;
+  c->fft = dct_mode == EPLACE_DCT_FP32_FFT && fft_supported(c->hp.BX, c->hp.BY);
   try {
     CK(cudaSetDevice(c->device));
     const size_t nb = (size_t)c->hp.BX * c->hp.BY;

@@ -66,7 +66,9 @@ void eplace_cfg_default(eplace_cfg *cfg);
 /* Build-only knobs with no reference counterpart. */
 typedef enum {
   EPLACE_DCT_FP32_SIMT = 0,    /* FP32 DCT-matrix GEMMs on the CUDA cores */
-  EPLACE_DCT_BF16X3_TC = 1     /* BF16 three-term split GEMMs on tcgen05, FP32 accumulate */
+  EPLACE_DCT_BF16X3_TC = 1,    /* BF16 three-term split GEMMs on tcgen05, FP32 accumulate */
+  EPLACE_DCT_FP32_FFT = 2      /* FP32 FFTs (one N-point FFT per line); power-of-two bin grids of
+                                  16 .. 1024 per axis, other grids take the FP32 GEMMs */
 } eplace_dct_mode;
 
 /* Field formula.  EPLACE_FIELD_REFERENCE reproduces density.rs:149-163

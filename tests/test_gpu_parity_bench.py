@@ -41,6 +41,7 @@ pytestmark = pytest.mark.gpu
 HERE = os.path.dirname(os.path.abspath(__file__))
 TC = E._abi.EPLACE_DCT_BF16X3_TC
 SIMT = E._abi.EPLACE_DCT_FP32_SIMT
+FFT = E._abi.EPLACE_DCT_FP32_FFT
 
 OVERLAP_TOL = 2e-3      # checkpoint overlap, absolute
 HPWL_TOL = 0.005        # legalised HPWL, relative
@@ -99,10 +100,10 @@ def test_density_bench(bench_case, clustered):
     assert abs(ov - orc.overlap(rd)) <= 1e-6
 
 
-@pytest.mark.parametrize("dct_mode", [SIMT, TC])
+@pytest.mark.parametrize("dct_mode", [SIMT, TC, FFT])
 @pytest.mark.parametrize("field_mode", [0, 1])
 def test_field_bench(bench_case, dct_mode, field_mode):
-    """Field and potential spectrum of a clustered density map, both
+    """Field and potential spectrum of a clustered density map, all three
     transforms, both field formulas."""
     name, nl, chip, ctx, orc = bench_case
     x, y = positions(nl, chip, 43, True)
@@ -198,16 +199,17 @@ def compare_job(r, g, cfg, orc, chip, label):
     return d_ov, d_hp
 
 
-def test_full_run_200k_matches_oracle():
-    """The benchmark's job (potential-gradient field, FP32 transform) against
-    the oracle's 200k run: convergence, exit iteration, final HPWL and the
-    overlap / HPWL trajectory over all checkpoints."""
+@pytest.mark.parametrize("dct_mode", [SIMT, FFT])
+def test_full_run_200k_matches_oracle(dct_mode):
+    """The benchmark's job (potential-gradient field, FP32 GEMM and FFT
+    transforms) against the oracle's 200k run: convergence, exit iteration,
+    final HPWL and the overlap / HPWL trajectory over all checkpoints."""
     nl, chip, cfg = E.workload("electro_200k_1024")
-    r = E.place_electro(nl, chip, cfg, E.RunOptions(field_mode=1, dct_mode=SIMT))
-    compare_job(r, golden("electro_200k_1024"), cfg, Oracle(nl, chip), chip, "200k fp32")
+    r = E.place_electro(nl, chip, cfg, E.RunOptions(field_mode=1, dct_mode=dct_mode))
+    compare_job(r, golden("electro_200k_1024"), cfg, Oracle(nl, chip), chip, "200k dct %d" % dct_mode)
 
 
-@pytest.mark.parametrize("dct_mode", [SIMT, TC])
+@pytest.mark.parametrize("dct_mode", [SIMT, TC, FFT])
 def test_full_run_800k_precision_forms(dct_mode):
     """The precision form: the 800k job with the BF16x3 tensor-core
     transform and with the FP32 transform, each against the FP64 oracle's
