@@ -954,7 +954,9 @@ void launch_final_stage(eplace_ctx *c, double *dens_out, bool tc = false) {
 // One of the four GEMM launches of a field solve (density.rs:96-166):
 //   0: T = rho * B1 (row DCT-II)          1: Coef = L2 * T + spectral epilogue
 //   2: U = Ex^ * B3, V = Ey^ * B5          3: Ex = L4 * U, Ey = L6 * V
-void launch_field_gemm(eplace_ctx *c, int g, float *phi, int field_mode, bool tc) {
+// from_dens (FFT form, stage 0): read the fixed-point density map itself,
+// with the finalise (charge, map clear, overlap) fused into the stage.
+void launch_field_gemm(eplace_ctx *c, int g, float *phi, int field_mode, bool tc, bool from_dens = false) {
   const int W = c->hp.BX, H = c->hp.BY;
   const int fm = field_mode == EPLACE_FIELD_POTENTIAL_GRADIENT ? 1 : 0;
   if (tc) {
@@ -1003,6 +1005,15 @@ void launch_field_gemm(eplace_ctx *c, int g, float *phi, int field_mode, bool tc
       case 0:
         a.in_a = c->rho.p;
         a.out_a = c->T.p;
+        if (from_dens) {
+          a.dens = c->dens.p;
+          a.cap = (double)c->hp.sx * c->hp.sy;
+          a.c0 = c->total_area / ((double)W * H);
+          a.part = c->part.p;
+          a.ticket = c->bar.p + 2;
+          a.sc = c->sc.p;
+          a.log = c->log.p;
+        }
         break;
       case 1:
         a.in_a = c->T.p;
@@ -1078,9 +1089,12 @@ void launch_field_gemm(eplace_ctx *c, int g, float *phi, int field_mode, bool tc
   }
 }
 
-void launch_field_stage(eplace_ctx *c, float *phi, int field_mode, bool tc = false) {
-  for (int g = 0; g < 4; ++g) launch_field_gemm(c, g, phi, field_mode, tc);
+void launch_field_stage(eplace_ctx *c, float *phi, int field_mode, bool tc = false, bool from_dens = false) {
+  for (int g = 0; g < 4; ++g) launch_field_gemm(c, g, phi, field_mode, tc, from_dens && g == 0);
 }
+
+// The FFT form takes the density finalise into its first stage.
+bool final_fused(const eplace_ctx *c, bool tc) { return c->fft && !tc; }
 
 // --- launch-shape autotuner ------------------------------------------------
 // Picks, by timing on the context's stream, the grid caps of the WA and
@@ -1251,13 +1265,14 @@ void launch_iteration(eplace_ctx *c, float gamma, int field_mode, bool tc) {
   launch_wa_stage(c, gamma, c->side);
   CK(cudaEventRecord(c->ev_join, c->side));
   launch_scatter_stage(c);
-  launch_final_stage(c, nullptr, tc);
-  launch_field_stage(c, nullptr, field_mode, tc);
+  const bool fuse = final_fused(c, tc);
+  if (!fuse) launch_final_stage(c, nullptr, tc);
+  launch_field_stage(c, nullptr, field_mode, tc, fuse);
   CK(cudaStreamWaitEvent(c->stream, c->ev_join, 0));
   launch_step_stage(c);
 }
 
-constexpr int kLaunchesPerIter = 8;  // with the cooperative step; +2 with the split step
+constexpr int kLaunchesPerIter = 8;  // with the cooperative step; +2 with the split step, -1 with the FFT form
 
 void upload_momentum(eplace_ctx *c, uint64_t iters) {
   AllocOn on_stream(c->stream);
@@ -1556,7 +1571,7 @@ void eplace_cfg_default(eplace_cfg *c) {
 void eplace_opts_default(eplace_opts *o) {
   if (!o) return;
   std::memset(o, 0, sizeof(*o));
-  o->dct_mode = EPLACE_DCT_FP32_SIMT;
+  o->dct_mode = EPLACE_DCT_FP32_FFT;
   o->legal_threads = 0;
   o->use_graphs = 1;
   o->verbose = 0;
@@ -2289,7 +2304,8 @@ struct JobState {
       float ms = 0.f;
       CK(cudaEventElapsedTime(&ms, ev0, ev1));
       res->gpu_seconds = ms * 1e-3;
-      res->gpu_launches = (uint64_t)(kLaunchesPerIter + (c->split_step ? 2 : 0) + (c->fold && !tc && !c->fft ? 2 : 0)) *
+      res->gpu_launches = (uint64_t)(kLaunchesPerIter + (c->split_step ? 2 : 0) + (c->fold && !tc && !c->fft ? 2 : 0) -
+                                         (final_fused(c, tc) ? 1 : 0)) *
                               launched_iters +
                           (gpu_legal ? 2 * cps.size() : 0) + (uint64_t)ip_launches;
       res->iters = (uint32_t)iters_done;
@@ -2694,10 +2710,11 @@ eplace_status eplace_profile_stages(eplace_ctx *c, const eplace_cfg *cfg, const 
       rec(ev[1]);
       launch_scatter_stage(c);
       rec(ev[2]);
-      launch_final_stage(c, nullptr, tc);
+      const bool fuse = final_fused(c, tc);  // then the finalise is timed with the first transform stage
+      if (!fuse) launch_final_stage(c, nullptr, tc);
       rec(ev[3]);
       for (int g = 0; g < 4; ++g) {
-        launch_field_gemm(c, g, nullptr, opts.field_mode, tc);
+        launch_field_gemm(c, g, nullptr, opts.field_mode, tc, fuse && g == 0);
         rec(ev[4 + g]);
       }
       launch_step_stage(c);

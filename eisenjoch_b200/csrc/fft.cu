@@ -79,6 +79,30 @@ __device__ __forceinline__ void fft_core(float2 *s, int logN, int nf, const floa
   __syncthreads();
 }
 
+// Sum of v over the CTA in a fixed order (a shuffle tree per warp, then the
+// warps in order); the result is valid in thread 0.  red: [2 * warps].
+__device__ __forceinline__ void block_sum2(double (&v)[2], double *red) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    v[0] += __shfl_down_sync(0xffffffffu, v[0], o);
+    v[1] += __shfl_down_sync(0xffffffffu, v[1], o);
+  }
+  const int w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) {
+    red[2 * w] = v[0];
+    red[2 * w + 1] = v[1];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    v[0] = v[1] = 0.0;
+    for (int k = 0; k < nw; ++k) {
+      v[0] += red[2 * k];
+      v[1] += red[2 * k + 1];
+    }
+  }
+}
+
 // Index in the line of X'[k] for a stage-2/3 kind (-1: the value is 0).
 __device__ __forceinline__ int pre_index(int kind, int k, int N) {
   if (kind == FFT_C3) return k;
@@ -156,7 +180,42 @@ __global__ void __launch_bounds__(kFftThreads) k_fft(const FftStageArgs a) {
   // v[N-1-m] = x[2m+1].
   for (int j = threadIdx.x; j < N / 2; j += kFftThreads) tw[j] = __ldg(tb.tw + j);
   for (int j = threadIdx.x; j < N; j += kFftThreads) tq[j] = __ldg(tb.tq + j);
-  {
+  __shared__ double red[2 * (kFftThreads / 32)];
+  double ov[2] = {0.0, 0.0};  // sum d, sum max(d - cap, 0) (stage 0 from the map)
+  if (STAGE == 0 && a.dens) {
+    for (int v0 = 0; v0 < nvec; v0 += kBatch * kFftThreads) {
+      ulonglong2 q0[kBatch], q1[kBatch];
+#pragma unroll
+      for (int u = 0; u < kBatch; ++u) {
+        const int v = v0 + u * kFftThreads + threadIdx.x;
+        int l, n;
+        const size_t g = vec_at(v < nvec ? v : 0, l, n);
+        const ulonglong2 *dp = reinterpret_cast<const ulonglong2 *>(a.dens + g);
+        q0[u] = v < nvec ? dp[0] : make_ulonglong2(0ull, 0ull);
+        q1[u] = v < nvec ? dp[1] : make_ulonglong2(0ull, 0ull);
+      }
+#pragma unroll
+      for (int u = 0; u < kBatch; ++u) {
+        const int v = v0 + u * kFftThreads + threadIdx.x;
+        if (v >= nvec) break;
+        int l, n;
+        const size_t g = vec_at(v, l, n);
+        ulonglong2 *dp = reinterpret_cast<ulonglong2 *>(a.dens + g);
+        dp[0] = make_ulonglong2(0ull, 0ull);
+        dp[1] = make_ulonglong2(0ull, 0ull);
+        const unsigned long long qq[4] = {q0[u].x, q0[u].y, q1[u].x, q1[u].y};
+        float *sf = reinterpret_cast<float *>(s) + (l & 1);
+        const int b0 = (l >> 1) << logN;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          const double d = (double)(long long)qq[c] * (1.0 / 4294967296.0);
+          ov[0] += d;
+          ov[1] += fmax(d - a.cap, 0.0);
+          sf[2 * pd(b0 + bitrev(vpos(n + c, N), logN))] = (float)(d - a.c0);
+        }
+      }
+    }
+  } else {
     const float *src[2] = {a.in_a, a.in_b};
     for (int v0 = 0; v0 < nvec; v0 += kBatch * kFftThreads) {
       float4 q[kArrays][kBatch];
@@ -286,6 +345,32 @@ __global__ void __launch_bounds__(kFftThreads) k_fft(const FftStageArgs a) {
     *reinterpret_cast<float4 *>(a.out_a + g) = make_float4(o[0][0], o[0][1], o[0][2], o[0][3]);
     if (STAGE >= 1) *reinterpret_cast<float4 *>(a.out_b + g) = make_float4(o[1][0], o[1][1], o[1][2], o[1][3]);
     if (STAGE == 1 && a.phi) *reinterpret_cast<float4 *>(a.phi + g) = make_float4(o[2][0], o[2][1], o[2][2], o[2][3]);
+  }
+  if (STAGE == 0 && a.dens) {
+    // the overlap: CTA partials, then the last CTA sums them in CTA order
+    __shared__ bool last;
+    block_sum2(ov, red);
+    if (threadIdx.x == 0) {
+      a.part[2 * blockIdx.x] = ov[0];
+      a.part[2 * blockIdx.x + 1] = ov[1];
+      __threadfence();
+      last = atomicAdd(a.ticket, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    double t[2] = {0.0, 0.0};
+    for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
+      t[0] += __ldcg(a.part + 2 * b);
+      t[1] += __ldcg(a.part + 2 * b + 1);
+    }
+    block_sum2(t, red);
+    if (threadIdx.x == 0) {
+      const double ovl = (t[0] < 1e-30) ? 0.0 : t[1] / t[0];  // compute_overlap
+      a.sc->overlap = ovl;
+      a.log[a.sc->iter].overlap = ovl;
+      *a.ticket = 0u;
+    }
   }
 }
 

@@ -29,6 +29,8 @@
 
 #include <cuda_runtime.h>
 
+#include "kernels.cuh"
+
 namespace eplace {
 
 // Twiddles of one transform length N (host-computed in FP64, stored FP32).
@@ -50,6 +52,18 @@ struct FftStageArgs {
   const float *wx, *gx2, *wy, *gy2;
   float scale;            // 4 / (W H)
   float *phi;             // optional [H][W] potential spectrum
+  // Stage 0 straight from the fixed-point density map (the finalise fused
+  // in): with dens set, the stage reads the map instead of in_a, forms
+  // rho = d - c0, clears the map for the next iteration, and sums the
+  // overlap (density.rs:79-86: sum d and sum max(d - cap, 0)) into part[]
+  // per CTA; the last CTA to finish writes sc->overlap and the iteration's
+  // log entry.
+  unsigned long long *dens;
+  double cap, c0;
+  double *part;           // [2 * CTAs of stage 0]
+  unsigned *ticket;
+  DevScalars *sc;
+  IterLog *log;
 };
 
 bool fft_supported(int W, int H);

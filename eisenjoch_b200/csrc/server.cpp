@@ -191,7 +191,7 @@ struct eplace_server {
       // The tensor-core transform needs bins_y % 128 == 0 and bins_x % 64 == 0;
       // smaller grids of a mixed stream run the FP32 transform.
       eplace_opts jo = cfg.opts;
-      if (jo.dct_mode == EPLACE_DCT_BF16X3_TC && !problem_tc_supported(r->hp)) jo.dct_mode = EPLACE_DCT_FP32_SIMT;
+      if (jo.dct_mode == EPLACE_DCT_BF16X3_TC && !problem_tc_supported(r->hp)) jo.dct_mode = EPLACE_DCT_FP32_FFT;
       eplace_status st = EPLACE_OK;
       eplace_ctx *c = take_context(*r, &st);
       if (!c) {

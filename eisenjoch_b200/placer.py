@@ -55,7 +55,7 @@ class ElectroPlaceCfg:
 class RunOptions:
     """Build-only knobs with no reference counterpart (eplace_opts)."""
 
-    dct_mode: int = _abi.EPLACE_DCT_FP32_SIMT
+    dct_mode: int = _abi.EPLACE_DCT_FP32_FFT
     legal_threads: int = 0
     use_graphs: bool = True
     verbose: int = 0
@@ -485,7 +485,7 @@ class PlacementContext:
                                                    _abi.ptr(d, ctypes.c_double), ctypes.byref(ov)))
         return d, ov.value
 
-    def field(self, density, dct_mode=_abi.EPLACE_DCT_FP32_SIMT, want_phi=False, field_mode=_abi.EPLACE_FIELD_REFERENCE):
+    def field(self, density, dct_mode=_abi.EPLACE_DCT_FP32_FFT, want_phi=False, field_mode=_abi.EPLACE_FIELD_REFERENCE):
         by, bx = self.bins
         d = _abi.f64(density).reshape(by, bx)
         ex, ey = np.zeros((by, bx), np.float32), np.zeros((by, bx), np.float32)

@@ -100,7 +100,7 @@ typedef enum {
 } eplace_legal_mode;
 
 typedef struct {
-  int32_t dct_mode;            /* eplace_dct_mode; default EPLACE_DCT_FP32_SIMT */
+  int32_t dct_mode;            /* eplace_dct_mode; default EPLACE_DCT_FP32_FFT */
   int32_t legal_threads;       /* host legaliser threads; 0 = hardware concurrency */
   int32_t use_graphs;          /* capture each legalise interval as a CUDA graph; default 1 */
   int32_t verbose;             /* 1 = print the reference's per-legalisation trajectory line */

@@ -113,12 +113,15 @@ def test_density_and_overlap(case, clustered):
     assert abs(d.sum() - rd.sum()) <= 1e-5 * rd.sum()
 
 
+@pytest.mark.parametrize("dct_mode", [E._abi.EPLACE_DCT_FP32_SIMT, E._abi.EPLACE_DCT_FP32_FFT])
 @pytest.mark.parametrize("clustered", [False, True])
-def test_field(case, clustered):
+def test_field(case, clustered, dct_mode):
+    """Both FP32 transforms (the FFT form falls back to the GEMMs on grids
+    that are not powers of two)."""
     name, nl, chip, ctx, orc = case
     x, y = positions(nl, chip, 14, clustered)
     rd = orc.density(x, y)
-    ex, ey, phi = ctx.field(rd, want_phi=True)
+    ex, ey, phi = ctx.field(rd, want_phi=True, dct_mode=dct_mode)
     rex, rey, rphi = orc.field(rd, 1.0, want_phi=True)
     assert rel_err(ex, rex) <= 1e-4, name
     assert rel_err(ey, rey) <= 1e-4, name
