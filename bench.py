@@ -73,6 +73,9 @@ def parse():
     ap.add_argument("--served-rate-2", type=float, default=0.0,
                     help="a second offered rate, e.g. 100 jobs/s, within the engine's capacity (0: skip)")
     ap.add_argument("--max-jobs", type=int, default=16, help="jobs the engine keeps on the GPU at once")
+    ap.add_argument("--engine-dct", default="bf16x3", choices=["bf16x3", "fft"],
+                    help="transform of the engine's jobs: bf16x3 (the mixed-precision form; FP32 FFT where the "
+                         "grid is below 128 bins) or fft")
     return ap.parse_args()
 
 
@@ -439,12 +442,15 @@ def _agree(a, b):
             "max_overflow": max(x.overlap for x in a)}
 
 
+ENGINE_DCT = {"bf16x3": "bf16x3 tcgen05 (fp32 fft where bins < 128)", "fft": "fp32 fft"}
+
+
 def batched_arm(args, dist, E, cfg):
     """64 instances, 2k..200k cells (log-uniform), mixed precision (BF16x3
     tensor-core transform where the bin grid allows it) through the engine,
     against the plain FP32 form one job at a time on the same jobs."""
     jobs = _mixed_jobs(E, E.batched_specs(args.batched_jobs), dist.rank)
-    eng_opts = E.RunOptions(field_mode=1, dct_mode=1)
+    eng_opts = E.RunOptions(field_mode=1, dct_mode=1 if args.engine_dct == "bf16x3" else 2)
     plain_opts = E.RunOptions(field_mode=1, dct_mode=2)
     with E.JobServer(device=dist.local, max_jobs=args.max_jobs, opts=eng_opts) as srv:
         # Warm-up: one untimed pass over the same jobs (contexts created and
@@ -473,7 +479,7 @@ def batched_arm(args, dist, E, cfg):
         "cells_total": int(sum(cells)), "cells_min": int(min(cells)), "cells_max": int(max(cells)),
         "engine": {"jobs_per_s": n / t_eng, "seconds": t_eng, "max_jobs": args.max_jobs,
                    "passes_jobs_per_s": [n / t for t in eng_passes],
-                   "dct": "bf16x3 tcgen05 (fp32 fft where bins < 128)", "contexts": stats["contexts"],
+                   "dct": ENGINE_DCT[args.engine_dct], "contexts": stats["contexts"],
                    "device_bytes": stats["device_bytes"],
                    "scheduler_s": {k: round(stats[k + "_seconds"], 3) for k in ("admit", "pump", "idle")}},
         "plain_fp32_reused_ctx": {"jobs_per_s": n / t_reuse, "seconds": t_reuse, "dct": "fp32 fft",
@@ -494,7 +500,7 @@ def served_arm(args, dist, E, cfg, rate):
     same stream one job at a time in arrival order."""
     specs, arrivals = E.served_stream(args.served_jobs, rate)
     jobs = _mixed_jobs(E, specs, dist.rank)
-    eng_opts = E.RunOptions(field_mode=1, dct_mode=1)
+    eng_opts = E.RunOptions(field_mode=1, dct_mode=1 if args.engine_dct == "bf16x3" else 2)
     plain_opts = E.RunOptions(field_mode=1, dct_mode=2)
     with E.JobServer(device=dist.local, max_jobs=args.max_jobs, opts=eng_opts) as srv:
         _engine(E, srv, jobs[: args.max_jobs], cfg)  # warm-up
@@ -514,7 +520,7 @@ def served_arm(args, dist, E, cfg, rate):
         "sample": ("the whole 2,000-job stream" if len(jobs) == 2000 else
                    "first %d jobs of the 2,000-job stream" % len(jobs)) + " (seeds 100000+j, arrivals seed 7)",
         "engine": {"jobs_per_s": n / t_eng, "p50_latency_s": pct(lat_eng, 50), "p99_latency_s": pct(lat_eng, 99),
-                   "max_jobs": args.max_jobs, "dct": "bf16x3 tcgen05 (fp32 fft where bins < 128)"},
+                   "max_jobs": args.max_jobs, "dct": ENGINE_DCT[args.engine_dct]},
         "plain_fp32": {"jobs_per_s": n / t_pl, "p50_latency_s": pct(lat_pl, 50), "p99_latency_s": pct(lat_pl, 99),
                        "dct": "fp32 fft"},
         "throughput_vs_plain": t_pl / t_eng,

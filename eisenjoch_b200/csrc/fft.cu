@@ -397,22 +397,27 @@ cudaError_t launch_fft_stage(int stage, const FftStageArgs &a, cudaStream_t s) {
   const FftGeom g = fft_geom(stage, a.W, a.H);
   const int grid = (g.L + g.lines - 1) / g.lines;
   const size_t smem = fft_smem(stage, g);
+  // The shared-memory limit is raised to the stage's largest need (a
+  // 1024 x 1024 grid) every time: the same value from every thread, so
+  // contexts launching from several host threads never lower it under one
+  // another's launch.
+  const int cap = (int)fft_smem(stage, fft_geom(stage, 1024, 1024));
   cudaError_t e = cudaSuccess;
   switch (stage) {
     case 0:
-      e = cudaFuncSetAttribute(k_fft<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      e = cudaFuncSetAttribute(k_fft<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, cap);
       if (e == cudaSuccess) k_fft<0><<<grid, kFftThreads, smem, s>>>(a);
       break;
     case 1:
-      e = cudaFuncSetAttribute(k_fft<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      e = cudaFuncSetAttribute(k_fft<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, cap);
       if (e == cudaSuccess) k_fft<1><<<grid, kFftThreads, smem, s>>>(a);
       break;
     case 2:
-      e = cudaFuncSetAttribute(k_fft<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      e = cudaFuncSetAttribute(k_fft<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, cap);
       if (e == cudaSuccess) k_fft<2><<<grid, kFftThreads, smem, s>>>(a);
       break;
     default:
-      e = cudaFuncSetAttribute(k_fft<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      e = cudaFuncSetAttribute(k_fft<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, cap);
       if (e == cudaSuccess) k_fft<3><<<grid, kFftThreads, smem, s>>>(a);
       break;
   }
