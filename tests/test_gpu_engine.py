@@ -22,6 +22,11 @@ SPECS = [
     E.SynthSpec(seed=1005, num_cells=1200, num_nets=1320, num_pads=80, width=48, height=48),
     E.SynthSpec(seed=1006, num_cells=6000, num_nets=6600, num_pads=250, width=128, height=128, bins_x=64,
                 bins_y=64),
+    # FFT transforms of different lengths launched side by side
+    E.SynthSpec(seed=1007, num_cells=12000, num_nets=13200, num_pads=400, width=256, height=256, bins_x=128,
+                bins_y=128, cluster_size=64),
+    E.SynthSpec(seed=1008, num_cells=30000, num_nets=33000, num_pads=600, width=512, height=512, bins_x=256,
+                bins_y=256, cluster_size=64, macro_fraction=0.05),
 ]
 CFG = E.ElectroPlaceCfg(max_iters=120)
 OPTS = E.RunOptions(field_mode=1)
