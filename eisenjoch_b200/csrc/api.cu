@@ -1000,7 +1000,7 @@ void launch_field_gemm(eplace_ctx *c, int g, float *phi, int field_mode, bool tc
     a.H = H;
     a.tx = FftTables{c->fft_twx.p, c->fft_tqx.p};
     a.ty = FftTables{c->fft_twy.p, c->fft_tqy.p};
-    const int sx = fm ? FFT_SG : FFT_S3;  // the x field's transform along x, the y field's along y
+    const int sn = fm ? FFT_SG : FFT_S3;  // Ex's transform along x, Ey's along y
     switch (g) {
       case 0:
         a.in_a = c->rho.p;
@@ -1015,10 +1015,12 @@ void launch_field_gemm(eplace_ctx *c, int g, float *phi, int field_mode, bool tc
           a.log = c->log.p;
         }
         break;
-      case 1:
+      case 1:  // forward along y, spectral, then back along y: U, V
         a.in_a = c->T.p;
-        a.out_a = c->Exh.p;
-        a.out_b = c->Eyh.p;
+        a.out_a = c->U.p;
+        a.out_b = c->V.p;
+        a.kind_a = FFT_C3;
+        a.kind_b = sn;
         a.wx = c->wx.p;
         a.gx2 = c->gx2.p;
         a.wy = c->wy.p;
@@ -1027,21 +1029,15 @@ void launch_field_gemm(eplace_ctx *c, int g, float *phi, int field_mode, bool tc
         a.phi = phi;
         break;
       case 2:
-        a.in_a = c->Exh.p;
-        a.in_b = c->Eyh.p;
-        a.out_a = c->U.p;
-        a.out_b = c->V.p;
-        a.kind_a = sx;
-        a.kind_b = FFT_C3;
-        break;
-      default:
         a.in_a = c->U.p;
         a.in_b = c->V.p;
         a.out_a = c->Ex.p;
         a.out_b = c->Ey.p;
-        a.kind_a = FFT_C3;
-        a.kind_b = sx;
+        a.kind_a = sn;
+        a.kind_b = FFT_C3;
         break;
+      default:
+        return;  // three stages: the fourth slot launches nothing
     }
     CK(launch_fft_stage(g, a, c->stream));
     return;
@@ -1272,7 +1268,7 @@ void launch_iteration(eplace_ctx *c, float gamma, int field_mode, bool tc) {
   launch_step_stage(c);
 }
 
-constexpr int kLaunchesPerIter = 8;  // with the cooperative step; +2 with the split step, -1 with the FFT form
+constexpr int kLaunchesPerIter = 8;  // with the cooperative step; +2 with the split step, -2 with the FFT form
 
 void upload_momentum(eplace_ctx *c, uint64_t iters) {
   AllocOn on_stream(c->stream);
@@ -2305,7 +2301,7 @@ struct JobState {
       CK(cudaEventElapsedTime(&ms, ev0, ev1));
       res->gpu_seconds = ms * 1e-3;
       res->gpu_launches = (uint64_t)(kLaunchesPerIter + (c->split_step ? 2 : 0) + (c->fold && !tc && !c->fft ? 2 : 0) -
-                                         (final_fused(c, tc) ? 1 : 0)) *
+                                         (final_fused(c, tc) ? 2 : 0)) *
                               launched_iters +
                           (gpu_legal ? 2 * cps.size() : 0) + (uint64_t)ip_launches;
       res->iters = (uint32_t)iters_done;

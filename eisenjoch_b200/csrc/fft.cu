@@ -125,7 +125,7 @@ struct FftGeom {
 
 __host__ __device__ inline FftGeom fft_geom(int stage, int W, int H) {
   FftGeom g;
-  const bool rows = stage == 0 || stage == 2;
+  const bool rows = stage != 1;
   g.N = rows ? W : H;
   g.L = rows ? H : W;
   g.logN = 0;
@@ -139,27 +139,33 @@ __host__ __device__ inline FftGeom fft_geom(int stage, int W, int H) {
   return g;
 }
 
-// Dynamic shared memory of a stage: the FFTs, the twiddles (N/2 + N), then
-// (stages 2 and 3) the lines as loaded.
+// Complex points of a stage's FFT buffers: stage 1 also runs one inverse FFT
+// per column after its forward ones.
+__host__ __device__ inline int fft_slots(int stage, const FftGeom &g) {
+  return (stage == 1 ? g.lines : g.ffts) * g.N;
+}
+
+// Dynamic shared memory of a stage: the FFTs (padded), the twiddles (N/2 +
+// N), then (stages 1 to 3) two arrays of the CTA's lines.
 __host__ __device__ inline size_t fft_smem(int stage, const FftGeom &g) {
-  const int arrays = stage <= 1 ? 0 : 2;
-  const size_t pts = (size_t)g.ffts * g.N;
+  const int arrays = stage == 0 ? 0 : 2;
+  const size_t pts = (size_t)fft_slots(stage, g);
   return sizeof(float2) * (pts + pts / 16 + g.N / 2 + g.N) + sizeof(float) * (size_t)arrays * g.lines * g.N;
 }
 
 template <int STAGE>
 __global__ void __launch_bounds__(kFftThreads) k_fft(const FftStageArgs a) {
   extern __shared__ float2 s[];
-  constexpr bool kRows = STAGE == 0 || STAGE == 2;
+  constexpr bool kRows = STAGE != 1;
   constexpr bool kFwd = STAGE <= 1;
   constexpr int kArrays = kFwd ? 1 : 2;
   const FftGeom G = fft_geom(STAGE, a.W, a.H);
   const int N = G.N, logN = G.logN, nl = G.lines;
   const FftTables tb = kRows ? a.tx : a.ty;
   const int line0 = blockIdx.x * nl;
-  float2 *tw = s + pd(G.ffts * N);  // [N/2] e^{-2 pi i j / N}
+  float2 *tw = s + pd(fft_slots(STAGE, G));  // [N/2] e^{-2 pi i j / N}
   float2 *tq = tw + N / 2;              // [N]   (cos, sin)(pi k / 2N)
-  float *R = reinterpret_cast<float *>(tq + N);  // stages 2, 3: R[array][line][pos]
+  float *R = reinterpret_cast<float *>(tq + N);  // stages 1 to 3: R[array][line][pos]
   // 16-byte vectors: rows hold 4 consecutive positions of one line, columns
   // the 4 lines of the CTA at one position.
   const int nvec = nl * N / 4;
@@ -264,12 +270,11 @@ __global__ void __launch_bounds__(kFftThreads) k_fft(const FftStageArgs a) {
     }
   }
   __syncthreads();
-  // 2. stages 2 and 3: the FFT inputs, bit-reversed
-  const int total = nl * N;
-  if (!kFwd) {
-    // line l of in_a and of in_b -> real and imaginary parts of FFT l
+  // 2. inverse stages: the FFT inputs, bit-reversed.  Line l of array a
+  // and of array b (R) -> real and imaginary parts of FFT l.
+  auto inv_build = [&]() {
     const float *Ra = R, *Rb = R + (size_t)nl * N;
-    for (int e = threadIdx.x; e < total; e += kFftThreads) {
+    for (int e = threadIdx.x; e < nl * N; e += kFftThreads) {
       const int l = e >> logN, k = e & (N - 1);
       const float *ra = Ra + (l << logN), *rb = Rb + (l << logN);
       const int ia = pre_index(a.kind_a, k, N), ib = pre_index(a.kind_b, k, N);
@@ -290,61 +295,88 @@ __global__ void __launch_bounds__(kFftThreads) k_fft(const FftStageArgs a) {
       // inverse sum
       s[pd((l << logN) + bitrev(k, logN))] = make_float2(va.x - vb.y, -(va.y + vb.x));
     }
-  }
-  __syncthreads();
-  fft_core(s, logN, G.ffts, tw);
-  // 3. outputs, one 16-byte vector per thread and array
-  for (int v = threadIdx.x; v < nvec; v += kFftThreads) {
-    int l0, n0;
-    const size_t g = vec_at(v, l0, n0);
-    float o[3][4];
+  };
+  // the inverse outputs, one 16-byte vector per thread and array
+  auto inv_out = [&]() {
+    for (int v = threadIdx.x; v < nvec; v += kFftThreads) {
+      int l0, n0;
+      const size_t g = vec_at(v, l0, n0);
+      float o[2][4];
 #pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      const int l = kRows ? l0 : c, n = kRows ? n0 + c : n0;
-      if (kFwd) {
-        const int k = n;
-        const int b0 = (l >> 1) << logN;
-        const float2 z = s[pd(b0 + k)], zc = s[pd(b0 + ((N - k) & (N - 1)))];
-        // the line's own spectrum V: (Z[k] + conj Z[N-k]) / 2 for the real
-        // part's line, (Z[k] - conj Z[N-k]) / 2i for the imaginary part's
-        float vx, vy;
-        if ((l & 1) == 0) {
-          vx = 0.5f * (z.x + zc.x);
-          vy = 0.5f * (z.y - zc.y);
-        } else {
-          vx = 0.5f * (z.y + zc.y);
-          vy = -0.5f * (z.x - zc.x);
-        }
-        const float2 q = tq[k];
-        const float X = q.x * vx + q.y * vy;  // Re(e^{-i pi k / 2N} V[k])
-        if (STAGE == 0) {
-          o[0][c] = X;
-        } else {
-          // spectral epilogue at (ky, kx) = (k, line)
-          const int kx = line0 + l, ky = k;
-          float sc = a.scale;
-          if (kx == 0) sc *= 0.5f;
-          if (ky == 0) sc *= 0.5f;
-          const float den = __ldg(a.gx2 + kx) + __ldg(a.gy2 + ky);
-          float ph = 0.0f, ex = 0.0f, ey = 0.0f;
-          if (!(den < 1e-30f)) {
-            ph = X * sc / den;
-            ex = ph * __ldg(a.wx + kx);
-            ey = ph * __ldg(a.wy + ky);
-          }
-          o[0][c] = ex;
-          o[1][c] = ey;
-          o[2][c] = ph;
-        }
-      } else {
+      for (int c = 0; c < 4; ++c) {
+        const int l = kRows ? l0 : c, n = kRows ? n0 + c : n0;
         const float2 z = s[pd((l << logN) + vpos(n, N))];
         o[0][c] = z.x * post_sign(a.kind_a, n);
         o[1][c] = -z.y * post_sign(a.kind_b, n);
       }
+      *reinterpret_cast<float4 *>(a.out_a + g) = make_float4(o[0][0], o[0][1], o[0][2], o[0][3]);
+      *reinterpret_cast<float4 *>(a.out_b + g) = make_float4(o[1][0], o[1][1], o[1][2], o[1][3]);
     }
-    *reinterpret_cast<float4 *>(a.out_a + g) = make_float4(o[0][0], o[0][1], o[0][2], o[0][3]);
-    if (STAGE >= 1) *reinterpret_cast<float4 *>(a.out_b + g) = make_float4(o[1][0], o[1][1], o[1][2], o[1][3]);
-    if (STAGE == 1 && a.phi) *reinterpret_cast<float4 *>(a.phi + g) = make_float4(o[2][0], o[2][1], o[2][2], o[2][3]);
+  };
+  if (!kFwd) {
+    inv_build();
+    __syncthreads();
+    fft_core(s, logN, nl, tw);
+    inv_out();
+    return;
+  }
+  __syncthreads();
+  fft_core(s, logN, G.ffts, tw);
+  // 3. forward outputs: stage 0 writes T; stage 1 applies the spectral
+  // epilogue, writes phi (when asked), keeps Ex^ and Ey^ of its columns in R
+  // and transforms them back along y (Ex: C3, Ey: S3 or SG) before writing.
+  float *Rx = R, *Ry = R + (size_t)nl * N;
+  for (int v = threadIdx.x; v < nvec; v += kFftThreads) {
+    int l0, n0;
+    const size_t g = vec_at(v, l0, n0);
+    float o[2][4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const int l = kRows ? l0 : c, k = kRows ? n0 + c : n0;
+      const int b0 = (l >> 1) << logN;
+      const float2 z = s[pd(b0 + k)], zc = s[pd(b0 + ((N - k) & (N - 1)))];
+      // the line's own spectrum V: (Z[k] + conj Z[N-k]) / 2 for the real
+      // part's line, (Z[k] - conj Z[N-k]) / 2i for the imaginary part's
+      float vx, vy;
+      if ((l & 1) == 0) {
+        vx = 0.5f * (z.x + zc.x);
+        vy = 0.5f * (z.y - zc.y);
+      } else {
+        vx = 0.5f * (z.y + zc.y);
+        vy = -0.5f * (z.x - zc.x);
+      }
+      const float2 q = tq[k];
+      const float X = q.x * vx + q.y * vy;  // Re(e^{-i pi k / 2N} V[k])
+      if (STAGE == 0) {
+        o[0][c] = X;
+      } else {
+        // spectral epilogue at (ky, kx) = (k, line)
+        const int kx = line0 + l, ky = k;
+        float sc = a.scale;
+        if (kx == 0) sc *= 0.5f;
+        if (ky == 0) sc *= 0.5f;
+        const float den = __ldg(a.gx2 + kx) + __ldg(a.gy2 + ky);
+        float ph = 0.0f, ex = 0.0f, ey = 0.0f;
+        if (!(den < 1e-30f)) {
+          ph = X * sc / den;
+          ex = ph * __ldg(a.wx + kx);
+          ey = ph * __ldg(a.wy + ky);
+        }
+        Rx[(l << logN) + ky] = ex;
+        Ry[(l << logN) + ky] = ey;
+        o[0][c] = ph;
+      }
+    }
+    if (STAGE == 0) *reinterpret_cast<float4 *>(a.out_a + g) = make_float4(o[0][0], o[0][1], o[0][2], o[0][3]);
+    if (STAGE == 1 && a.phi) *reinterpret_cast<float4 *>(a.phi + g) = make_float4(o[0][0], o[0][1], o[0][2], o[0][3]);
+  }
+  if (STAGE == 1) {
+    __syncthreads();  // every forward output read before the buffers are reused
+    inv_build();
+    __syncthreads();
+    fft_core(s, logN, nl, tw);
+    inv_out();
+    return;
   }
   if (STAGE == 0 && a.dens) {
     // the overlap: CTA partials, then the last CTA sums them in CTA order
@@ -412,13 +444,9 @@ cudaError_t launch_fft_stage(int stage, const FftStageArgs &a, cudaStream_t s) {
       e = cudaFuncSetAttribute(k_fft<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, cap);
       if (e == cudaSuccess) k_fft<1><<<grid, kFftThreads, smem, s>>>(a);
       break;
-    case 2:
+    default:
       e = cudaFuncSetAttribute(k_fft<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, cap);
       if (e == cudaSuccess) k_fft<2><<<grid, kFftThreads, smem, s>>>(a);
-      break;
-    default:
-      e = cudaFuncSetAttribute(k_fft<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, cap);
-      if (e == cudaSuccess) k_fft<3><<<grid, kFftThreads, smem, s>>>(a);
       break;
   }
   return e != cudaSuccess ? e : cudaGetLastError();

@@ -1,13 +1,14 @@
 // fft.cuh -- the spectral Poisson solve's transforms as FFTs (FP32).
 //
-// The four transform stages of one iteration (density.rs:96-166, the same
-// linear maps as the DCT-matrix GEMMs of kernels.cu / dct_tc.cu):
-//   stage 0  T   = DCT-II along x of rho                 (rows)
-//   stage 1  A   = DCT-II along y of T, then the spectral scale / Poisson
-//                  divide / field weights -> Ex^, Ey^ (and phi)  (columns)
-//   stage 2  U   = S3 (reference field) or SG (potential-gradient field)
-//                  along x of Ex^;  V = C3 along x of Ey^    (rows)
-//   stage 3  Ex  = C3 along y of U;  Ey = S3 or SG along y of V  (columns)
+// The linear maps of density.rs:96-166 (the same as the DCT-matrix GEMMs of
+// kernels.cu / dct_tc.cu), in three stages per iteration:
+//   stage 0  T   = DCT-II along x of rho                        (rows)
+//   stage 1  A   = DCT-II along y of T; the spectral scale, Poisson divide
+//                  and field weights -> Ex^, Ey^ (and phi); then along y
+//                  U = C3 of Ex^, V = S3 (reference field) or SG
+//                  (potential-gradient field) of Ey^            (columns)
+//   stage 2  Ex  = S3 or SG along x of U;  Ey = C3 along x of V (rows)
+// (the 2D transforms are separable, so the inverse may take y before x),
 // with, for a line of length N and theta = pi k (n + 1/2) / N,
 //   DCT-II  X[k] = sum_n x[n] cos(theta)
 //   C3      x[n] = sum_k c_k X[k] cos(theta),  c_0 = 1/2
@@ -21,8 +22,8 @@
 //   S3(X)[n] = (-1)^n C3(X reversed)[n];
 //   SG(X)[n] = -(-1)^n C3(Y)[n], Y[0] = 0, Y[k] = X[N-k].
 // Two real transforms share one complex FFT: two lines of the same array
-// (stages 0 and 1, split by the conjugate symmetry of real inputs) or the
-// same line of two arrays (stages 2 and 3, whose outputs are real).
+// (the forward transforms, split by the conjugate symmetry of real inputs)
+// or the same line of two arrays (the inverse ones, whose outputs are real).
 // O(N log N) per line instead of the GEMMs' O(N^2); FP32 rounding error grows
 // with log N instead of N.  Power-of-two grids of 16 .. 1024 bins per axis.
 #pragma once
@@ -47,7 +48,7 @@ struct FftStageArgs {
   const float *in_a, *in_b;
   float *out_a, *out_b;
   FftTables tx, ty;       // length W and length H tables
-  int kind_a, kind_b;     // stage 2 / 3: FftKind of each array
+  int kind_a, kind_b;     // FftKind of the inverse transform of each array (stages 1, 2)
   // stage 1 spectral epilogue (same formula as the GEMM epilogues)
   const float *wx, *gx2, *wy, *gy2;
   float scale;            // 4 / (W H)
@@ -69,7 +70,7 @@ struct FftStageArgs {
 bool fft_supported(int W, int H);
 // Host-side tables for length N: tw [N/2], tq [N].
 void fft_tables_host(int N, float2 *tw, float2 *tq);
-// One of the four stages (0..3) on stream s.
+// One of the three stages (0..2) on stream s.
 cudaError_t launch_fft_stage(int stage, const FftStageArgs &a, cudaStream_t s);
 
 }  // namespace eplace
