@@ -6,7 +6,7 @@
 // and stored once per stage, as 16-byte vectors (four positions of a row, or
 // the four columns of a CTA at one row), with the lines staged in shared
 // memory; the working set of a 1024^2 grid (4 MB per array) stays in L2
-// across the four stages.
+// across the three stages.
 #include <cmath>
 
 #include "fft.cuh"
