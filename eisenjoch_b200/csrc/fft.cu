@@ -146,7 +146,7 @@ __host__ __device__ inline int fft_slots(int stage, const FftGeom &g) {
 }
 
 // Dynamic shared memory of a stage: the FFTs (padded), the twiddles (N/2 +
-// N), then (stages 1 to 3) two arrays of the CTA's lines.
+// N), then (stages 1 and 2) two arrays of the CTA's lines.
 __host__ __device__ inline size_t fft_smem(int stage, const FftGeom &g) {
   const int arrays = stage == 0 ? 0 : 2;
   const size_t pts = (size_t)fft_slots(stage, g);
@@ -165,7 +165,7 @@ __global__ void __launch_bounds__(kFftThreads) k_fft(const FftStageArgs a) {
   const int line0 = blockIdx.x * nl;
   float2 *tw = s + pd(fft_slots(STAGE, G));  // [N/2] e^{-2 pi i j / N}
   float2 *tq = tw + N / 2;              // [N]   (cos, sin)(pi k / 2N)
-  float *R = reinterpret_cast<float *>(tq + N);  // stages 1 to 3: R[array][line][pos]
+  float *R = reinterpret_cast<float *>(tq + N);  // stages 1 and 2: R[array][line][pos]
   // 16-byte vectors: rows hold 4 consecutive positions of one line, columns
   // the 4 lines of the CTA at one position.
   const int nvec = nl * N / 4;
