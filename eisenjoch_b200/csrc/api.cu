@@ -27,6 +27,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <exception>
 #include <thread>
 #include <vector>
 
@@ -199,6 +200,23 @@ class PinArena {
   std::vector<void *> free_[kMaxClass - kMinClass + 1];
 };
 
+// A pinned host block from the arena, grown on demand and kept by its owner.
+struct PinBlock {
+  void *p = nullptr;
+  size_t bytes = 0;
+  int cls = 0;
+  PinBlock() = default;
+  PinBlock(const PinBlock &) = delete;
+  PinBlock &operator=(const PinBlock &) = delete;
+  ~PinBlock() { PinArena::get().put(p, cls); }
+  void reserve(size_t need) {
+    if (p && need <= bytes) return;
+    PinArena::get().put(p, cls);
+    p = PinArena::get().take(std::max<size_t>(need, 1), &cls);
+    bytes = (size_t)1 << cls;
+  }
+};
+
 // A checkpoint's positions in pinned memory (the interval's device-to-host
 // copy lands here) and the host legaliser's binding of them.  Kept by the
 // context and reused across checkpoints and runs.
@@ -286,6 +304,10 @@ struct eplace_ctx {
   DBuf<float> area, pw;
   DBuf<uint8_t> mflag;      // [N] 1 for a macro
   DBuf<uint32_t> mac_idx;   // the macros' cell ids
+  // The WA pin table is built in pinned memory and uploaded asynchronously;
+  // wa_pin_ev marks the end of the last upload from it.
+  PinBlock wa_pin;
+  cudaEvent_t wa_pin_ev = nullptr;
   uint32_t n_mac = 0;
   // state
   DBuf<float2> look;  // [N + F]
@@ -405,6 +427,7 @@ struct eplace_ctx {
     if (side) cudaStreamSynchronize(side);
     if (ev_fork) cudaEventDestroy(ev_fork);
     if (ev_join) cudaEventDestroy(ev_join);
+    if (wa_pin_ev) cudaEventDestroy(wa_pin_ev);
     if (side) cudaStreamDestroy(side);
     if (stream) cudaStreamDestroy(stream);
   }
@@ -456,10 +479,13 @@ void sorted_pins(const HostProblem &hp, const std::vector<uint32_t> &order, cons
 // The padded pin table of the degree classes: net idx of class j takes
 // G * S slots (G = kWaGroup[j], S = kWaSlots[j]) from the class base (a
 // multiple of 4 slots, for 16-byte loads); pin q of the net goes to lane
-// q % G, slot q / G of that lane.  Sets each class's slot_base.  Three
-// threads fill disjoint runs of classes of about equal size.
-std::vector<uint32_t> build_wa_slots(const HostProblem &hp, const std::vector<uint32_t> &order,
-                                     WaClass (&cls)[kWaClasses]) {
+// q % G, slot q / G of that lane, unused slots 0xffffffff.  Sets each
+// class's slot_base, writes the table to t (cap slots) and returns its
+// length.  A class pads a net of d pins to fewer than 2d slots (2 for 2,
+// 4 for 3..4, 8 for 5..8, ..., 256 for 129..224), so 2P + 64 slots always
+// suffice.  Three threads fill disjoint runs of classes of about equal size.
+size_t build_wa_slots(const HostProblem &hp, const std::vector<uint32_t> &order, WaClass (&cls)[kWaClasses],
+                      uint32_t *t, size_t cap) {
   size_t total = 0;
   size_t upto[kWaClasses + 1] = {0};
   for (int j = 0; j < kWaClasses; ++j) {
@@ -468,15 +494,18 @@ std::vector<uint32_t> build_wa_slots(const HostProblem &hp, const std::vector<ui
     total += (size_t)cls[j].nets * kWaGroup[j] * kWaSlots[j];
     upto[j + 1] = total;
   }
-  std::vector<uint32_t> t(std::max<size_t>(total, 4), 0xffffffffu);
+  const size_t len = std::max<size_t>(total, 4);
+  if (len > cap) throw CudaError{cudaErrorInvalidValue, "build_wa_slots: table larger than its bound"};
   auto fill = [&](int j0, int j1) {
     for (int j = j0; j < j1; ++j) {
       const int G = kWaGroup[j], S = kWaSlots[j];
+      const size_t b0 = (size_t)cls[j].slot_base;
+      std::fill(t + b0, t + upto[j + 1], 0xffffffffu);
       if (S == 0) continue;
       const int gs = __builtin_ctz(G);  // G is a power of two
       for (int idx = 0; idx < cls[j].nets; ++idx) {
         const uint32_t n = order[(uint32_t)(cls[j].first_net + idx)];
-        const size_t base = (size_t)cls[j].slot_base + (size_t)idx * G * S;
+        const size_t base = b0 + (size_t)idx * G * S;
         const uint32_t b = hp.net_off[n], d = hp.net_off[n + 1] - b;
         for (uint32_t r = 0; r < d; ++r) t[base + (size_t)(r & (G - 1)) * S + (r >> gs)] = hp.pin_cell[b + r];
       }
@@ -492,7 +521,10 @@ std::vector<uint32_t> build_wa_slots(const HostProblem &hp, const std::vector<ui
   fill(cut[0], cut[1]);
   t1.join();
   t2.join();
-  return t;
+  // the alignment gaps between classes and the tail of a short table
+  for (int j = 0; j + 1 < kWaClasses; ++j) std::fill(t + upto[j + 1], t + (size_t)cls[j + 1].slot_base, 0xffffffffu);
+  std::fill(t + total, t + len, 0xffffffffu);
+  return len;
 }
 
 // Fixed-point exponent k of the packed WA gradient: every cell's x and y
@@ -1426,14 +1458,24 @@ void load_into(eplace_ctx *c, HostProblem &&hp_in) {
   ++c->buf_epoch;
   // Host-side derived arrays are built on two helper threads while this
   // thread uploads the netlist; all CUDA calls stay on this thread.
-  std::vector<uint32_t> sorder, soff, spins, slots;
+  std::vector<uint32_t> sorder, soff, spins;
   WaClass cls[kWaClasses];
   int wa_warps = 0;
+  const size_t wa_cap = 2 * (size_t)hp.P + 64;
+  if (c->wa_pin_ev) CK(cudaEventSynchronize(c->wa_pin_ev));  // the last upload from the block is done
+  c->wa_pin.reserve(sizeof(uint32_t) * wa_cap);
+  uint32_t *slots = static_cast<uint32_t *>(c->wa_pin.p);
+  size_t nslots = 0;
+  std::exception_ptr wa_err;
   std::thread t_wa([&] {
     degree_order(hp, sorder, soff);
     wa_warps = build_wa_classes(soff, cls);
     sorted_pins(hp, sorder, soff, (uint32_t)cls[kWaClasses - 1].first_net, hp.NN, spins);
-    slots = build_wa_slots(hp, sorder, cls);
+    try {
+      nslots = build_wa_slots(hp, sorder, cls, slots, wa_cap);
+    } catch (...) {
+      wa_err = std::current_exception();
+    }
   });
   int grad_k = 24;
   std::thread t_pw([&] { pin_weights(hp, c->pw_host); });
@@ -1531,8 +1573,11 @@ void load_into(eplace_ctx *c, HostProblem &&hp_in) {
       CK(cudaMemcpyAsync(c->wa_pins.p + at, spins.data(), sizeof(uint32_t) * spins.size(), cudaMemcpyHostToDevice, s));
       g_h2d += sizeof(uint32_t) * spins.size();
     }
-    c->wa_slots.ensure(slots.size());
-    c->wa_slots.upload(slots.data(), slots.size(), s);
+    if (wa_err) std::rethrow_exception(wa_err);
+    c->wa_slots.ensure(nslots);
+    c->wa_slots.upload(slots, nslots, s);  // from pinned memory: asynchronous
+    if (!c->wa_pin_ev) CK(cudaEventCreateWithFlags(&c->wa_pin_ev, cudaEventDisableTiming));
+    CK(cudaEventRecord(c->wa_pin_ev, s));
   }
   t_pw.join();
   std::vector<float> pwf(c->pw_host.begin(), c->pw_host.end());
