@@ -847,14 +847,33 @@ eplace_status Legalizer::run(const float *x, const float *y, size_t stride, int3
       bx = (int32_t)(best_t % W);
       by = (int32_t)(best_t / W);
     }
-    for (int dy = 0; dy < h; ++dy)
-      for (int dx = 0; dx < w; ++dx) {
-        const int32_t xx = bx + dx;
-        uint64_t &word = fm[(size_t)(by + dy) * WR + (xx >> 6)];
-        word &= ~(1ull << (xx & 63));
-        if (sm && !word) sm[by + dy] &= ~(1ull << (xx >> 6));
-        if (xx == lc[by + dy] || xx == rc[by + dy]) lc[by + dy] = INT32_MAX;
+    if (w == 1 && h == 1) {
+      // A unit cell takes one site.  When it is one of its row's two cached
+      // candidates, the next free site past it (on the same side) becomes
+      // the candidate: every site between the two stays taken, so the entry
+      // stays valid and the next cell of a pile reads it instead of
+      // searching the row again.
+      uint64_t *row = fm + (size_t)by * WR;
+      row[bx >> 6] &= ~(1ull << (bx & 63));
+      if (sm && !row[bx >> 6]) sm[by] &= ~(1ull << (bx >> 6));
+      if (lc[by] != INT32_MAX) {
+        if (bx == lc[by]) {
+          lc[by] = free_at_or_left(row, sm ? sm + by : nullptr, bx - 1);
+        } else if (bx == rc[by]) {
+          const int32_t r2 = free_at_or_right(row, sm ? sm + by : nullptr, bx + 1, W, WR);
+          rc[by] = r2 >= 0 ? r2 : W;
+        }
       }
+    } else {
+      for (int dy = 0; dy < h; ++dy)
+        for (int dx = 0; dx < w; ++dx) {
+          const int32_t xx = bx + dx;
+          uint64_t &word = fm[(size_t)(by + dy) * WR + (xx >> 6)];
+          word &= ~(1ull << (xx & 63));
+          if (sm && !word) sm[by + dy] &= ~(1ull << (xx >> 6));
+          if (xx == lc[by + dy] || xx == rc[by + dy]) lc[by + dy] = INT32_MAX;
+        }
+    }
     site_x[i] = bx;
     site_y[i] = by;
     total += best;
