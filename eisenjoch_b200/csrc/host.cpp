@@ -573,7 +573,7 @@ struct Lanes8 {
   __m512d bc;   // best cost per lane
   __m512i bt;   // its tile (INT64_MAX: none)
   __m512i kw;   // k * W for lane k
-  double best;  // minimum over the lanes and the scalar rows
+  double best;  // minimum over the scalar rows (the lanes keep theirs in bc)
 };
 
 __attribute__((target("avx512f,avx2"))) inline void lane_update(Lanes8 &L, __m512d c, __m512i t, __mmask8 ok) {
@@ -592,11 +592,12 @@ __attribute__((target("avx512f,avx2"))) inline void rows8(RowSearch &s, Lanes8 &
                                         _mm256_cmpgt_epi32(_mm256_add_epi32(fxv, _mm256_set1_epi32(1)), r));
   if (_mm256_movemask_epi8(stale)) {
     // Refresh only the rows still within reach (as in rows4).
+    const double bnow = std::min(L.best, _mm512_reduce_min_pd(L.bc));
     alignas(32) int32_t la[8], ra[8];
     for (int32_t k = 0; k < 8; ++k) {
       const int32_t row = r0 + k;
       const double d = (double)row - s.ty;
-      if (d * d > L.best) {
+      if (d * d > bnow) {
         la[k] = -1;
         ra[k] = s.W;
       } else {
@@ -621,7 +622,13 @@ __attribute__((target("avx512f,avx2"))) inline void rows8(RowSearch &s, Lanes8 &
       (__mmask8)_mm256_movemask_ps(_mm256_castsi256_ps(_mm256_cmpgt_epi32(_mm256_set1_epi32(s.W), r)));
   const __m512d dxr = _mm512_sub_pd(_mm512_cvtepi32_pd(r), txv);
   lane_update(L, _mm512_add_pd(_mm512_mul_pd(dxr, dxr), dy2), _mm512_add_epi64(base, _mm512_cvtepi32_epi64(r)), okr);
-  L.best = std::min(L.best, _mm512_reduce_min_pd(L.bc));
+}
+
+// Whether a row at squared distance d2 from the target can no longer win or
+// tie: d2 exceeds the best of the scalar rows or of some lane (no horizontal
+// minimum needed).
+__attribute__((target("avx512f,avx2"))) inline bool past(const Lanes8 &L, double d2) {
+  return d2 > L.best || _mm512_cmp_pd_mask(L.bc, _mm512_set1_pd(d2), _CMP_LT_OQ) != 0;
 }
 
 __attribute__((target("avx512f,avx2"), noinline)) void search_rows8(RowSearch &s, int32_t cy) {
@@ -635,7 +642,7 @@ __attribute__((target("avx512f,avx2"), noinline)) void search_rows8(RowSearch &s
     if (down) {
       const int32_t row = cy - dd;
       const double d = (double)row - s.ty;
-      if (row < 0 || d * d > L.best) {
+      if (row < 0 || past(L, d * d)) {
         down = false;
       } else if (row >= 7) {
         rows8(s, L, row - 7);
@@ -649,7 +656,7 @@ __attribute__((target("avx512f,avx2"), noinline)) void search_rows8(RowSearch &s
     if (up) {
       const int32_t row = cy + du;
       const double d = (double)row - s.ty;
-      if (row >= s.H || d * d > L.best) {
+      if (row >= s.H || past(L, d * d)) {
         up = false;
       } else if (row + 7 < s.H) {
         rows8(s, L, row);
