@@ -576,14 +576,23 @@ struct Lanes8 {
   double best;  // minimum over the scalar rows (the lanes keep theirs in bc)
 };
 
-__attribute__((target("avx512f,avx2"))) inline void lane_update(Lanes8 &L, __m512d c, __m512i t, __mmask8 ok) {
-  const __mmask8 lt = _mm512_cmp_pd_mask(c, L.bc, _CMP_LT_OQ);
-  const __mmask8 eq = _mm512_cmp_pd_mask(c, L.bc, _CMP_EQ_OQ) & _mm512_cmplt_epi64_mask(t, L.bt);
-  const __mmask8 u = ok & (lt | eq);
+// Lane update with the tile order taken from the visiting order, so no tile
+// compare is needed.  Rows below the target are visited downward (their
+// tiles decrease), rows above it upward (tiles increase), and every row
+// below has lower tiles than every row above.  So an upward candidate never
+// displaces one of equal cost (its tile is higher: strict <) and a downward
+// candidate always does (its tile is lower: <=); within a row the left site
+// (the lower tile) comes first upward and last downward.  A lane thus keeps
+// the lowest tile among its least-cost candidates, as (cost, tile) order
+// asks.
+template <bool DOWN>
+__attribute__((target("avx512f,avx2"))) inline void lane_keep(Lanes8 &L, __m512d c, __m512i t, __mmask8 ok) {
+  const __mmask8 u = ok & _mm512_cmp_pd_mask(c, L.bc, DOWN ? _CMP_LE_OQ : _CMP_LT_OQ);
   L.bc = _mm512_mask_blend_pd(u, L.bc, c);
   L.bt = _mm512_mask_blend_epi64(u, L.bt, t);
 }
 
+template <bool DOWN>
 __attribute__((target("avx512f,avx2"))) inline void rows8(RowSearch &s, Lanes8 &L, int32_t r0) {
   __m256i l = _mm256_loadu_si256(reinterpret_cast<const __m256i *>(s.lc + r0));
   __m256i r = _mm256_loadu_si256(reinterpret_cast<const __m256i *>(s.rc + r0));
@@ -617,11 +626,20 @@ __attribute__((target("avx512f,avx2"))) inline void rows8(RowSearch &s, Lanes8 &
   const __m512i base = _mm512_add_epi64(_mm512_set1_epi64((int64_t)r0 * s.W), L.kw);
   const __mmask8 okl = (__mmask8)_mm256_movemask_ps(_mm256_castsi256_ps(_mm256_cmpgt_epi32(l, _mm256_set1_epi32(-1))));
   const __m512d dxl = _mm512_sub_pd(_mm512_cvtepi32_pd(l), txv);
-  lane_update(L, _mm512_add_pd(_mm512_mul_pd(dxl, dxl), dy2), _mm512_add_epi64(base, _mm512_cvtepi32_epi64(l)), okl);
+  const __m512d cl = _mm512_add_pd(_mm512_mul_pd(dxl, dxl), dy2);
+  const __m512i tl = _mm512_add_epi64(base, _mm512_cvtepi32_epi64(l));
   const __mmask8 okr =
       (__mmask8)_mm256_movemask_ps(_mm256_castsi256_ps(_mm256_cmpgt_epi32(_mm256_set1_epi32(s.W), r)));
   const __m512d dxr = _mm512_sub_pd(_mm512_cvtepi32_pd(r), txv);
-  lane_update(L, _mm512_add_pd(_mm512_mul_pd(dxr, dxr), dy2), _mm512_add_epi64(base, _mm512_cvtepi32_epi64(r)), okr);
+  const __m512d cr = _mm512_add_pd(_mm512_mul_pd(dxr, dxr), dy2);
+  const __m512i tr = _mm512_add_epi64(base, _mm512_cvtepi32_epi64(r));
+  if (DOWN) {
+    lane_keep<true>(L, cr, tr, okr);
+    lane_keep<true>(L, cl, tl, okl);
+  } else {
+    lane_keep<false>(L, cl, tl, okl);
+    lane_keep<false>(L, cr, tr, okr);
+  }
 }
 
 // Whether a row at squared distance d2 from the target can no longer win or
@@ -645,7 +663,7 @@ __attribute__((target("avx512f,avx2"), noinline)) void search_rows8(RowSearch &s
       if (row < 0 || past(L, d * d)) {
         down = false;
       } else if (row >= 7) {
-        rows8(s, L, row - 7);
+        rows8<true>(s, L, row - 7);
         dd += 8;
       } else {
         scan_row(s, row);
@@ -659,7 +677,7 @@ __attribute__((target("avx512f,avx2"), noinline)) void search_rows8(RowSearch &s
       if (row >= s.H || past(L, d * d)) {
         up = false;
       } else if (row + 7 < s.H) {
-        rows8(s, L, row);
+        rows8<false>(s, L, row);
         du += 8;
       } else {
         scan_row(s, row);
