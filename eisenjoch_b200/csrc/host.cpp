@@ -228,7 +228,7 @@ Legalizer::Legalizer(const HostProblem &hp, const LegalBase &base) : hp_(hp), ba
   const char *cap = std::getenv("EPLACE_LEGAL_SIMD");
   const int level = cap ? std::atoi(cap) : 2;
   simd_ = level >= 1 && __builtin_cpu_supports("avx2");
-  simd512_ = simd_ && level >= 2 && __builtin_cpu_supports("avx512f");
+  simd512_ = simd_ && level >= 2 && __builtin_cpu_supports("avx512f") && __builtin_cpu_supports("avx512vl");
   free_.resize(base.free0.size());
   sum_.resize(base.sum0.size());
   lc_.resize(std::max(base.H, 0));
@@ -586,20 +586,26 @@ struct Lanes8 {
 // the lowest tile among its least-cost candidates, as (cost, tile) order
 // asks.
 template <bool DOWN>
-__attribute__((target("avx512f,avx2"))) inline void lane_keep(Lanes8 &L, __m512d c, __m512i t, __mmask8 ok) {
+__attribute__((target("avx512f,avx512vl,avx2"))) inline void lane_keep(Lanes8 &L, __m512d c, __m512i t, __mmask8 ok) {
   const __mmask8 u = ok & _mm512_cmp_pd_mask(c, L.bc, DOWN ? _CMP_LE_OQ : _CMP_LT_OQ);
   L.bc = _mm512_mask_blend_pd(u, L.bc, c);
   L.bt = _mm512_mask_blend_epi64(u, L.bt, t);
 }
 
+// Per-search constants of rows8.
+struct Rows8K {
+  __m256i fxv, fx1v, m1, Wv;  // fx0, fx0 + 1, -1, W in eight lanes
+  __m512d txv;
+};
+
+// Rows r0 .. r0 + 7: dy holds (r0 + k) - ty and base (r0 + k) W per lane
+// (the caller steps both by 8 rows per call, exactly).
 template <bool DOWN>
-__attribute__((target("avx512f,avx2"))) inline void rows8(RowSearch &s, Lanes8 &L, int32_t r0) {
+__attribute__((target("avx512f,avx512vl,avx2"))) inline void rows8(RowSearch &s, Lanes8 &L, int32_t r0, __m512d dy,
+                                                                 __m512i base, const Rows8K &K) {
   __m256i l = _mm256_loadu_si256(reinterpret_cast<const __m256i *>(s.lc + r0));
   __m256i r = _mm256_loadu_si256(reinterpret_cast<const __m256i *>(s.rc + r0));
-  const __m256i fxv = _mm256_set1_epi32(s.fx0);
-  const __m256i stale = _mm256_or_si256(_mm256_cmpgt_epi32(l, fxv),
-                                        _mm256_cmpgt_epi32(_mm256_add_epi32(fxv, _mm256_set1_epi32(1)), r));
-  if (_mm256_movemask_epi8(stale)) {
+  if (_mm256_cmpgt_epi32_mask(l, K.fxv) | _mm256_cmpgt_epi32_mask(K.fx1v, r)) {
     // Refresh only the rows still within reach (as in rows4).
     const double bnow = std::min(L.best, _mm512_reduce_min_pd(L.bc));
     alignas(32) int32_t la[8], ra[8];
@@ -619,18 +625,13 @@ __attribute__((target("avx512f,avx2"))) inline void rows8(RowSearch &s, Lanes8 &
     l = _mm256_load_si256(reinterpret_cast<const __m256i *>(la));
     r = _mm256_load_si256(reinterpret_cast<const __m256i *>(ra));
   }
-  const __m512d txv = _mm512_set1_pd(s.tx);
-  const __m256i rows = _mm256_add_epi32(_mm256_set1_epi32(r0), _mm256_setr_epi32(0, 1, 2, 3, 4, 5, 6, 7));
-  const __m512d dy = _mm512_sub_pd(_mm512_cvtepi32_pd(rows), _mm512_set1_pd(s.ty));
   const __m512d dy2 = _mm512_mul_pd(dy, dy);
-  const __m512i base = _mm512_add_epi64(_mm512_set1_epi64((int64_t)r0 * s.W), L.kw);
-  const __mmask8 okl = (__mmask8)_mm256_movemask_ps(_mm256_castsi256_ps(_mm256_cmpgt_epi32(l, _mm256_set1_epi32(-1))));
-  const __m512d dxl = _mm512_sub_pd(_mm512_cvtepi32_pd(l), txv);
+  const __mmask8 okl = _mm256_cmpgt_epi32_mask(l, K.m1);
+  const __m512d dxl = _mm512_sub_pd(_mm512_cvtepi32_pd(l), K.txv);
   const __m512d cl = _mm512_add_pd(_mm512_mul_pd(dxl, dxl), dy2);
   const __m512i tl = _mm512_add_epi64(base, _mm512_cvtepi32_epi64(l));
-  const __mmask8 okr =
-      (__mmask8)_mm256_movemask_ps(_mm256_castsi256_ps(_mm256_cmpgt_epi32(_mm256_set1_epi32(s.W), r)));
-  const __m512d dxr = _mm512_sub_pd(_mm512_cvtepi32_pd(r), txv);
+  const __mmask8 okr = _mm256_cmpgt_epi32_mask(K.Wv, r);
+  const __m512d dxr = _mm512_sub_pd(_mm512_cvtepi32_pd(r), K.txv);
   const __m512d cr = _mm512_add_pd(_mm512_mul_pd(dxr, dxr), dy2);
   const __m512i tr = _mm512_add_epi64(base, _mm512_cvtepi32_epi64(r));
   if (DOWN) {
@@ -645,15 +646,27 @@ __attribute__((target("avx512f,avx2"))) inline void rows8(RowSearch &s, Lanes8 &
 // Whether a row at squared distance d2 from the target can no longer win or
 // tie: d2 exceeds the best of the scalar rows or of some lane (no horizontal
 // minimum needed).
-__attribute__((target("avx512f,avx2"))) inline bool past(const Lanes8 &L, double d2) {
+__attribute__((target("avx512f,avx512vl,avx2"))) inline bool past(const Lanes8 &L, double d2) {
   return d2 > L.best || _mm512_cmp_pd_mask(L.bc, _mm512_set1_pd(d2), _CMP_LT_OQ) != 0;
 }
 
-__attribute__((target("avx512f,avx2"), noinline)) void search_rows8(RowSearch &s, int32_t cy) {
+__attribute__((target("avx512f,avx512vl,avx2"), noinline)) void search_rows8(RowSearch &s, int32_t cy) {
   scan_row(s, cy);
   const int64_t W = s.W;
   Lanes8 L{_mm512_set1_pd(INFINITY), _mm512_set1_epi64(INT64_MAX),
            _mm512_setr_epi64(0, W, 2 * W, 3 * W, 4 * W, 5 * W, 6 * W, 7 * W), s.best};
+  const Rows8K K{_mm256_set1_epi32(s.fx0), _mm256_set1_epi32(s.fx0 + 1), _mm256_set1_epi32(-1),
+                 _mm256_set1_epi32(s.W), _mm512_set1_pd(s.tx)};
+  const __m256i iota = _mm256_setr_epi32(0, 1, 2, 3, 4, 5, 6, 7);
+  const __m512d tyv = _mm512_set1_pd(s.ty);
+  // lanes of the next call each way: rows cy - 8 .. cy - 1 down, cy + 1 ..
+  // cy + 8 up, then eight rows further per call
+  __m512d dyd = _mm512_sub_pd(_mm512_cvtepi32_pd(_mm256_add_epi32(_mm256_set1_epi32(cy - 8), iota)), tyv);
+  __m512d dyu = _mm512_sub_pd(_mm512_cvtepi32_pd(_mm256_add_epi32(_mm256_set1_epi32(cy + 1), iota)), tyv);
+  __m512i bsd = _mm512_add_epi64(_mm512_set1_epi64((int64_t)(cy - 8) * W), L.kw);
+  __m512i bsu = _mm512_add_epi64(_mm512_set1_epi64((int64_t)(cy + 1) * W), L.kw);
+  const __m512d step = _mm512_set1_pd(8.0);
+  const __m512i stepw = _mm512_set1_epi64(8 * W);
   bool up = true, down = true;
   int32_t dd = 1, du = 1;
   while (up || down) {
@@ -663,7 +676,9 @@ __attribute__((target("avx512f,avx2"), noinline)) void search_rows8(RowSearch &s
       if (row < 0 || past(L, d * d)) {
         down = false;
       } else if (row >= 7) {
-        rows8<true>(s, L, row - 7);
+        rows8<true>(s, L, row - 7, dyd, bsd, K);
+        dyd = _mm512_sub_pd(dyd, step);
+        bsd = _mm512_sub_epi64(bsd, stepw);
         dd += 8;
       } else {
         scan_row(s, row);
@@ -677,7 +692,9 @@ __attribute__((target("avx512f,avx2"), noinline)) void search_rows8(RowSearch &s
       if (row >= s.H || past(L, d * d)) {
         up = false;
       } else if (row + 7 < s.H) {
-        rows8<false>(s, L, row);
+        rows8<false>(s, L, row, dyu, bsu, K);
+        dyu = _mm512_add_pd(dyu, step);
+        bsu = _mm512_add_epi64(bsu, stepw);
         du += 8;
       } else {
         scan_row(s, row);
