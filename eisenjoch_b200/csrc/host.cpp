@@ -228,7 +228,9 @@ Legalizer::Legalizer(const HostProblem &hp, const LegalBase &base) : hp_(hp), ba
   const char *cap = std::getenv("EPLACE_LEGAL_SIMD");
   const int level = cap ? std::atoi(cap) : 2;
   simd_ = level >= 1 && __builtin_cpu_supports("avx2");
-  simd512_ = simd_ && level >= 2 && __builtin_cpu_supports("avx512f") && __builtin_cpu_supports("avx512vl");
+  // The eight-row search keeps tiles in 32 bits: chips below 2^31 sites.
+  simd512_ = simd_ && level >= 2 && __builtin_cpu_supports("avx512f") && __builtin_cpu_supports("avx512vl") &&
+             (int64_t)hp.W * hp.H < ((int64_t)1 << 31);
   free_.resize(base.free0.size());
   sum_.resize(base.sum0.size());
   lc_.resize(std::max(base.H, 0));
@@ -318,37 +320,6 @@ inline int nearest_ints(double t, int32_t n, int32_t (&out)[2]) {
 // the minimum over the grid.  Visited in tile order with a strict <, so the
 // lowest tile wins a tie, as in the reference's scan.  Leaves best / best_t
 // at the block's best free site (or unchanged when all nine are taken).
-inline void probe3(const uint64_t *fm, int32_t WR, int32_t W, int32_t H, int32_t cx, int32_t cy, double tx, double ty,
-                   double &best, int64_t &best_t, int32_t &bx, int32_t &by) {
-  double dx2[3], dy2[3];
-  for (int k = 0; k < 3; ++k) {
-    const double dx = (double)(cx - 1 + k) - tx, dy = (double)(cy - 1 + k) - ty;
-    dx2[k] = dx * dx;
-    dy2[k] = dy * dy;
-  }
-  for (int a = 0; a < 3; ++a) {
-    const int32_t y = cy - 1 + a;
-    if (y < 0 || y >= H) continue;
-    const uint64_t *row = fm + (size_t)y * WR;
-    uint32_t m = 0;
-    for (int k = 0; k < 3; ++k) {
-      const int32_t x = cx - 1 + k;
-      if (x >= 0 && x < W) m |= (uint32_t)((row[x >> 6] >> (x & 63)) & 1) << k;
-    }
-    while (m) {
-      const int k = __builtin_ctz(m);
-      m &= m - 1;
-      const double cost = dx2[k] + dy2[a];
-      if (cost < best) {
-        best = cost;
-        best_t = (int64_t)y * W + cx - 1 + k;
-        bx = cx - 1 + k;
-        by = y;
-      }
-    }
-  }
-}
-
 // Bits of columns x0 .. x0 + n - 1 of a row (n <= 57), 0 for columns off
 // the grid (the map's bits past W are 0 already).
 inline uint64_t window_bits(const uint64_t *row, int32_t x0, int n, int32_t WR) {
@@ -361,6 +332,32 @@ inline uint64_t window_bits(const uint64_t *row, int32_t x0, int n, int32_t WR) 
     m = row[0] << (-x0);
   }
   return m & ((1ull << n) - 1);
+}
+
+// The 3 x 3 block around the nearest site (cx, cy), row-major (tile
+// order), keeping the first least cost: all nine costs formed and selected
+// without branches (a taken or off-grid site counts as infinite).
+inline void probe3(const uint64_t *fm, int32_t WR, int32_t W, int32_t H, int32_t cx, int32_t cy, double tx, double ty,
+                   double &best, int64_t &best_t, int32_t &bx, int32_t &by) {
+  double dx2[3], dy2[3];
+  for (int k = 0; k < 3; ++k) {
+    const double dx = (double)(cx - 1 + k) - tx, dy = (double)(cy - 1 + k) - ty;
+    dx2[k] = dx * dx;
+    dy2[k] = dy * dy;
+  }
+  for (int a = 0; a < 3; ++a) {
+    const int32_t y = cy - 1 + a;
+    if (y < 0 || y >= H) continue;
+    const uint64_t m = window_bits(fm + (size_t)y * WR, cx - 1, 3, WR);
+    for (int k = 0; k < 3; ++k) {
+      const double cost = ((m >> k) & 1) ? dx2[k] + dy2[a] : INFINITY;
+      const bool take = cost < best;
+      best = take ? cost : best;
+      best_t = take ? (int64_t)y * W + cx - 1 + k : best_t;
+      bx = take ? cx - 1 + k : bx;
+      by = take ? y : by;
+    }
+  }
 }
 
 // The (2k+1)^2 block around the unique nearest site (cx, cy): in each of
@@ -571,8 +568,8 @@ __attribute__((target("avx2"), noinline)) void search_rows4(RowSearch &s, int32_
 // only ever shrinks, so every row that could win or tie is visited.
 struct Lanes8 {
   __m512d bc;   // best cost per lane
-  __m512i bt;   // its tile (INT64_MAX: none)
-  __m512i kw;   // k * W for lane k
+  __m256i bt;   // its tile (INT32_MAX: none; the eight-row search runs on chips below 2^31 sites)
+  __m256i kw;   // k * W for lane k
   double best;  // minimum over the scalar rows (the lanes keep theirs in bc)
 };
 
@@ -586,10 +583,10 @@ struct Lanes8 {
 // the lowest tile among its least-cost candidates, as (cost, tile) order
 // asks.
 template <bool DOWN>
-__attribute__((target("avx512f,avx512vl,avx2"))) inline void lane_keep(Lanes8 &L, __m512d c, __m512i t, __mmask8 ok) {
+__attribute__((target("avx512f,avx512vl,avx2"))) inline void lane_keep(Lanes8 &L, __m512d c, __m256i t, __mmask8 ok) {
   const __mmask8 u = ok & _mm512_cmp_pd_mask(c, L.bc, DOWN ? _CMP_LE_OQ : _CMP_LT_OQ);
   L.bc = _mm512_mask_blend_pd(u, L.bc, c);
-  L.bt = _mm512_mask_blend_epi64(u, L.bt, t);
+  L.bt = _mm256_mask_blend_epi32(u, L.bt, t);
 }
 
 // Per-search constants of rows8.
@@ -602,7 +599,7 @@ struct Rows8K {
 // (the caller steps both by 8 rows per call, exactly).
 template <bool DOWN>
 __attribute__((target("avx512f,avx512vl,avx2"))) inline void rows8(RowSearch &s, Lanes8 &L, int32_t r0, __m512d dy,
-                                                                 __m512i base, const Rows8K &K) {
+                                                                 __m256i base, const Rows8K &K) {
   __m256i l = _mm256_loadu_si256(reinterpret_cast<const __m256i *>(s.lc + r0));
   __m256i r = _mm256_loadu_si256(reinterpret_cast<const __m256i *>(s.rc + r0));
   if (_mm256_cmpgt_epi32_mask(l, K.fxv) | _mm256_cmpgt_epi32_mask(K.fx1v, r)) {
@@ -629,11 +626,11 @@ __attribute__((target("avx512f,avx512vl,avx2"))) inline void rows8(RowSearch &s,
   const __mmask8 okl = _mm256_cmpgt_epi32_mask(l, K.m1);
   const __m512d dxl = _mm512_sub_pd(_mm512_cvtepi32_pd(l), K.txv);
   const __m512d cl = _mm512_add_pd(_mm512_mul_pd(dxl, dxl), dy2);
-  const __m512i tl = _mm512_add_epi64(base, _mm512_cvtepi32_epi64(l));
+  const __m256i tl = _mm256_add_epi32(base, l);
   const __mmask8 okr = _mm256_cmpgt_epi32_mask(K.Wv, r);
   const __m512d dxr = _mm512_sub_pd(_mm512_cvtepi32_pd(r), K.txv);
   const __m512d cr = _mm512_add_pd(_mm512_mul_pd(dxr, dxr), dy2);
-  const __m512i tr = _mm512_add_epi64(base, _mm512_cvtepi32_epi64(r));
+  const __m256i tr = _mm256_add_epi32(base, r);
   if (DOWN) {
     lane_keep<true>(L, cr, tr, okr);
     lane_keep<true>(L, cl, tl, okl);
@@ -652,9 +649,9 @@ __attribute__((target("avx512f,avx512vl,avx2"))) inline bool past(const Lanes8 &
 
 __attribute__((target("avx512f,avx512vl,avx2"), noinline)) void search_rows8(RowSearch &s, int32_t cy) {
   scan_row(s, cy);
-  const int64_t W = s.W;
-  Lanes8 L{_mm512_set1_pd(INFINITY), _mm512_set1_epi64(INT64_MAX),
-           _mm512_setr_epi64(0, W, 2 * W, 3 * W, 4 * W, 5 * W, 6 * W, 7 * W), s.best};
+  const int32_t W32 = s.W;
+  Lanes8 L{_mm512_set1_pd(INFINITY), _mm256_set1_epi32(INT32_MAX),
+           _mm256_setr_epi32(0, W32, 2 * W32, 3 * W32, 4 * W32, 5 * W32, 6 * W32, 7 * W32), s.best};
   const Rows8K K{_mm256_set1_epi32(s.fx0), _mm256_set1_epi32(s.fx0 + 1), _mm256_set1_epi32(-1),
                  _mm256_set1_epi32(s.W), _mm512_set1_pd(s.tx)};
   const __m256i iota = _mm256_setr_epi32(0, 1, 2, 3, 4, 5, 6, 7);
@@ -663,10 +660,10 @@ __attribute__((target("avx512f,avx512vl,avx2"), noinline)) void search_rows8(Row
   // cy + 8 up, then eight rows further per call
   __m512d dyd = _mm512_sub_pd(_mm512_cvtepi32_pd(_mm256_add_epi32(_mm256_set1_epi32(cy - 8), iota)), tyv);
   __m512d dyu = _mm512_sub_pd(_mm512_cvtepi32_pd(_mm256_add_epi32(_mm256_set1_epi32(cy + 1), iota)), tyv);
-  __m512i bsd = _mm512_add_epi64(_mm512_set1_epi64((int64_t)(cy - 8) * W), L.kw);
-  __m512i bsu = _mm512_add_epi64(_mm512_set1_epi64((int64_t)(cy + 1) * W), L.kw);
+  __m256i bsd = _mm256_add_epi32(_mm256_set1_epi32((cy - 8) * W32), L.kw);
+  __m256i bsu = _mm256_add_epi32(_mm256_set1_epi32((cy + 1) * W32), L.kw);
   const __m512d step = _mm512_set1_pd(8.0);
-  const __m512i stepw = _mm512_set1_epi64(8 * W);
+  const __m256i stepw = _mm256_set1_epi32(8 * W32);
   bool up = true, down = true;
   int32_t dd = 1, du = 1;
   while (up || down) {
@@ -678,7 +675,7 @@ __attribute__((target("avx512f,avx512vl,avx2"), noinline)) void search_rows8(Row
       } else if (row >= 7) {
         rows8<true>(s, L, row - 7, dyd, bsd, K);
         dyd = _mm512_sub_pd(dyd, step);
-        bsd = _mm512_sub_epi64(bsd, stepw);
+        bsd = _mm256_sub_epi32(bsd, stepw);
         dd += 8;
       } else {
         scan_row(s, row);
@@ -694,7 +691,7 @@ __attribute__((target("avx512f,avx512vl,avx2"), noinline)) void search_rows8(Row
       } else if (row + 7 < s.H) {
         rows8<false>(s, L, row, dyu, bsu, K);
         dyu = _mm512_add_pd(dyu, step);
-        bsu = _mm512_add_epi64(bsu, stepw);
+        bsu = _mm256_add_epi32(bsu, stepw);
         du += 8;
       } else {
         scan_row(s, row);
@@ -704,11 +701,11 @@ __attribute__((target("avx512f,avx512vl,avx2"), noinline)) void search_rows8(Row
     }
   }
   alignas(64) double cs[8];
-  alignas(64) int64_t ts[8];
+  alignas(32) int32_t ts[8];
   _mm512_store_pd(cs, L.bc);
-  _mm512_store_si512(reinterpret_cast<__m512i *>(ts), L.bt);
+  _mm256_store_si256(reinterpret_cast<__m256i *>(ts), L.bt);
   for (int k = 0; k < 8; ++k)
-    if (ts[k] != INT64_MAX) consider(s, cs[k], ts[k]);
+    if (ts[k] != INT32_MAX) consider(s, cs[k], (int64_t)ts[k]);
 }
 }  // namespace
 
