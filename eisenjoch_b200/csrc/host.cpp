@@ -369,7 +369,7 @@ inline void probe_window(const uint64_t *fm, int32_t WR, int32_t W, int32_t H, i
                          int k, double tx, double ty, double &best, int64_t &best_t) {
   const int32_t x0 = cx - k, n = 2 * k + 1, off = fx0 - x0;  // off in [k - 1, k]
   const uint64_t lmask = (2ull << off) - 1;
-  for (int32_t y = std::max(cy - k, 0); y <= std::min(cy + k, H - 1); ++y) {
+  auto row = [&](int32_t y) {
     const uint64_t m = window_bits(fm + (size_t)y * WR, x0, n, WR);
     const double dy = (double)y - ty, dy2 = dy * dy;
     const uint64_t ml = m & lmask, mr = m & ~lmask;
@@ -385,6 +385,18 @@ inline void probe_window(const uint64_t *fm, int32_t WR, int32_t W, int32_t H, i
       const int64_t t = (int64_t)y * W + x;
       if (c < best || (c == best && t < best_t)) { best = c; best_t = t; }
     }
+  };
+  // Rows outward from cy; a side stops once dy^2 exceeds the best cost (no
+  // row past it can win or tie).  The (cost, tile) compare makes the order
+  // of the rows immaterial.
+  row(cy);
+  for (int32_t d = 1; d <= k; ++d) {
+    const int32_t yd = cy - d, yu = cy + d;
+    const double dd = (double)yd - ty, du = (double)yu - ty;
+    const bool okd = yd >= 0 && dd * dd <= best, oku = yu < H && du * du <= best;
+    if (!okd && !oku) break;  // both sides done: |dy| only grows, best only shrinks
+    if (okd) row(yd);
+    if (oku) row(yu);
   }
 }
 
