@@ -841,9 +841,12 @@ eplace_status Legalizer::run(const float *x, const float *y, size_t stride, int3
               best_t = t;
             }
           };
+          // The word holding fa serves both sides when fa + 1 falls in it too.
+          const int32_t jf = fa >> 6;
+          const uint64_t vf = fa >= 0 ? valid_word(ay, jf) : 0ull;
           if (fa >= 0) {  // nearest valid anchor <= fa
-            int32_t j = fa >> 6;
-            uint64_t v = valid_word(ay, j) & (((fa & 63) == 63) ? ~0ull : ((2ull << (fa & 63)) - 1));
+            int32_t j = jf;
+            uint64_t v = vf & (((fa & 63) == 63) ? ~0ull : ((2ull << (fa & 63)) - 1));
             while (true) {
               if (v) {
                 consider((j << 6) + 63 - __builtin_clzll(v));
@@ -856,7 +859,7 @@ eplace_status Legalizer::run(const float *x, const float *y, size_t stride, int3
           if (fa + 1 <= AW - 1) {  // nearest valid anchor >= fa + 1
             const int32_t p = fa + 1;
             int32_t j = p >> 6;
-            uint64_t v = valid_word(ay, j) & (~0ull << (p & 63));
+            uint64_t v = (fa >= 0 && j == jf ? vf : valid_word(ay, j)) & (~0ull << (p & 63));
             while (true) {
               if (v) {
                 consider((j << 6) + __builtin_ctzll(v));
