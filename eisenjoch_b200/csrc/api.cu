@@ -2322,7 +2322,11 @@ struct JobState {
           h.sx.resize(php.N);
           h.sy.resize(php.N);
           raw->st = cc->legal[tid]->run(&h.pos[0].x, &h.pos[0].y, 2, h.sx.data(), h.sy.data(), &raw->disp);
-          if (raw->st == EPLACE_OK) raw->hpwl = hpwl_host(php, h.sx.data(), h.sy.data());
+          // A lone job's last legalisations finish with cores to spare: the
+          // HPWL of a large netlist is summed on four threads there (the job
+          // engine's contexts keep one; its cores are busy with other jobs).
+          const int hpwl_threads = (!cc->shared_device && php.P >= (1u << 19)) ? 4 : 1;
+          if (raw->st == EPLACE_OK) raw->hpwl = hpwl_host(php, h.sx.data(), h.sy.data(), hpwl_threads);
           raw->secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
           raw->done.store(true, std::memory_order_release);
           out->fetch_sub(1, std::memory_order_acq_rel);

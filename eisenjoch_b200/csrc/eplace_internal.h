@@ -91,8 +91,9 @@ struct Legalizer {
   bool simd512_ = false;          // AVX-512F available: eight rows per step
 };
 
-// total_hpwl (metrics/wirelength.rs:10-51) on the host.
-int64_t hpwl_host(const HostProblem &hp, const int32_t *site_x, const int32_t *site_y);
+// total_hpwl (metrics/wirelength.rs:10-51) on the host; with threads > 1 the
+// degree-grouped table is summed in that many pieces at once.
+int64_t hpwl_host(const HostProblem &hp, const int32_t *site_x, const int32_t *site_y, int threads = 1);
 // Fills hp.hpwl_pins / hp.hpwl_runs (counting sort by degree, O(pins)).
 void build_hpwl_table(HostProblem &hp);
 

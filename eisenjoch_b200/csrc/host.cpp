@@ -7,6 +7,8 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <system_error>
+#include <thread>
 
 #include "eplace_internal.h"
 
@@ -977,7 +979,7 @@ void build_hpwl_table(HostProblem &hp) {
   hp.hpwl_table = true;
 }
 
-int64_t hpwl_host(const HostProblem &hp, const int32_t *sx, const int32_t *sy) {
+int64_t hpwl_host(const HostProblem &hp, const int32_t *sx, const int32_t *sy, int threads) {
   int64_t total = 0;
   if (hp.W > 65536 || hp.H > 65536) {
     // Wide grids: the footprint and binding arrays directly.
@@ -1025,11 +1027,55 @@ int64_t hpwl_host(const HostProblem &hp, const int32_t *sx, const int32_t *sy) {
   };
   if (hp.hpwl_table) {
     // Nets grouped by degree: the inner trip count repeats from net to net.
-    const uint32_t *p = hp.hpwl_pins.data();
-    for (const auto &run : hp.hpwl_runs) {
-      const uint32_t d = run.first;
-      for (uint32_t k = 0; k < run.second; ++k, p += d) total += box(p, d);
+    // With threads > 1 the table is cut into that many pieces of about equal
+    // pin count, at net boundaries; the sums are integers, so the total does
+    // not depend on the cut.
+    struct Piece {
+      const uint32_t *p;
+      uint32_t d, nets;
+    };
+    const int nt = std::max(1, std::min(threads, 16));
+    std::vector<std::vector<Piece>> parts((size_t)nt);
+    {
+      const size_t per = (hp.hpwl_pins.size() + nt - 1) / nt;
+      const uint32_t *p = hp.hpwl_pins.data();
+      size_t filled = 0;
+      int t = 0;
+      for (const auto &run : hp.hpwl_runs) {
+        uint32_t d = run.first, left = run.second;
+        while (left) {
+          const size_t room = (size_t)(t + 1) * per > filled ? (size_t)(t + 1) * per - filled : 0;
+          uint32_t take = (uint32_t)std::min<size_t>(left, std::max<size_t>(1, (room + d - 1) / d));
+          if (t == nt - 1) take = left;
+          parts[(size_t)t].push_back(Piece{p, d, take});
+          p += (size_t)take * d;
+          filled += (size_t)take * d;
+          left -= take;
+          if (t < nt - 1 && filled >= (size_t)(t + 1) * per) ++t;
+        }
+      }
     }
+    auto sum = [&](const std::vector<Piece> &ps) {
+      int64_t s = 0;
+      for (const Piece &pc : ps) {
+        const uint32_t *p = pc.p;
+        for (uint32_t k = 0; k < pc.nets; ++k, p += pc.d) s += box(p, pc.d);
+      }
+      return s;
+    };
+    if (nt == 1) return sum(parts[0]);
+    std::vector<int64_t> part((size_t)nt, 0);
+    std::vector<std::thread> th;
+    for (int t = 1; t < nt; ++t) {
+      try {
+        th.emplace_back([&, t] { part[(size_t)t] = sum(parts[(size_t)t]); });
+      } catch (const std::system_error &) {  // no thread to be had: this one sums the piece
+        part[(size_t)t] = sum(parts[(size_t)t]);
+      }
+    }
+    part[0] = sum(parts[0]);
+    for (auto &x : th) x.join();
+    for (int64_t v : part) total += v;
     return total;
   }
   for (uint32_t n = 0; n < hp.NN; ++n) {
