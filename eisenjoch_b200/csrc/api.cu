@@ -3225,7 +3225,7 @@ eplace_status eplace_hpwl_host(const eplace_netlist *nl, const eplace_chip *chip
   }
   if (!hpwl || (hp.N && (!sx || !sy))) return EPLACE_ERR_INVALID;
   build_hpwl_table(hp);
-  *hpwl = hpwl_host(hp, sx, sy);
+  *hpwl = hpwl_host(hp, sx, sy, hp.P >= (1u << 19) ? 4 : 1);  // as a lone job's checkpoints
   return EPLACE_OK;
 }
 

@@ -297,3 +297,17 @@ def test_pin_weights_equal_oracle():
                       fixed_x=np.array([0], np.int32), fixed_y=np.array([0], np.int32))
     w = E.pin_weights(small, E.Chip(4, 4))
     assert np.array_equal(w, np.array([1 / 2 + 1 / 3, 1 / 2 + 1 / 3, 1 / 3 + 1 / 2]))
+
+
+def test_host_hpwl_large_netlist_equals_oracle():
+    """The HPWL of a netlist of 2^19 pins and more is summed in four pieces
+    of the degree table (as a lone job's checkpoints do): the same integer
+    as the oracle's net-by-net walk."""
+    sp = E.SynthSpec(seed=4, num_cells=80000, num_nets=88000, num_pads=800, width=512, height=512, bins_x=256,
+                     bins_y=256, cluster_size=64, macro_fraction=0.05)
+    nl, chip = E.synth_netlist(sp)
+    assert nl.num_pins >= 1 << 19
+    rng = np.random.default_rng(3)
+    sx = rng.integers(0, chip.width - 8, nl.num_cells).astype(np.int32)
+    sy = rng.integers(0, chip.height - 8, nl.num_cells).astype(np.int32)
+    assert E.placer.hpwl_host(nl, chip, sx, sy) == O.Oracle(nl, chip).hpwl(sx, sy)
